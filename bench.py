@@ -1,0 +1,302 @@
+"""Benchmark: solved MDOF/s to relative residual 1e-8 on the L-bracket model (256x128x128 voxels,
+12.8 M DOF), mixed-precision MG-PCG next to the plain FP64 MG-PCG, on one B200 per rank.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl psfea|reference]
+
+A step is one complete solve K u = f to rel. res. 1e-8 (the hierarchy is built once, outside the
+timed region, as the reference keeps its model between solves). Multi-GPU runs are independent
+replicas (one model per GPU, no collective in the data path); the value is the whole-job rate,
+N * nDOF * K / (max over ranks of the timed region). Prints one JSON line on rank 0.
+
+``--impl reference`` times the reference's own CPU solver (oracle/_ref, compiled from its sources;
+the CPU restatement in oracle/ when that library is absent) on the host cores instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "parts-sim_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "solved MDOF/s to rel. res. 1e-8, mixed/batched vs plain FP64 MG-PCG; p50/p99 ms"
+TOL = 1e-8
+MAX_ITER = 5000
+# FP32 V-cycle operator kernel: bytes the algorithm must move per active node (x and y 3x4 B, the
+# mask byte, r, d, 1/diag read and d written: 4x12 B) and per solid voxel (its 4-byte word)
+BYTES_PER_NODE_CHEB32 = 12 + 12 + 1 + 4 * 12
+BYTES_PER_VOXEL = 4
+# iterations of the reference's FP64 MG-PCG on this model to 1e-8, measured with its own solver
+# (oracle/_ref, 8 threads): used to turn a bounded CPU sample into a full-solve time
+REFERENCE_ITERATIONS_L_BRACKET = 1181
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="psfea", choices=["psfea", "reference"])
+    ap.add_argument("--cpu-sample-s", type=float, default=15.0, help="CPU baseline budget (seconds of CPU work)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = os.environ.get("PSFEA_DIST_BACKEND", "nccl")
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def reduce_max(pg, value, device=None):
+    """max over ranks of a float (the driver's rule: time multi-GPU runs as the slowest rank)."""
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[q] for r in self.rows if len(r) > 8 for q in range(4) if r[5 + q].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def active_counts(m):
+    nx, ny, nz = m.dims
+    d = (m.density.reshape(nz, ny, nx) > 0)
+    act = np.zeros((nz + 1, ny + 1, nx + 1), bool)
+    for dk in (0, 1):
+        for dj in (0, 1):
+            for di in (0, 1):
+                act[dk:dk + nz, dj:dj + ny, di:di + nx] |= d
+    return int(act.sum()), int(d.sum())
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(m, sample_s, kind_pref=("reference", "port")):
+    """The reference's CPU solve on this host's cores, on a bounded sample: after one warm-up solve
+    (which also estimates the smoothers), a solve capped at S iterations is timed and the
+    per-iteration time scaled to the full iteration count."""
+    import oracle
+    kind = next(k for k in kind_pref if oracle.available(k))
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("PARTS_SIM_THREADS", str(cores))
+    M = oracle.OracleModel(kind, m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    M.solve(m.f, TOL, 1)
+    t0 = time.perf_counter()
+    M.solve(m.f, TOL, 3)
+    t3 = time.perf_counter() - t0
+    per = max(t3 / 4, 1e-3)
+    S = int(max(4, min(200, sample_s / per)))
+    t0 = time.perf_counter()
+    _, it, _, _ = M.solve(m.f, TOL, S)
+    ts = time.perf_counter() - t0
+    per_it = ts / max(it, 1)
+    full = per_it * REFERENCE_ITERATIONS_L_BRACKET
+    M.close()
+    return {"value": m.n_dof / full / 1e6, "unit": "MDOF/s", "cores": int(os.environ["PARTS_SIM_THREADS"]), "kind": kind,
+            "sample": f"{it} CG iterations of the {m.dims[0]}x{m.dims[1]}x{m.dims[2]} solve timed ({ts:.1f} s), scaled to the "
+                      f"{REFERENCE_ITERATIONS_L_BRACKET} iterations the reference needs for rel. res. 1e-8",
+            "s_per_iteration": per_it}
+
+
+def run_reference(args):
+    rank, world, local, pg = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    from psfea import workloads as W
+    m = W.l_bracket()
+    vals = []
+    for s in range(args.warmup + args.steps):
+        cb = cpu_baseline(m, args.cpu_sample_s / 2)
+        if s >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.median(vals)
+    line = {"metric": METRIC, "value": v, "unit": "MDOF/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": m.n_dof / v / 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "l_bracket 256x128x128 voxels, 64 holes, 500 N tip patch, rtol 1e-8", "n_dof": m.n_dof},
+            "cpu_baseline": {"value": v, "unit": "MDOF/s", "cores": cb["cores"], "kind": cb["kind"], "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": "MDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local, pg = dist_setup(args.gpus)
+    import torch
+    import psfea
+    from psfea import workloads as W
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    m = W.l_bracket()
+    n = m.n_dof
+    S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    stream = torch.cuda.Stream(device=dev)
+    S.set_stream(stream.cuda_stream)
+    f_dev = torch.from_numpy(m.f).to(dev)
+    u_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+
+    def timed(precision, steps, warmup):
+        """device-resident solves; per-solve CUDA-event times on the solver's stream"""
+        for _ in range(warmup):
+            S.solve_dev(f_dev.data_ptr(), u_dev.data_ptr(), tol=TOL, max_iter=MAX_ITER, precision=precision)
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        per, its, kern, res = [], [], 0, []
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        ev[0].record(stream)
+        for s in range(steps):
+            r = S.solve_dev(f_dev.data_ptr(), u_dev.data_ptr(), tol=TOL, max_iter=MAX_ITER, precision=precision)
+            ev[s + 1].record(stream)
+            its.append(r.iterations)
+            kern += r.kernels
+            res.append(r.residual)
+            if not r.converged:
+                raise RuntimeError(f"{precision} solve did not converge: {r}")
+        torch.cuda.synchronize()
+        for s in range(steps):
+            per.append(ev[s].elapsed_time(ev[s + 1]))
+        total = ev[0].elapsed_time(ev[steps])
+        return total, per, its, kern, res
+
+    # plain FP64 MG-PCG (the drop-in), then the mixed-precision form (the headline)
+    t64, per64, it64, k64, res64 = timed("fp64", args.steps, args.warmup)
+    with Clocks(local) as clk:
+        tmx, permx, itmx, kmx, resmx = timed("mixed", args.steps, args.warmup)
+    tmx_max = reduce_max(pg, tmx, dev)
+    t64_max = reduce_max(pg, t64, dev)
+    value = world * n * args.steps / (tmx_max / 1e3) / 1e6
+    plain = world * n * args.steps / (t64_max / 1e3) / 1e6
+
+    # end to end through the C ABI with host buffers (f up, u down, every step)
+    f_host = np.ascontiguousarray(m.f)
+    e2e_t = []
+    for s in range(max(1, args.steps)):
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        r = S.solve(f_host, tol=TOL, max_iter=MAX_ITER, precision="mixed")
+        e2e_t.append(time.perf_counter() - t0)
+        assert r.converged
+    e2e_total = reduce_max(pg, sum(e2e_t), dev)
+    e2e_value = world * n * len(e2e_t) / e2e_total / 1e6
+
+    # roofline of the dominant kernel: the finest level's FP32 Chebyshev operator step
+    ms_cheb = S.time_kernel(0, 20)
+    ms_apply64 = S.time_kernel(1, 20)
+    act_nodes, act_vox = active_counts(m)
+    alg_bytes = act_nodes * BYTES_PER_NODE_CHEB32 + act_vox * BYTES_PER_VOXEL
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ms_cheb / 1e3) / 1e9
+    if rank != 0:
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    cb = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_baseline(m, args.cpu_sample_s)
+            cb.pop("s_per_iteration", None)
+        except Exception as e:  # the oracle build is missing: say so instead of guessing
+            cb = {"value": None, "unit": "MDOF/s", "cores": os.cpu_count(), "kind": "port", "sample": f"unavailable: {e}"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "MDOF/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tmx_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 CG + f32 V-cycle (f16 coarse matrices), f64 refinement", "data": "synthetic",
+        "config": {"workload": "l_bracket 256x128x128 voxels (0.5 mm), 64 y-holes, y=0 held, 500 N tip patch, rtol 1e-8",
+                   "n_dof": n, "free_dof": int(S.level_info(0)["freeDof"]), "levels": S.n_levels,
+                   "parallelism": f"replicas x{world}", "l2": "inputs > L2 (126 MB): x/r/d/1/diag at 51 MB each per level-0 vector"},
+        "latency_ms": {"p50": float(np.percentile(permx, 50)), "p99": float(np.percentile(permx, 99)),
+                       "plain_fp64_p50": float(np.percentile(per64, 50))},
+        "iterations": {"mixed": itmx, "plain_fp64": it64},
+        "residual": {"mixed": max(resmx), "plain_fp64": max(res64)},
+        "plain_fp64": {"value": plain, "unit": "MDOF/s", "ms_per_solve": t64_max / args.steps},
+        "mixed_over_plain": value / plain,
+        "e2e": {"value": e2e_value, "unit": "MDOF/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "kernel": "k_op<float,OP_CHEB> level 0 (FP32 Chebyshev step)", "ms": ms_cheb,
+                     "algorithmic_bytes": alg_bytes, "peak_kind": peak_kind, "fp64_apply_ms": ms_apply64},
+        "cpu_baseline": cb,
+        "gpu_launches": int(kmx),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,182 @@
+/*
+ * psfea — B200 (sm_100a) matrix-free voxel elasticity solver behind a C ABI.
+ *
+ * Drop-in for Parts Sim's linear-static solve: the reference's C++ class
+ *   ps::VoxelFEA(dims, density, nu, bc, coarsestMaxDof = 1100, diagAdd = nullptr)
+ *       native/src/fea/voxel_fea.hpp:136-137
+ *   SolveResult VoxelFEA::solve(const std::vector<double>& f, const SolveOptions&)
+ *       native/src/fea/voxel_fea.hpp:112-124, :153
+ *   void VoxelFEA::precondition(const double* r, double* z)      native/src/fea/voxel_fea.hpp:151
+ *   void VoxelFEA::apply(int l, const double* x, double* y, bool raw) native/src/fea/voxel_fea.hpp:143
+ *   NodalStresses VoxelFEA::stresses(u, E, h, principals)        native/src/fea/voxel_fea.hpp:157
+ *   std::array<double,3> VoxelFEA::reactions(u, f)              native/src/fea/voxel_fea.hpp:154
+ * and of its GPU sibling ps::GpuFeaSolver (native/src/gpu/gpu_fea.hpp:17-35), which has the same
+ * solve/precondition contract.
+ *
+ * Layout (identical to the reference): voxel e = i + nx*(j + ny*k); node n = i + NX*(j + NY*k)
+ * with NX = nx+1 etc.; DOF 3n + d. Units are the solver's normalised ones (E = 1, voxel size 1):
+ * u_physical = u / (E*h) for forces in N.
+ *
+ * All pointers are plain host pointers unless the name says _dev (device pointers on the
+ * handle's CUDA device). Errors are status codes (the reference throws std::invalid_argument for
+ * the PS_EINVAL / PS_ENONFINITE cases). ps_last_error() gives the message of the calling thread's
+ * last failure. A handle may be used from one thread at a time.
+ */
+#ifndef PS_FEA_H
+#define PS_FEA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PS_FEA_ABI_VERSION 1
+
+typedef enum ps_status {
+    PS_OK = 0,              /* converged: true relative residual <= 10 * tol (voxel_fea.cpp:925) */
+    PS_NOT_CONVERGED = 1,   /* iteration cap reached; u and residual are still returned */
+    PS_BREAKDOWN = 2,       /* p.Kp <= 0 (a mechanism; voxel_fea.cpp:904); u is returned */
+    PS_CANCELLED = 3,       /* the cancel flag was raised; u is returned */
+    PS_TIMEOUT = 4,         /* the time limit ran out; u is returned */
+    PS_EINVAL = 10,         /* bad dims, sizes, density or nu (voxel_fea.cpp:141-146, hex8.cpp:9) */
+    PS_ENONFINITE = 11,     /* non-finite f or x0 (voxel_fea.cpp:866-868) */
+    PS_EOOM = 12,           /* device memory or admission budget exhausted */
+    PS_ECUDA = 13,          /* CUDA runtime failure */
+    PS_ENODEV = 14          /* no usable CUDA device */
+} ps_status;
+
+typedef enum ps_precision {
+    /* The drop-in: FP64 flexible CG (Polak-Ribiere beta) preconditioned by the FP32 multigrid
+     * V-cycle with r scaled to order one, exactly the reference's VoxelFEA::solve
+     * (voxel_fea.cpp:835-927). */
+    PS_PREC_FP64 = 0,
+    /* FP32 CG and FP32 V-cycle with FP16 coarse-level element matrices, kept to FP64 accuracy by
+     * reliable updates: whenever the FP32 residual has dropped tenfold the FP32 iterate is folded
+     * into the FP64 solution and the FP64 defect f - K u replaces the FP32 residual. */
+    PS_PREC_MIXED = 1
+} ps_precision;
+
+typedef struct ps_fea ps_fea_t;
+
+typedef struct ps_solve_opts {
+    double tol;                       /* relative residual target (reference default 1e-6) */
+    int32_t max_iter;                 /* reference default 500 */
+    int32_t precision;                /* ps_precision */
+    const double* x0;                 /* warm start, nDof values, or NULL (voxel_fea.hpp:115) */
+    const volatile int32_t* cancel;   /* polled between iteration batches; nonzero cancels (the
+                                         onProgress-returns-true contract, voxel_fea.cpp:910) */
+    double time_limit_s;              /* 0 = none */
+} ps_solve_opts;
+
+typedef struct ps_solve_result {
+    int32_t iterations;   /* CG iterations (voxel_fea.hpp:121) */
+    int32_t converged;    /* residual <= 10 * tol */
+    int32_t status;       /* ps_status of the outcome */
+    int32_t folds;        /* PS_PREC_MIXED: number of FP64 reliable updates */
+    double residual;      /* true relative residual ||f - K u|| / ||f_free||, in FP64 */
+    double seconds;       /* wall time of the call */
+    int64_t kernels;      /* device kernels this call launched */
+} ps_solve_result;
+
+/* tol 1e-6, max_iter 500, PS_PREC_FP64, no warm start, no cancel flag, no time limit */
+void ps_solve_opts_default(ps_solve_opts* opts);
+
+/* Builds the multigrid hierarchy (2:1 coarsening with exact Galerkin coarse elements until the
+ * free DOFs are <= coarsest_max_dof or 12 levels; dense FP64 factor of the coarsest level) and
+ * uploads it to the current CUDA device. Replaces VoxelFEA::VoxelFEA (voxel_fea.cpp:138-183).
+ * density: nx*ny*nz floats in [0, 1]; bc: 3*NX*NY*NZ bytes (1 = held); diag_add: nDof doubles
+ * added to K's diagonal, or NULL. */
+ps_status ps_fea_create(const int32_t dims[3], const float* density, double nu, const uint8_t* bc,
+                        int64_t coarsest_max_dof, const double* diag_add, ps_fea_t** out);
+
+/* K u = f (voxel_fea.cpp:863-927 / gpu_fea.cpp:452-574). f and u_out: nDof doubles on the host.
+ * Returns the outcome status; u_out and *result are filled for PS_OK .. PS_TIMEOUT.
+ * result may be NULL; opts may be NULL (defaults). */
+ps_status ps_fea_solve(ps_fea_t* h, const double* f, const ps_solve_opts* opts, double* u_out,
+                       ps_solve_result* result);
+
+/* The same solve with f, x0 (opts->x0 is then a device pointer) and u already in device memory. */
+ps_status ps_fea_solve_dev(ps_fea_t* h, const double* f_dev, const ps_solve_opts* opts, double* u_dev,
+                           ps_solve_result* result);
+
+/* nrhs solves on one hierarchy (the multi-load-case form: the sizing study's load groups,
+ * study_runner.cpp:453-465, run as one batch). f and u_out: nrhs consecutive nDof vectors.
+ * results: nrhs entries or NULL. opts->x0 (if set) holds nrhs warm starts. Returns the worst
+ * outcome status. */
+ps_status ps_fea_solve_batch(ps_fea_t* h, int32_t nrhs, const double* f, const ps_solve_opts* opts,
+                             double* u_out, ps_solve_result* results);
+
+/* One V-cycle as a preconditioner, z ~ K^-1 r (voxel_fea.cpp:830-861; gpu_fea.cpp:431-450). */
+ps_status ps_fea_precondition(ps_fea_t* h, const double* r, double* z);
+
+/* y = K x on level `level` in FP64; held/inactive DOFs of y zeroed unless raw
+ * (voxel_fea.cpp:388). */
+ps_status ps_fea_apply(ps_fea_t* h, int32_t level, const double* x, double* y, int32_t raw);
+
+/* Nodal von Mises and (if principals) first/third principal stresses in Pa from physical
+ * displacements u [m] (voxel_fea.cpp:968-1037). vm, p1, p3: NX*NY*NZ floats; p1/p3 may be NULL
+ * when principals == 0. */
+ps_status ps_fea_stresses(ps_fea_t* h, const double* u, double E, double vox, int32_t principals,
+                          float* vm, float* p1, float* p3);
+
+/* Support reactions: sum over held DOFs of active nodes of (K u - f); f may be NULL
+ * (voxel_fea.cpp:929-940). */
+ps_status ps_fea_reactions(ps_fea_t* h, const double* u, const double* f, double reaction[3]);
+
+/* Routes all of the handle's device work to a caller-owned cudaStream_t (NULL = its own stream). */
+ps_status ps_fea_set_stream(ps_fea_t* h, void* cuda_stream);
+
+/* Mean device time in ms (CUDA events, `reps` back-to-back launches on the handle's stream) of the
+ * finest level's operator kernel: which = 0 the FP32 Chebyshev smoothing step of the V-cycle,
+ * 1 the FP64 product of the CG. Diagnostics for roofline reports. */
+ps_status ps_fea_time_kernel(ps_fea_t* h, int32_t which, int32_t reps, double* ms);
+
+/* Device kernels the handle has launched since it was created. */
+int64_t ps_fea_kernel_launches(const ps_fea_t* h);
+
+int64_t ps_fea_ndof(const ps_fea_t* h);
+int32_t ps_fea_num_levels(const ps_fea_t* h);
+/* info[9] = nx, ny, nz, nNodes, nDof, freeDof, nElems, nOwn (own coarse matrices), coarsest m */
+ps_status ps_fea_level_info(const ps_fea_t* h, int32_t level, int64_t info[9]);
+/* the level's fixed-DOF mask (1 = held, inactive or zero diagonal; voxel_fea.cpp:227-232) */
+ps_status ps_fea_level_fixed(const ps_fea_t* h, int32_t level, uint8_t* out);
+/* the smoother's eigenvalue estimate of D^-1 K on a level (0 until the first solve) */
+double ps_fea_level_lmax(const ps_fea_t* h, int32_t level);
+/* bytes of device memory the handle holds */
+int64_t ps_fea_device_bytes(const ps_fea_t* h);
+
+void ps_fea_destroy(ps_fea_t* h);
+
+/* The host-side hierarchy alone (no device memory, no GPU needed): the same build as
+ * ps_fea_create, for inspecting levels, masks and coarse matrices (the reference exposes them as
+ * the public member VoxelFEA::levels, voxel_fea.hpp:164). */
+typedef struct ps_hierarchy ps_hierarchy_t;
+ps_status ps_hierarchy_create(const int32_t dims[3], const float* density, double nu, const uint8_t* bc,
+                              int64_t coarsest_max_dof, const double* diag_add, ps_hierarchy_t** out);
+int32_t ps_hierarchy_num_levels(const ps_hierarchy_t* h);
+ps_status ps_hierarchy_level_info(const ps_hierarchy_t* h, int32_t level, int64_t info[9]);
+ps_status ps_hierarchy_level_fixed(const ps_hierarchy_t* h, int32_t level, uint8_t* out);
+/* own coarse matrices in increasing coarse-voxel order: nOwn * 576 floats */
+ps_status ps_hierarchy_level_own(const ps_hierarchy_t* h, int32_t level, float* out);
+/* the level's uniform element Kb (576 doubles) */
+ps_status ps_hierarchy_level_kb(const ps_hierarchy_t* h, int32_t level, double* out);
+void ps_hierarchy_destroy(ps_hierarchy_t* h);
+
+/* Condensed 24x24 unit-cube element (E = 1) with 9 Wilson incompatible modes, and its corner
+ * stress matrices D*Bbar (8 x 6 x 24); corner_stress may be NULL (hex8.cpp:104-155). */
+ps_status ps_element_matrix(double nu, double K[576], double* corner_stress);
+
+/* Voxels not face-connected to a voxel touching a held node become empty
+ * (pruneFloating, voxel_fea.cpp:1086-1119). held_node: NX*NY*NZ bytes. */
+ps_status ps_prune_floating(const int32_t dims[3], const float* density, const uint8_t* held_node,
+                            float* out, int32_t* removed);
+
+/* Message of the calling thread's last error ("" if none). */
+const char* ps_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PS_FEA_H */

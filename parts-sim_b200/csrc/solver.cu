@@ -1,0 +1,1345 @@
+// Device-resident multigrid-preconditioned CG for one voxel model on one B200 (sm_100a).
+//
+// The solve loop never waits for the host inside an iteration: dot products finish in the last
+// block of the kernel that computes them (deterministic order), which also derives alpha / beta
+// and the stop decision into a device-side state record; every later kernel of the iteration reads
+// that record and exits at once when the solve is over. The host replays a CUDA graph of one
+// iteration in batches and reads the record back only between batches.
+//
+// Algorithms (rules of the reference, native/src/fea/voxel_fea.cpp):
+//   operator apply ......................... :393-504
+//   degree-2 Chebyshev smoother ............ :692-725
+//   restriction / prolongation ............. :739-815
+//   V-cycle ................................ :817-828
+//   FP32 preconditioner, r scaled to O(1) .. :835-861
+//   flexible PCG, Polak-Ribiere beta ....... :863-927
+//   Lanczos smoother bound (LCG start) ..... :579-610
+// The mixed-precision form keeps the CG in FP32 and folds its iterate into an FP64 solution with
+// the FP64 defect as its new residual whenever the FP32 residual has fallen tenfold ("reliable
+// updates", Sleijpen & van der Vorst 1996; the reference GPU solver does the fold on the CPU,
+// native/src/gpu/gpu_fea.cpp:452-574); here it is a device kernel.
+#include "solver.hpp"
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "host_util.hpp"
+#include "kernels.cuh"
+
+namespace psfea {
+
+namespace dev {
+
+// ---------------------------------------------------------------- control
+
+struct SolveState {
+    double bnorm, rel, tol, rz, alpha, beta, rmax, scale, peak, est, pq;
+    int it, maxIter, done, status, fold, folds, first, mixed;
+};
+enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_BREAKDOWN = 3 };
+
+// a kernel runs unless *skipIf != 0 or (runIf and *runIf == 0)
+struct Ctl {
+    const int* skipIf;
+    const int* runIf;
+};
+__device__ __forceinline__ bool skipped(const Ctl& c) {
+    if (c.skipIf && *((volatile const int*)c.skipIf)) return true;
+    if (c.runIf && !*((volatile const int*)c.runIf)) return true;
+    return false;
+}
+
+__device__ __forceinline__ bool fixedDof(uint8_t mask, int d) { return (mask >> d) & 1; }
+
+constexpr int NODE_THREADS = 128;
+constexpr int VEC_THREADS = 256;
+
+// ---------------------------------------------------------------- operator kernels
+
+enum { OP_APPLY = 0, OP_CHEB = 1, OP_RESID = 2 };
+
+// One pass over the level's nodes of y = K x with a per-node epilogue:
+//   OP_APPLY  y = K x (held DOFs 0 unless raw)
+//   OP_CHEB   d = c1 d + c2 D^-1 (r - K x); y = x + d      (Chebyshev / Jacobi step, 32-bit)
+//   OP_RESID  y = r - K x
+template <class T, int MODE, bool OWN16>
+__global__ void __launch_bounds__(NODE_THREADS) k_op(LevelView L, Coefs<T> C, const T* __restrict__ x, T* __restrict__ y,
+                                                      const float* __restrict__ r, float* __restrict__ d, float c1, float c2, int raw,
+                                                      Ctl ctl) {
+    if (skipped(ctl)) return;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < L.nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = __ldg(L.nmask + n);
+        int i, j, k;
+        nodeCoords(L, n, i, j, k);
+        T acc[3];
+        applyAt<T, OWN16>(L, C, x, i, j, k, n, mask, acc);
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const long long id = 3 * n + q;
+            const bool fx = fixedDof(mask, q);
+            if (MODE == OP_APPLY) {
+                y[id] = (!raw && fx) ? T(0) : acc[q];
+            } else if (MODE == OP_RESID) {
+                y[id] = fx ? T(0) : T(r[id]) - acc[q];
+            } else {
+                if (fx) {
+                    d[id] = 0.f;
+                    y[id] = T(0);
+                } else {
+                    const float dn = c1 * d[id] + c2 * L.invD[id] * (r[id] - float(acc[q]));
+                    d[id] = dn;
+                    y[id] = x[id] + T(dn);
+                }
+            }
+        }
+    }
+}
+
+// q = K p on the finest level with the CG step length: alpha = rz / (p . q) (FP64 accumulation);
+// p.q <= 0 ends the solve as a breakdown (voxel_fea.cpp:902-905)
+template <class T, bool OWN16>
+__global__ void __launch_bounds__(NODE_THREADS) k_apply_alpha(LevelView L, Coefs<T> C, const T* __restrict__ p, T* __restrict__ q,
+                                                              SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
+    if (skipped(ctl)) return;
+    double v[1] = {0.0};
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < L.nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = __ldg(L.nmask + n);
+        int i, j, k;
+        nodeCoords(L, n, i, j, k);
+        T acc[3];
+        applyAt<T, OWN16, (sizeof(T) == 4)>(L, C, p, i, j, k, n, mask, acc);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const T y = fixedDof(mask, c) ? T(0) : acc[c];
+            q[3 * n + c] = y;
+            v[0] += double(p[3 * n + c]) * double(y);
+        }
+    }
+    double tot[1];
+    if (gridReduce<1>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) {
+        const double pq = tot[0];
+        st->pq = pq;
+        if (!(pq > 0)) {
+            st->status = ST_BREAKDOWN;
+            if (st->mixed) st->fold = 1;  // fold what there is, then stop
+            else st->done = 1;
+        } else {
+            st->alpha = st->rz / pq;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- V-cycle pieces (32-bit)
+
+// z = d = c0 D^-1 r (the first Chebyshev step from zero)
+__global__ void k_cheb_first(long long nDof, const float* __restrict__ r, const float* __restrict__ invD, float* __restrict__ d,
+                             float* __restrict__ z, float c0, Ctl ctl) {
+    if (skipped(ctl)) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x) {
+        const float v = c0 * invD[i] * r[i];
+        d[i] = v;
+        z[i] = v;
+    }
+}
+
+// rc = P^T rf gathered per coarse node: fine 2I (weight 1) and 2I +- 1 (weight 1/2) per axis;
+// held / inactive coarse DOFs 0
+__global__ void k_restrict(int FNX, int FNY, int FNZ, LevelView C, const float* __restrict__ rf, float* __restrict__ rc, Ctl ctl) {
+    if (skipped(ctl)) return;
+    const long long FNXY = (long long)FNX * FNY;
+    for (long long cn = blockIdx.x * (long long)blockDim.x + threadIdx.x; cn < C.nNodes; cn += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = C.nmask[cn];
+        float s0 = 0, s1 = 0, s2 = 0;
+        if (mask & NM_ACTIVE) {
+            int I, J, K;
+            nodeCoords(C, cn, I, J, K);
+            for (int dk = -1; dk <= 1; dk++) {
+                const int k = 2 * K + dk;
+                if (k < 0 || k >= FNZ) continue;
+                const float wk = dk ? 0.5f : 1.f;
+                for (int dj = -1; dj <= 1; dj++) {
+                    const int j = 2 * J + dj;
+                    if (j < 0 || j >= FNY) continue;
+                    const float wj = (dj ? 0.5f : 1.f) * wk;
+                    for (int di = -1; di <= 1; di++) {
+                        const int i = 2 * I + di;
+                        if (i < 0 || i >= FNX) continue;
+                        const float w = (di ? 0.5f : 1.f) * wj;
+                        const float* p = rf + 3 * (i + j * (long long)FNX + k * FNXY);
+                        s0 += w * p[0];
+                        s1 += w * p[1];
+                        s2 += w * p[2];
+                    }
+                }
+            }
+        }
+        rc[3 * cn] = fixedDof(mask, 0) ? 0.f : s0;
+        rc[3 * cn + 1] = fixedDof(mask, 1) ? 0.f : s1;
+        rc[3 * cn + 2] = fixedDof(mask, 2) ? 0.f : s2;
+    }
+}
+
+// zf += P zc at free fine DOFs (trilinear: coarse i/2 and, when odd, (i+1)/2, weight 1/2 each)
+__global__ void k_prolong(LevelView F, int CNX, int CNY, const float* __restrict__ zc, float* __restrict__ zf, Ctl ctl) {
+    if (skipped(ctl)) return;
+    const long long CNXY = (long long)CNX * CNY;
+    for (long long fn = blockIdx.x * (long long)blockDim.x + threadIdx.x; fn < F.nNodes; fn += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = F.nmask[fn];
+        if ((mask & 7) == 7) continue;
+        int i, j, k;
+        nodeCoords(F, fn, i, j, k);
+        const int i0 = i >> 1, j0 = j >> 1, k0 = k >> 1;
+        const int ni = (i & 1) ? 2 : 1, nj = (j & 1) ? 2 : 1, nk = (k & 1) ? 2 : 1;
+        const float w = ((i & 1) ? 0.5f : 1.f) * ((j & 1) ? 0.5f : 1.f) * ((k & 1) ? 0.5f : 1.f);
+        float s0 = 0, s1 = 0, s2 = 0;
+        for (int c = 0; c < nk; c++)
+            for (int b = 0; b < nj; b++)
+                for (int a = 0; a < ni; a++) {
+                    const float* p = zc + 3 * ((i0 + a) + (j0 + b) * (long long)CNX + (k0 + c) * CNXY);
+                    s0 += w * p[0];
+                    s1 += w * p[1];
+                    s2 += w * p[2];
+                }
+        if (!fixedDof(mask, 0)) zf[3 * fn] += s0;
+        if (!fixedDof(mask, 1)) zf[3 * fn + 1] += s1;
+        if (!fixedDof(mask, 2)) zf[3 * fn + 2] += s2;
+    }
+}
+
+// coarsest level: z = A^-1 r over the m free DOFs (FP64 dense inverse, one warp per row);
+// r, z are the level's vectors (float or double), held DOFs of z are never written (stay 0)
+template <class TI, class TO>
+__global__ void k_coarse(int m, const int* __restrict__ dof, const double* __restrict__ Ainv, const TI* __restrict__ r, TO* __restrict__ z,
+                         Ctl ctl) {
+    if (skipped(ctl)) return;
+    extern __shared__ double rs[];
+    for (int q = threadIdx.x; q < m; q += blockDim.x) rs[q] = double(r[dof[q]]);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < m; row += gridDim.x * warps) {
+        const double* a = Ainv + (size_t)row * m;
+        double s = 0;
+        for (int c = lane; c < m; c += 32) s += a[c] * rs[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) z[dof[row]] = TO(s);
+    }
+}
+
+// ---------------------------------------------------------------- FP64 CG vector kernels
+
+// r = f - q at free DOFs (0 at held); bnorm = ||f_free||, rel = ||r|| / bnorm, rmax = max |r_free|
+// (voxel_fea.cpp:876-886). Zero load: x = 0 and the solve is over (voxel_fea.cpp:880-884).
+__global__ void k_cg_init(long long nNodes, const uint8_t* __restrict__ nmask, const double* __restrict__ f, const double* __restrict__ q,
+                          double* __restrict__ r, float* __restrict__ r32, SolveState* st, double* partials, unsigned* ticket) {
+    double v[3] = {0, 0, 0};
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const long long id = 3 * n + c;
+            double rv = 0;
+            if (!fixedDof(mask, c)) {
+                const double fv = f[id];
+                rv = fv - q[id];
+                v[0] += fv * fv;
+                v[1] += rv * rv;
+                v[2] = fmax(v[2], fabs(rv));
+            }
+            r[id] = rv;
+        }
+    }
+    double tot[3];
+    if (gridReduce<3>(v, 4u, partials, ticket, tot) && threadIdx.x == 0) {
+        st->bnorm = sqrt(tot[0]);
+        st->rmax = tot[2];
+        st->scale = tot[2] > 0 ? 1.0 / tot[2] : 1.0;
+        st->peak = 0;
+        if (st->bnorm == 0) {
+            st->rel = 0;
+            st->status = ST_CONVERGED;
+            st->done = 2;  // 2 = zero load: the solution is zero
+        } else {
+            st->rel = sqrt(tot[1]) / st->bnorm;
+            st->peak = st->rel;
+            if (st->rel <= st->tol) {
+                st->status = ST_CONVERGED;
+                st->done = 1;
+            } else if (st->maxIter <= 0) {
+                st->status = ST_MAXITER;
+                st->done = 1;
+            }
+        }
+    }
+    (void)r32;
+}
+
+// x += alpha p, r -= alpha q at free DOFs; rel = ||r|| / bnorm; stop on rel <= tol or the cap
+__global__ void k_cg_update(long long nNodes, const uint8_t* __restrict__ nmask, double* __restrict__ x, double* __restrict__ r,
+                            const double* __restrict__ p, const double* __restrict__ q, SolveState* st, double* partials, unsigned* ticket,
+                            Ctl ctl) {
+    if (skipped(ctl)) return;
+    const double alpha = st->alpha;
+    double v[2] = {0, 0};
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            if (fixedDof(mask, c)) continue;
+            const long long id = 3 * n + c;
+            x[id] += alpha * p[id];
+            const double rv = r[id] - alpha * q[id];
+            r[id] = rv;
+            v[0] += rv * rv;
+            v[1] = fmax(v[1], fabs(rv));
+        }
+    }
+    double tot[2];
+    if (gridReduce<2>(v, 2u, partials, ticket, tot) && threadIdx.x == 0) {
+        st->rel = sqrt(tot[0]) / st->bnorm;
+        st->rmax = tot[1];
+        st->scale = tot[1] > 0 ? 1.0 / tot[1] : 1.0;
+        st->it += 1;
+        if (st->rel <= st->tol) {
+            st->status = ST_CONVERGED;
+            st->done = 1;
+        } else if (st->it >= st->maxIter) {
+            st->status = ST_MAXITER;
+            st->done = 1;
+        }
+    }
+}
+
+// the preconditioner's input: r32 = float(r / max|r_free|) at free DOFs (voxel_fea.cpp:856-857)
+__global__ void k_vc_load(long long nNodes, const uint8_t* __restrict__ nmask, const double* __restrict__ r, float* __restrict__ r32,
+                          const SolveState* st, Ctl ctl) {
+    if (skipped(ctl)) return;
+    const double s = st->scale;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+#pragma unroll
+        for (int c = 0; c < 3; c++) r32[3 * n + c] = fixedDof(mask, c) ? 0.f : float(r[3 * n + c] * s);
+    }
+}
+
+// z = z32 * rmax (or z64); rzNew = r.z, zq = z.q; beta = max(0, -alpha zq / rz) (voxel_fea.cpp:913-917);
+// on the first pass beta = 0
+__global__ void k_cg_dots(long long nDof, const double* __restrict__ r, const float* __restrict__ z32, const double* __restrict__ z64,
+                          const double* __restrict__ q, SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
+    if (skipped(ctl)) return;
+    const double rmax = st->rmax;
+    const bool first = st->first;
+    double v[2] = {0, 0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x) {
+        const double z = z64 ? z64[i] : double(z32[i]) * rmax;
+        v[0] += r[i] * z;
+        if (!first) v[1] += z * q[i];
+    }
+    double tot[2];
+    if (gridReduce<2>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) {
+        st->beta = first ? 0.0 : fmax(0.0, -st->alpha * tot[1] / st->rz);
+        st->rz = tot[0];
+    }
+}
+
+// p = z + beta p
+__global__ void k_cg_p(long long nDof, const float* __restrict__ z32, const double* __restrict__ z64, double* __restrict__ p, SolveState* st,
+                       Ctl ctl) {
+    if (skipped(ctl)) return;
+    const double rmax = st->rmax, beta = st->beta;
+    const bool first = st->first;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x) {
+        const double z = z64 ? z64[i] : double(z32[i]) * rmax;
+        p[i] = first ? z : z + beta * p[i];
+    }
+}
+
+__global__ void k_clear_first(SolveState* st) { st->first = 0; }
+
+// true residual after the loop: ||f - K x|| over all DOFs / bnorm (voxel_fea.cpp:921-925)
+__global__ void k_final(long long nNodes, const uint8_t* __restrict__ nmask, const double* __restrict__ f, const double* __restrict__ q,
+                        SolveState* st, double* partials, unsigned* ticket) {
+    double v[1] = {0};
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            if (!fixedDof(mask, c)) {
+                const double rv = f[3 * n + c] - q[3 * n + c];
+                v[0] += rv * rv;
+            }
+    }
+    double tot[1];
+    if (gridReduce<1>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) st->rel = st->bnorm > 0 ? sqrt(tot[0]) / st->bnorm : 0.0;
+}
+
+// ---------------------------------------------------------------- mixed precision (FP32 CG + FP64 folds)
+
+// x32 += alpha p32, r32 -= alpha q32; est = ||r32|| / (scale * bnorm); fold when est <= tol or it has
+// fallen tenfold since the last fold, or at the iteration cap
+__global__ void k_mx_update(long long nNodes, const uint8_t* __restrict__ nmask, float* __restrict__ x, float* __restrict__ r,
+                            const float* __restrict__ p, const float* __restrict__ q, SolveState* st, double* partials, unsigned* ticket,
+                            Ctl ctl) {
+    if (skipped(ctl) || st->fold) return;
+    const float alpha = float(st->alpha);
+    double v[1] = {0};
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            if (fixedDof(mask, c)) continue;
+            const long long id = 3 * n + c;
+            x[id] += alpha * p[id];
+            const float rv = r[id] - alpha * q[id];
+            r[id] = rv;
+            v[0] += double(rv) * rv;
+        }
+    }
+    double tot[1];
+    if (gridReduce<1>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) {
+        st->est = sqrt(tot[0]) / st->scale / st->bnorm;
+        st->it += 1;
+        st->peak = fmax(st->peak, st->est);
+        if (st->est <= st->tol || st->est <= 0.1 * st->peak || st->it >= st->maxIter || !(st->est == st->est)) st->fold = 1;
+    }
+}
+
+// fold part 1: u += x32 / scale, x32 = 0
+__global__ void k_mx_fold1(long long nDof, double* __restrict__ u, float* __restrict__ x32, const SolveState* st, Ctl ctl) {
+    if (skipped(ctl)) return;
+    const double inv = 1.0 / st->scale;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x) {
+        u[i] += double(x32[i]) * inv;
+        x32[i] = 0.f;
+    }
+}
+
+// fold part 2 (after q = K u in FP64): r64 = f - q, rel = ||r64|| / bnorm, r32 = float(r64 * scale);
+// stop when rel <= tol, at the cap or after a breakdown
+__global__ void k_mx_fold2(long long nNodes, const uint8_t* __restrict__ nmask, const double* __restrict__ f, const double* __restrict__ q,
+                           float* __restrict__ r32, SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
+    if (skipped(ctl)) return;
+    const double s = st->scale;
+    double v[1] = {0};
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const long long id = 3 * n + c;
+            double rv = 0;
+            if (!fixedDof(mask, c)) rv = f[id] - q[id];
+            v[0] += rv * rv;
+            r32[id] = float(rv * s);
+        }
+    }
+    double tot[1];
+    if (gridReduce<1>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) {
+        st->rel = sqrt(tot[0]) / st->bnorm;
+        st->peak = st->rel;
+        st->folds += 1;
+        st->fold = 0;
+        if (st->status == ST_BREAKDOWN) st->done = 1;
+        else if (st->rel <= st->tol) {
+            st->status = ST_CONVERGED;
+            st->done = 1;
+        } else if (st->it >= st->maxIter || !(st->rel == st->rel)) {
+            st->status = ST_MAXITER;
+            st->done = 1;
+        }
+    }
+}
+
+// rzNew = r32.z32, zq = z32.q32 (FP64 sums); beta as in the FP64 form
+__global__ void k_mx_dots(long long nDof, const float* __restrict__ r, const float* __restrict__ z, const float* __restrict__ q,
+                          SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
+    if (skipped(ctl)) return;
+    const bool first = st->first;
+    double v[2] = {0, 0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x) {
+        v[0] += double(r[i]) * z[i];
+        if (!first) v[1] += double(z[i]) * q[i];
+    }
+    double tot[2];
+    if (gridReduce<2>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) {
+        st->beta = first ? 0.0 : fmax(0.0, -st->alpha * tot[1] / st->rz);
+        st->rz = tot[0];
+    }
+}
+
+__global__ void k_mx_p(long long nDof, const float* __restrict__ z, float* __restrict__ p, const SolveState* st, Ctl ctl) {
+    if (skipped(ctl)) return;
+    const float beta = float(st->beta);
+    const bool first = st->first;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x)
+        p[i] = first ? z[i] : z[i] + beta * p[i];
+}
+
+// ---------------------------------------------------------------- misc
+
+__global__ void k_mask_copy(long long nNodes, const uint8_t* __restrict__ nmask, const double* __restrict__ src, double* __restrict__ dst) {
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+#pragma unroll
+        for (int c = 0; c < 3; c++) dst[3 * n + c] = (src && !fixedDof(mask, c)) ? src[3 * n + c] : 0.0;
+    }
+}
+
+// max |r| over free DOFs into st->rmax / st->scale (the preconditioner entry point)
+__global__ void k_rmax(long long nNodes, const uint8_t* __restrict__ nmask, const double* __restrict__ r, SolveState* st, double* partials,
+                       unsigned* ticket) {
+    double v[1] = {0};
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            if (!fixedDof(mask, c)) v[0] = fmax(v[0], fabs(r[3 * n + c]));
+    }
+    double tot[1];
+    if (gridReduce<1>(v, 1u, partials, ticket, tot) && threadIdx.x == 0) {
+        st->rmax = tot[0];
+        st->scale = tot[0] > 0 ? 1.0 / tot[0] : 1.0;
+    }
+}
+
+// z = z32 * rmax on active nodes, 0 elsewhere (voxel_fea.cpp:859-860)
+__global__ void k_vc_store(long long nNodes, const uint8_t* __restrict__ nmask, const float* __restrict__ z32, double* __restrict__ z,
+                           const SolveState* st) {
+    const double rmax = st->rmax;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const bool act = nmask[n] & NM_ACTIVE;
+#pragma unroll
+        for (int c = 0; c < 3; c++) z[3 * n + c] = (act && rmax > 0) ? double(z32[3 * n + c]) * rmax : 0.0;
+    }
+}
+
+// ---- Lanczos (FP64) for the smoother's eigenvalue bound
+
+// v_i = LCG value i (seed 12345, s <- (1103515245 s + 12345) mod 2^31, voxel_fea.cpp:584-588),
+// computed for every index at once by jumping the affine recurrence ahead i + 1 steps
+__global__ void k_lz_start(long long nNodes, const uint8_t* __restrict__ nmask, double* __restrict__ v, double* partials, unsigned* ticket,
+                           SolveState* st) {
+    double acc[1] = {0};
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const unsigned long long steps = (unsigned long long)(3 * n + c) + 1;
+            // (A, B): s -> A s + B for 2^bit steps; (RA, RB) accumulated
+            unsigned long long A = 1103515245ull, B = 12345ull, RA = 1, RB = 0;
+            const unsigned long long M = 0x7fffffffull;
+            for (unsigned long long e = steps; e; e >>= 1) {
+                if (e & 1) {
+                    RB = (A * RB + B) & M;
+                    RA = (A * RA) & M;
+                }
+                B = (A * B + B) & M;
+                A = (A * A) & M;
+            }
+            const unsigned long long s = (RA * 12345ull + RB) & M;
+            const double val = fixedDof(mask, c) ? 0.0 : double(s) / 2147483647.0 - 0.5;
+            v[3 * n + c] = val;
+            acc[0] += val * val;
+        }
+    }
+    double tot[1];
+    if (gridReduce<1>(acc, 0u, partials, ticket, tot) && threadIdx.x == 0) st->est = sqrt(tot[0]);
+}
+
+__global__ void k_scale(long long n, double* __restrict__ v, const SolveState* st) {
+    const double nv = st->est;
+    const double inv = nv > 0 ? 1.0 / nv : 1.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) v[i] *= inv;
+}
+
+__global__ void k_lz_x(long long n, const double* __restrict__ invD, const double* __restrict__ v, double* __restrict__ x) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) x[i] = sqrt(invD[i]) * v[i];
+}
+
+// w = sq w - b vp; alpha = w . v
+__global__ void k_lz_w(long long n, const double* __restrict__ invD, double* __restrict__ w, const double* __restrict__ v,
+                       const double* __restrict__ vp, double b, SolveState* st, double* partials, unsigned* ticket) {
+    double acc[1] = {0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double wv = sqrt(invD[i]) * w[i] - b * vp[i];
+        w[i] = wv;
+        acc[0] += wv * v[i];
+    }
+    double tot[1];
+    if (gridReduce<1>(acc, 0u, partials, ticket, tot) && threadIdx.x == 0) st->alpha = tot[0];
+}
+
+// w -= alpha v; beta^2 = w . w
+__global__ void k_lz_axpy(long long n, double* __restrict__ w, const double* __restrict__ v, SolveState* st, double* partials,
+                          unsigned* ticket) {
+    const double a = st->alpha;
+    double acc[1] = {0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double wv = w[i] - a * v[i];
+        w[i] = wv;
+        acc[0] += wv * wv;
+    }
+    double tot[1];
+    if (gridReduce<1>(acc, 0u, partials, ticket, tot) && threadIdx.x == 0) st->beta = tot[0];
+}
+
+__global__ void k_lz_next(long long n, const double* __restrict__ w, double* __restrict__ v, double* __restrict__ vp, double b) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        vp[i] = v[i];
+        v[i] = w[i] / b;
+    }
+}
+
+// ---- post-processing: nodal stresses (voxel_fea.cpp:968-1037) and reactions (:929-940)
+
+struct StressCoefs {
+    double S[8][144];  // corner stress matrices times E / h, [a][row * 24 + q]
+};
+
+__device__ void principals3(double sx, double sy, double sz, double txy, double tyz, double tzx, double out[3]) {
+    // eigenvalues of the symmetric stress tensor by the trigonometric solution of its cubic
+    const double p1 = txy * txy + tyz * tyz + tzx * tzx;
+    const double q = (sx + sy + sz) / 3;
+    const double sc = fabs(sx) + fabs(sy) + fabs(sz) + sqrt(p1);
+    if (p1 <= 1e-24 * sc * sc) {
+        double a = sx, b = sy, c = sz, t;
+        if (a < b) { t = a; a = b; b = t; }
+        if (b < c) { t = b; b = c; c = t; }
+        if (a < b) { t = a; a = b; b = t; }
+        out[0] = a; out[1] = b; out[2] = c;
+        return;
+    }
+    const double p2 = (sx - q) * (sx - q) + (sy - q) * (sy - q) + (sz - q) * (sz - q) + 2 * p1;
+    const double p = sqrt(p2 / 6);
+    const double b11 = (sx - q) / p, b22 = (sy - q) / p, b33 = (sz - q) / p, b12 = txy / p, b23 = tyz / p, b13 = tzx / p;
+    const double det = b11 * (b22 * b33 - b23 * b23) - b12 * (b12 * b33 - b23 * b13) + b13 * (b12 * b23 - b22 * b13);
+    const double rr = fmin(1.0, fmax(-1.0, det / 2));
+    const double phi = acos(rr) / 3;
+    out[0] = q + 2 * p * cos(phi);
+    out[2] = q + 2 * p * cos(phi + 2.0943951023931954923);
+    out[1] = 3 * q - out[0] - out[2];
+}
+
+__global__ void __launch_bounds__(NODE_THREADS) k_stresses(LevelView L, StressCoefs SC, const double* __restrict__ u, int principals,
+                                                           float* __restrict__ vm, float* __restrict__ p1, float* __restrict__ p3) {
+    const long long NX = L.NX, NXY = (long long)L.NX * L.NY;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < L.nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = L.nmask[n];
+        float ovm = 0, op1 = 0, op3 = 0;
+        if (mask & NM_ACTIVE) {
+            int i, j, k;
+            nodeCoords(L, n, i, j, k);
+            double svm = 0, sp1 = 0, sp3 = 0, wsum = 0;
+#pragma unroll
+            for (int v = 0; v < 8; v++) {
+                const int di = v & 1, dj = (v >> 1) & 1, dk = v >> 2;
+                const int ei = i - 1 + di, ej = j - 1 + dj, ek = k - 1 + dk;
+                if (ei < 0 || ej < 0 || ek < 0 || ei >= L.nx || ej >= L.ny || ek >= L.nz) continue;
+                const uint32_t w = L.word[ei + (long long)L.nx * (ej + (long long)L.ny * ek)];
+                if (w == 0) continue;
+                const int a = cornerOf(1 - di, 1 - dj, 1 - dk);
+                double sig[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+                for (int b = 0; b < 8; b++) {
+                    const int bx = (b == 1 || b == 2 || b == 5 || b == 6), by = (b == 2 || b == 3 || b == 6 || b == 7), bz = b >> 2;
+                    const double* xp = u + 3 * (n + (di + bx - 1) + (dj + by - 1) * NX + (dk + bz - 1) * NXY);
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        const double xv = xp[c];
+#pragma unroll
+                        for (int rr = 0; rr < 6; rr++) sig[rr] += SC.S[a][rr * 24 + 3 * b + c] * xv;
+                    }
+                }
+                const double rho = double(__uint_as_float(w));
+                svm += rho * sqrt(0.5 * ((sig[0] - sig[1]) * (sig[0] - sig[1]) + (sig[1] - sig[2]) * (sig[1] - sig[2]) +
+                                         (sig[2] - sig[0]) * (sig[2] - sig[0])) +
+                                  3 * (sig[3] * sig[3] + sig[4] * sig[4] + sig[5] * sig[5]));
+                if (principals) {
+                    double pr[3];
+                    principals3(sig[0], sig[1], sig[2], sig[3], sig[4], sig[5], pr);
+                    sp1 += rho * pr[0];
+                    sp3 += rho * pr[2];
+                }
+                wsum += rho;
+            }
+            if (wsum > 0) {
+                ovm = float(svm / wsum);
+                op1 = float(sp1 / wsum);
+                op3 = float(sp3 / wsum);
+            }
+        }
+        vm[n] = ovm;
+        if (principals) {
+            p1[n] = op1;
+            p3[n] = op3;
+        }
+    }
+}
+
+__global__ void k_reactions(long long nNodes, const uint8_t* __restrict__ nmask, const uint8_t* __restrict__ bc, const double* __restrict__ y,
+                            const double* __restrict__ f, SolveState* st, double* partials, unsigned* ticket) {
+    double v[3] = {0, 0, 0};
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        if (!(nmask[n] & NM_ACTIVE)) continue;
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            if (bc[3 * n + c]) v[c] += y[3 * n + c] - (f ? f[3 * n + c] : 0.0);
+    }
+    double tot[3];
+    if (gridReduce<3>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) {
+        st->alpha = tot[0];
+        st->beta = tot[1];
+        st->pq = tot[2];
+    }
+}
+
+}  // namespace dev
+
+// ==================================================================== host side
+
+namespace {
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        if (e == cudaErrorMemoryAllocation) throw Error(PS_EOOM, std::string(what) + ": " + cudaGetErrorString(e));
+        if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) throw Error(PS_ENODEV, std::string(what) + ": " + cudaGetErrorString(e));
+        throw Error(PS_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+struct DevMem {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevMem() = default;
+    DevMem(const DevMem&) = delete;
+    DevMem& operator=(const DevMem&) = delete;
+    DevMem(DevMem&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevMem& operator=(DevMem&& o) noexcept {
+        if (this != &o) { release(); p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0; }
+        return *this;
+    }
+    ~DevMem() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    void alloc(size_t n, int64_t& total) {
+        release();
+        if (n == 0) return;
+        check(cudaMalloc(&p, n), "cudaMalloc");
+        check(cudaMemset(p, 0, n), "cudaMemset");
+        bytes = n;
+        total += int64_t(n);
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+template <class T>
+void upload(DevMem& m, const std::vector<T>& v, int64_t& total) {
+    m.alloc(v.size() * sizeof(T), total);
+    if (!v.empty()) check(cudaMemcpy(m.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+}
+
+int gridFor(int64_t n, int threads, int cap) {
+    const int64_t b = (n + threads - 1) / threads;
+    return int(std::max<int64_t>(1, std::min<int64_t>(b, cap)));
+}
+
+}  // namespace
+
+struct DevLevel {
+    dev::LevelView view{};
+    dev::Coefs<double> c64{};
+    dev::Coefs<float> c32{};
+    DevMem word, nmask, own, own16, invD, invD64, dadd, dadd32, bc;
+    DevMem r, z, t, d;
+    float cf0 = 0, cf1 = 0, cf2 = 0, omega = 0.5f;
+    bool hasOwn = false;
+};
+
+struct SolverImpl {
+    Hierarchy H;
+    std::vector<DevLevel> L;
+    int64_t bytes = 0;
+    int smCount = 148;
+    // coarsest
+    DevMem cDof, cInv;
+    int m = 0;
+    // finest-level FP64 work vectors and FP32 mixed-precision ones
+    DevMem f, x, r, p, q, z64, x32, p32, q32, tmp;
+    // control
+    DevMem state, partials, ticket;
+    dev::SolveState* hostState = nullptr;  // pinned mirror
+    cudaStream_t stream = nullptr;      // the stream every kernel goes to (own, or the caller's)
+    cudaStream_t ownStream = nullptr;
+    bool smoothersReady = false;
+    int64_t launches = 0;     // kernels launched by this handle (graph replays add their kernel count)
+    int64_t graphKernels[2] = {0, 0};
+
+    template <class... KArgs, class... Args>
+    void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+        kernel<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+        ++launches;
+    }
+    // graphs of one iteration, per precision
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+
+    int nodeGrid(int64_t nNodes) const { return gridFor(nNodes, dev::NODE_THREADS, smCount * 16); }
+    int vecGrid(int64_t n) const { return gridFor(n, dev::VEC_THREADS, smCount * 8); }
+    dev::SolveState* st() const { return state.as<dev::SolveState>(); }
+    double* part() const { return partials.as<double>(); }
+    unsigned* tick() const { return ticket.as<unsigned>(); }
+
+    void build(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsest, const double* diagAdd);
+    void uploadLevel(int l);
+    void prepareSmoothers();
+    double lanczos(int l);
+
+    // operator launches
+    void op64(int l, const double* x, double* y, bool raw, dev::Ctl ctl);
+    template <int MODE>
+    void op32(int l, const float* x, float* y, float c1, float c2, dev::Ctl ctl, bool own16 = false);
+    // V-cycle on level l from L[l].r; returns the buffer holding the result
+    float* vcycle(int l, dev::Ctl ctl, bool own16);
+    bool exactOneLevel() const { return L.size() == 1 && H.hasFactor(); }
+
+    void recordPlainIteration(dev::Ctl ctl);
+    void recordMixedIteration(dev::Ctl ctl);
+    ps_status runSolve(const double* fDev, const double* x0Dev, const ps_solve_opts& o, double* uDev, ps_solve_result& res);
+    void readState() {
+        check(cudaMemcpyAsync(hostState, state.p, sizeof(dev::SolveState), cudaMemcpyDeviceToHost, stream), "state read");
+        check(cudaStreamSynchronize(stream), "sync");
+    }
+
+    ~SolverImpl() {
+        for (auto& g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        if (hostState) cudaFreeHost(hostState);
+        if (ownStream) cudaStreamDestroy(ownStream);
+    }
+};
+
+void SolverImpl::build(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsest, const double* diagAdd) {
+    H = buildHierarchy(dims, density, nu, bc, coarsest, diagAdd);
+    int devId = 0;
+    check(cudaGetDevice(&devId), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, devId), "attribute");
+    check(cudaStreamCreateWithFlags(&ownStream, cudaStreamNonBlocking), "stream");
+    stream = ownStream;
+    check(cudaMallocHost(&hostState, sizeof(dev::SolveState)), "cudaMallocHost");
+    L.resize(H.levels.size());
+    for (int l = 0; l < int(H.levels.size()); l++) uploadLevel(l);
+    const HostLevel& L0 = H.levels[0];
+    const size_t n = size_t(L0.nDof);
+    f.alloc(n * 8, bytes);
+    x.alloc(n * 8, bytes);
+    r.alloc(n * 8, bytes);
+    p.alloc(n * 8, bytes);
+    q.alloc(n * 8, bytes);
+    if (exactOneLevel()) z64.alloc(n * 8, bytes);
+    x32.alloc(n * 4, bytes);
+    p32.alloc(n * 4, bytes);
+    q32.alloc(n * 4, bytes);
+    m = int(H.coarseM);
+    if (H.hasFactor()) {
+        upload(cDof, H.coarseDof, bytes);
+        upload(cInv, H.coarseInv, bytes);
+    }
+    state.alloc(sizeof(dev::SolveState), bytes);
+    partials.alloc(size_t(smCount) * 16 * 4 * sizeof(double) + 4096, bytes);
+    ticket.alloc(64, bytes);
+}
+
+void SolverImpl::uploadLevel(int l) {
+    const HostLevel& h = H.levels[size_t(l)];
+    DevLevel& D = L[size_t(l)];
+    upload(D.word, h.word, bytes);
+    upload(D.nmask, h.nmask, bytes);
+    D.hasOwn = h.nOwn > 0;
+    if (D.hasOwn) {
+        upload(D.own, h.own, bytes);
+        // halves with a power-of-two level scale keeping the largest entry near 2^14
+        double kmax = 0;
+        for (float v : h.own) kmax = std::max(kmax, double(std::fabs(v)));
+        const float hs = kmax > 0 ? float(std::exp2(std::ceil(std::log2(kmax / 16384.0)))) : 1.f;
+        std::vector<__half> h16(h.own.size());
+        const float inv = 1.f / hs;
+        parallelFor(int64_t(h.own.size()), [&](int64_t lo, int64_t hi) {
+            for (int64_t i = lo; i < hi; i++) h16[size_t(i)] = __float2half_rn(h.own[size_t(i)] * inv);
+        });
+        upload(D.own16, h16, bytes);
+        D.view.hs = hs;
+    }
+    std::vector<float> invD(h.invDiag.begin(), h.invDiag.end());
+    upload(D.invD, invD, bytes);
+    if (!h.diagAdd.empty()) {
+        upload(D.dadd, h.diagAdd, bytes);
+        std::vector<float> d32(h.diagAdd.begin(), h.diagAdd.end());
+        upload(D.dadd32, d32, bytes);
+    }
+    if (l == 0) upload(D.bc, h.bc, bytes);
+    const size_t n = size_t(h.nDof);
+    D.r.alloc(n * 4, bytes);
+    D.z.alloc(n * 4, bytes);
+    D.t.alloc(n * 4, bytes);
+    D.d.alloc(n * 4, bytes);
+    dev::LevelView& v = D.view;
+    v.nx = h.nx; v.ny = h.ny; v.nz = h.nz; v.NX = h.NX; v.NY = h.NY; v.NZ = h.NZ;
+    v.nNodes = h.nNodes;
+    v.word = D.word.as<uint32_t>();
+    v.nmask = D.nmask.as<uint8_t>();
+    v.own = D.own.as<float>();
+    v.own16 = D.own16.as<__half>();
+    v.dadd = D.dadd.as<double>();
+    v.dadd32 = D.dadd32.as<float>();
+    v.invD = D.invD.as<float>();
+    for (int i = 0; i < 576; i++) {
+        D.c64.Kb[i] = h.Kb[i];
+        D.c32.Kb[i] = float(h.Kb[i]);
+    }
+    for (int m = 0; m < 27; m++)
+        for (int e = 0; e < 9; e++) {
+            D.c64.S[m * 9 + e] = h.S[m][e];
+            D.c32.S[m * 9 + e] = float(h.S[m][e]);
+        }
+}
+
+void SolverImpl::op64(int l, const double* xin, double* y, bool raw, dev::Ctl ctl) {
+    DevLevel& D = L[size_t(l)];
+    launch(dev::k_op<double, dev::OP_APPLY, false>, nodeGrid(D.view.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c64, xin, y, nullptr, nullptr, 0.f,
+                                                                                                         0.f, raw ? 1 : 0, ctl);
+}
+
+template <int MODE>
+void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev::Ctl ctl, bool own16) {
+    DevLevel& D = L[size_t(l)];
+    const int g = nodeGrid(D.view.nNodes);
+    if (own16 && D.hasOwn)
+        launch(dev::k_op<float, MODE, true>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, D.r.as<float>(), D.d.as<float>(), c1, c2, 0, ctl);
+    else
+        launch(dev::k_op<float, MODE, false>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, D.r.as<float>(), D.d.as<float>(), c1, c2, 0, ctl);
+}
+
+// pre-smoothing from zero, residual, restriction, coarse correction, prolongation, post-smoothing
+// (voxel_fea.cpp:817-828); buffers alternate between the level's z and t
+float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16) {
+    DevLevel& D = L[size_t(l)];
+    const HostLevel& h = H.levels[size_t(l)];
+    float *z = D.z.as<float>(), *t = D.t.as<float>(), *r = D.r.as<float>(), *d = D.d.as<float>();
+    if (l == int(L.size()) - 1) {
+        if (H.hasFactor()) {
+            const int threads = 256, warps = threads / 32;
+            const int grid = std::max(1, std::min(smCount * 2, (m + warps - 1) / warps));
+            launch(dev::k_coarse<float, float>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(), r, z, ctl);
+            return z;
+        }
+        // no factor: 40 damped Jacobi sweeps with the default weight (voxel_fea.cpp:676-678)
+        launch(dev::k_cheb_first, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, r, D.invD.as<float>(), d, z, D.omega, ctl);
+        float* a = z;
+        float* b = t;
+        for (int s = 1; s < 40; s++) {
+            op32<dev::OP_CHEB>(l, a, b, 0.f, D.omega, ctl, own16);
+            std::swap(a, b);
+        }
+        return a;
+    }
+    DevLevel& C = L[size_t(l + 1)];
+    const HostLevel& hc = H.levels[size_t(l + 1)];
+    launch(dev::k_cheb_first, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, r, D.invD.as<float>(), d, z, D.cf0, ctl);
+    op32<dev::OP_CHEB>(l, z, t, D.cf1, D.cf2, ctl, own16);    // t = smoothed
+    op32<dev::OP_RESID>(l, t, z, 0.f, 0.f, ctl, own16);       // z = r - K t
+    launch(dev::k_restrict, gridFor(hc.nNodes, 256, smCount * 16), 256, 0, stream, h.NX, h.NY, h.NZ, C.view, z, C.r.as<float>(), ctl);
+    float* zc = vcycle(l + 1, ctl, own16);
+    launch(dev::k_prolong, gridFor(h.nNodes, 256, smCount * 16), 256, 0, stream, D.view, hc.NX, hc.NY, zc, t, ctl);
+    op32<dev::OP_CHEB>(l, t, z, 0.f, D.cf0, ctl, own16);      // d = c0 D^-1 (r - K t); z = t + d
+    op32<dev::OP_CHEB>(l, z, t, D.cf1, D.cf2, ctl, own16);    // second step
+    return t;
+}
+
+double SolverImpl::lanczos(int l) {
+    DevLevel& D = L[size_t(l)];
+    const HostLevel& h = H.levels[size_t(l)];
+    const int64_t n = h.nDof;
+    int64_t scratch = 0;
+    DevMem v, vp, w, xx, invD;
+    v.alloc(size_t(n) * 8, scratch);
+    vp.alloc(size_t(n) * 8, scratch);
+    w.alloc(size_t(n) * 8, scratch);
+    xx.alloc(size_t(n) * 8, scratch);
+    upload(invD, h.invDiag, scratch);
+    const int vg = vecGrid(n);
+    launch(dev::k_lz_start, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, h.nNodes, D.view.nmask, v.as<double>(), part(), tick(), st());
+    launch(dev::k_scale, vg, dev::VEC_THREADS, 0, stream, n, v.as<double>(), st());
+    std::vector<double> alpha, beta;
+    double b = 0;
+    const dev::Ctl none{nullptr, nullptr};
+    for (int s = 0; s < 10; s++) {
+        launch(dev::k_lz_x, vg, dev::VEC_THREADS, 0, stream, n, invD.as<double>(), v.as<double>(), xx.as<double>());
+        op64(l, xx.as<double>(), w.as<double>(), false, none);
+        launch(dev::k_lz_w, vg, dev::VEC_THREADS, 0, stream, n, invD.as<double>(), w.as<double>(), v.as<double>(), vp.as<double>(), b, st(), part(),
+                                                          tick());
+        launch(dev::k_lz_axpy, vg, dev::VEC_THREADS, 0, stream, n, w.as<double>(), v.as<double>(), st(), part(), tick());
+        readState();
+        const double a = hostState->alpha;
+        alpha.push_back(a);
+        b = std::sqrt(hostState->beta);
+        if (!(b > 1e-12 * std::fabs(a))) break;
+        beta.push_back(b);
+        launch(dev::k_lz_next, vg, dev::VEC_THREADS, 0, stream, n, w.as<double>(), v.as<double>(), vp.as<double>(), b);
+    }
+    beta.resize(alpha.size() - 1);
+    check(cudaGetLastError(), "lanczos");
+    return tridiagonalMax(alpha, beta);
+}
+
+void SolverImpl::prepareSmoothers() {
+    if (smoothersReady) return;
+    for (int l = 0; l + 1 < int(L.size()); l++) {
+        HostLevel& h = H.levels[size_t(l)];
+        if (!(h.lmax > 0)) h.lmax = lanczos(l);
+        double c0, c1, c2;
+        chebyshevCoefficients(h.lmax, c0, c1, c2);
+        L[size_t(l)].cf0 = float(c0);
+        L[size_t(l)].cf1 = float(c1);
+        L[size_t(l)].cf2 = float(c2);
+        L[size_t(l)].omega = float(1.2 / (h.lmax * 1.05));
+    }
+    // the coarsest level keeps the default Jacobi weight 0.5 (its eigenvalue is never estimated)
+    smoothersReady = true;
+}
+
+// one FP64 CG iteration (voxel_fea.cpp:901-919)
+void SolverImpl::recordPlainIteration(dev::Ctl ctl) {
+    const HostLevel& h = H.levels[0];
+    DevLevel& D = L[0];
+    launch(dev::k_apply_alpha<double, false>, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c64, p.as<double>(), q.as<double>(), st(),
+                                                                                            part(), tick(), ctl);
+    launch(dev::k_cg_update, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x.as<double>(), r.as<double>(), p.as<double>(),
+                                                                         q.as<double>(), st(), part(), tick(), ctl);
+    float* z32 = nullptr;
+    if (exactOneLevel()) {
+        const int threads = 256, warps = threads / 32;
+        const int grid = std::max(1, std::min(smCount * 2, (m + warps - 1) / warps));
+        launch(dev::k_coarse<double, double>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(), r.as<double>(),
+                                                                                           z64.as<double>(), ctl);
+    } else {
+        launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), D.r.as<float>(), st(), ctl);
+        z32 = vcycle(0, ctl, false);
+    }
+    launch(dev::k_cg_dots, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, r.as<double>(), z32, z64.as<double>(), q.as<double>(), st(), part(),
+                                                                     tick(), ctl);
+    launch(dev::k_cg_p, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, z32, z64.as<double>(), p.as<double>(), st(), ctl);
+}
+
+// one FP32 CG iteration with the FP64 fold (runs only when due)
+void SolverImpl::recordMixedIteration(dev::Ctl ctl) {
+    const HostLevel& h = H.levels[0];
+    DevLevel& D = L[0];
+    const int* foldFlag = &st()->fold;
+    launch(dev::k_apply_alpha<float, true>, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c32, p32.as<float>(), q32.as<float>(), st(),
+                                                                                          part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
+    launch(dev::k_mx_update, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x32.as<float>(), D.r.as<float>(), p32.as<float>(),
+                                                                         q32.as<float>(), st(), part(), tick(), ctl);
+    const dev::Ctl foldCtl{ctl.skipIf, foldFlag};
+    launch(dev::k_mx_fold1, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, x.as<double>(), x32.as<float>(), st(), foldCtl);
+    op64(0, x.as<double>(), q.as<double>(), false, foldCtl);
+    launch(dev::k_mx_fold2, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), D.r.as<float>(),
+                                                                        st(), part(), tick(), foldCtl);
+    float* z32 = vcycle(0, ctl, true);
+    launch(dev::k_mx_dots, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, D.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
+    launch(dev::k_mx_p, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, z32, p32.as<float>(), st(), ctl);
+}
+
+ps_status SolverImpl::runSolve(const double* fDev, const double* x0Dev, const ps_solve_opts& o, double* uDev, ps_solve_result& res) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const int64_t launches0 = launches;
+    const HostLevel& h = H.levels[0];
+    DevLevel& D = L[0];
+    const bool mixed = o.precision == PS_PREC_MIXED && !exactOneLevel();
+    const int64_t n = h.nDof;
+    prepareSmoothers();
+    // state
+    dev::SolveState s{};
+    s.tol = o.tol;
+    s.maxIter = o.max_iter;
+    s.first = 1;
+    s.mixed = mixed ? 1 : 0;
+    check(cudaMemcpyAsync(state.p, &s, sizeof s, cudaMemcpyHostToDevice, stream), "state");
+    if (fDev != f.p) check(cudaMemcpyAsync(f.p, fDev, size_t(n) * 8, cudaMemcpyDeviceToDevice, stream), "f copy");
+    launch(dev::k_mask_copy, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x0Dev, x.as<double>());
+    const dev::Ctl none{nullptr, nullptr};
+    const dev::Ctl ctl{&st()->done, nullptr};
+    op64(0, x.as<double>(), q.as<double>(), false, none);
+    launch(dev::k_cg_init, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), r.as<double>(),
+                                                                       nullptr, st(), part(), tick());
+    // first preconditioned direction
+    if (mixed) {
+        check(cudaMemsetAsync(x32.p, 0, size_t(n) * 4, stream), "memset");
+        launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), D.r.as<float>(), st(), ctl);
+        float* z32 = vcycle(0, ctl, true);
+        launch(dev::k_mx_dots, vecGrid(n), dev::VEC_THREADS, 0, stream, n, D.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
+        launch(dev::k_mx_p, vecGrid(n), dev::VEC_THREADS, 0, stream, n, z32, p32.as<float>(), st(), ctl);
+    } else {
+        float* z32 = nullptr;
+        if (exactOneLevel()) {
+            const int threads = 256, warps = threads / 32;
+            const int grid = std::max(1, std::min(smCount * 2, (m + warps - 1) / warps));
+            check(cudaMemsetAsync(z64.p, 0, size_t(n) * 8, stream), "memset");
+            launch(dev::k_coarse<double, double>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(),
+                                                                                               r.as<double>(), z64.as<double>(), ctl);
+        } else {
+            launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), D.r.as<float>(), st(), ctl);
+            z32 = vcycle(0, ctl, false);
+        }
+        launch(dev::k_cg_dots, vecGrid(n), dev::VEC_THREADS, 0, stream, n, r.as<double>(), z32, z64.as<double>(), q.as<double>(), st(), part(), tick(),
+                                                                    ctl);
+        launch(dev::k_cg_p, vecGrid(n), dev::VEC_THREADS, 0, stream, n, z32, z64.as<double>(), p.as<double>(), st(), ctl);
+    }
+    launch(dev::k_clear_first, 1, 1, 0, stream, st());
+    check(cudaGetLastError(), "solve setup");
+    // the iteration graph (recorded once per precision)
+    cudaGraphExec_t& g = graph[mixed ? 1 : 0];
+    if (!g) {
+        cudaGraph_t gr;
+        check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
+        if (mixed) recordMixedIteration(ctl);
+        else recordPlainIteration(ctl);
+        check(cudaStreamEndCapture(stream, &gr), "capture end");
+        size_t nodes = 0;
+        check(cudaGraphGetNodes(gr, nullptr, &nodes), "graph nodes");
+        graphKernels[mixed ? 1 : 0] = int64_t(nodes);
+        launches -= int64_t(nodes);  // captured, not run
+        check(cudaGraphInstantiate(&g, gr, 0), "instantiate");
+        cudaGraphDestroy(gr);
+    }
+    // batches of iterations, sized from the observed convergence rate
+    int batch = 2;
+    double lastRel = 0;
+    int lastIt = 0;
+    ps_status outcome = PS_OK;
+    for (;;) {
+        readState();
+        const dev::SolveState& hs = *hostState;
+        if (hs.done) break;
+        if (o.cancel && *o.cancel) { outcome = PS_CANCELLED; break; }
+        if (o.time_limit_s > 0 && std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o.time_limit_s) {
+            outcome = PS_TIMEOUT;
+            break;
+        }
+        const double rel = mixed ? std::max(hs.est, 0.0) : hs.rel;
+        if (lastIt > 0 && hs.it > lastIt && rel > 0 && lastRel > 0) {
+            const double rate = std::pow(rel / lastRel, 1.0 / (hs.it - lastIt));
+            int need = 32;
+            if (rate < 0.999) need = int(std::ceil(std::log(o.tol / rel) / std::log(rate)));
+            batch = std::max(1, std::min({need, 32, 2 * batch}));
+        }
+        lastRel = rel;
+        lastIt = hs.it;
+        batch = std::max(1, std::min(batch, o.max_iter - hs.it + 1));
+        for (int b = 0; b < batch; b++) check(cudaGraphLaunch(g, stream), "graph launch");
+        launches += int64_t(batch) * graphKernels[mixed ? 1 : 0];
+    }
+    // the result
+    if (!mixed) {
+        if (hostState->done == 2) check(cudaMemsetAsync(x.p, 0, size_t(n) * 8, stream), "memset");
+        op64(0, x.as<double>(), q.as<double>(), false, none);
+        launch(dev::k_final, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), st(), part(),
+                                                                         tick());
+    } else {
+        if (hostState->done == 2) check(cudaMemsetAsync(x.p, 0, size_t(n) * 8, stream), "memset");
+        if (outcome == PS_CANCELLED || outcome == PS_TIMEOUT) {
+            // fold what the FP32 iterate holds and report the true residual
+            launch(dev::k_mx_fold1, vecGrid(n), dev::VEC_THREADS, 0, stream, n, x.as<double>(), x32.as<float>(), st(), none);
+            op64(0, x.as<double>(), q.as<double>(), false, none);
+            launch(dev::k_final, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), st(), part(),
+                                                                             tick());
+        }
+    }
+    if (uDev != x.p) check(cudaMemcpyAsync(uDev, x.p, size_t(n) * 8, cudaMemcpyDeviceToDevice, stream), "u copy");
+    readState();
+    check(cudaGetLastError(), "solve");
+    const dev::SolveState& hs = *hostState;
+    res.iterations = hs.it;
+    res.residual = hs.rel;
+    res.folds = hs.folds;
+    res.converged = (outcome == PS_OK) && std::isfinite(hs.rel) && hs.rel <= o.tol * 10;
+    if (outcome == PS_OK) {
+        if (hs.status == dev::ST_BREAKDOWN && !res.converged) outcome = PS_BREAKDOWN;
+        else if (!res.converged) outcome = PS_NOT_CONVERGED;
+    }
+    res.status = outcome;
+    res.kernels = launches - launches0;
+    res.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return outcome;
+}
+
+// ==================================================================== Solver
+
+Solver::Solver(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsestMaxDof, const double* diagAdd)
+    : impl_(new SolverImpl) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        throw Error(PS_ENODEV, "no CUDA device is available");
+    }
+    impl_->build(dims, density, nu, bc, coarsestMaxDof, diagAdd);
+}
+
+Solver::~Solver() = default;
+
+const Hierarchy& Solver::hierarchy() const { return impl_->H; }
+int64_t Solver::nDof() const { return impl_->H.levels[0].nDof; }
+int64_t Solver::deviceBytes() const { return impl_->bytes; }
+double Solver::levelLmax(int l) const { return impl_->H.levels[size_t(l)].lmax; }
+
+static void validateF(const double* f, const double* x0, int64_t n) {
+    for (int64_t i = 0; i < n; i++)
+        if (!std::isfinite(f[i]) || (x0 && !std::isfinite(x0[i]))) throw Error(PS_ENONFINITE, "Forces and displacements must be finite numbers.");
+}
+
+ps_status Solver::solve(const double* f, const ps_solve_opts& o, double* u, ps_solve_result& res) {
+    SolverImpl& I = *impl_;
+    const int64_t n = nDof();
+    validateF(f, o.x0, n);
+    const auto t0 = std::chrono::steady_clock::now();
+    check(cudaMemcpyAsync(I.f.p, f, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "f upload");
+    const double* x0 = nullptr;
+    if (o.x0) {
+        check(cudaMemcpyAsync(I.p.p, o.x0, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "x0 upload");
+        x0 = I.p.as<double>();
+    }
+    const ps_status s = I.runSolve(I.f.as<double>(), x0, o, I.x.as<double>(), res);
+    check(cudaMemcpyAsync(u, I.x.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "u download");
+    check(cudaStreamSynchronize(I.stream), "sync");
+    res.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return s;
+}
+
+ps_status Solver::solveDevice(const double* fDev, const ps_solve_opts& o, double* uDev, ps_solve_result& res) {
+    SolverImpl& I = *impl_;
+    const double* x0 = o.x0;
+    if (x0) {
+        check(cudaMemcpyAsync(I.p.p, x0, size_t(nDof()) * 8, cudaMemcpyDeviceToDevice, I.stream), "x0 copy");
+        x0 = I.p.as<double>();
+    }
+    const ps_status s = I.runSolve(fDev, x0, o, uDev, res);
+    check(cudaStreamSynchronize(I.stream), "sync");
+    return s;
+}
+
+void Solver::precondition(const double* rHost, double* zHost) {
+    SolverImpl& I = *impl_;
+    const HostLevel& h = I.H.levels[0];
+    DevLevel& D = I.L[0];
+    const int64_t n = h.nDof;
+    I.prepareSmoothers();
+    check(cudaMemcpyAsync(I.r.p, rHost, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "r upload");
+    const dev::Ctl none{nullptr, nullptr};
+    if (I.exactOneLevel()) {
+        // the whole model is the coarsest level: its direct FP64 solve (voxel_fea.cpp:838-842)
+        const int threads = 256, warps = threads / 32;
+        const int grid = std::max(1, std::min(I.smCount * 2, (I.m + warps - 1) / warps));
+        check(cudaMemsetAsync(I.z64.p, 0, size_t(n) * 8, I.stream), "memset");
+        I.launch(dev::k_coarse<double, double>, grid, threads, size_t(I.m) * sizeof(double), I.stream, I.m, I.cDof.as<int>(), I.cInv.as<double>(),
+                                                                                               I.r.as<double>(), I.z64.as<double>(), none);
+        check(cudaMemcpyAsync(zHost, I.z64.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "z download");
+    } else {
+        I.launch(dev::k_rmax, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, I.r.as<double>(), I.st(), I.part(), I.tick());
+        I.launch(dev::k_vc_load, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, I.r.as<double>(), D.r.as<float>(), I.st(),
+                                                                               none);
+        float* z32 = I.vcycle(0, none, false);
+        I.launch(dev::k_vc_store, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, z32, I.q.as<double>(), I.st());
+        check(cudaMemcpyAsync(zHost, I.q.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "z download");
+    }
+    check(cudaStreamSynchronize(I.stream), "precondition");
+}
+
+void Solver::setStream(void* s) {
+    SolverImpl& I = *impl_;
+    cudaStream_t want = s ? static_cast<cudaStream_t>(s) : I.ownStream;
+    if (want != I.stream) {
+        // graphs were captured from the old stream's work; replays may go to any stream, so keep them
+        check(cudaStreamSynchronize(I.stream), "sync");
+        I.stream = want;
+    }
+}
+
+double Solver::timeKernel(int which, int reps) {
+    SolverImpl& I = *impl_;
+    I.prepareSmoothers();
+    const dev::Ctl none{nullptr, nullptr};
+    DevLevel& D = I.L[0];
+    cudaEvent_t e0, e1;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    auto once = [&] {
+        if (which == 0) I.op32<dev::OP_CHEB>(0, D.z.as<float>(), D.t.as<float>(), D.cf1, D.cf2, none, true);
+        else I.op64(0, I.p.as<double>(), I.q.as<double>(), false, none);
+    };
+    once();
+    check(cudaEventRecord(e0, I.stream), "event");
+    for (int k = 0; k < reps; k++) once();
+    check(cudaEventRecord(e1, I.stream), "event");
+    check(cudaEventSynchronize(e1), "event");
+    float ms = 0;
+    check(cudaEventElapsedTime(&ms, e0, e1), "event");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return double(ms) / reps;
+}
+
+int64_t Solver::launches() const { return impl_->launches; }
+
+void Solver::apply(int level, const double* xHost, double* yHost, bool raw) {
+    SolverImpl& I = *impl_;
+    if (level < 0 || level >= int(I.L.size())) throw Error(PS_EINVAL, "level out of range");
+    const int64_t n = I.H.levels[size_t(level)].nDof;
+    check(cudaMemcpyAsync(I.p.p, xHost, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "x upload");
+    I.op64(level, I.p.as<double>(), I.q.as<double>(), raw, dev::Ctl{nullptr, nullptr});
+    check(cudaMemcpyAsync(yHost, I.q.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "y download");
+    check(cudaStreamSynchronize(I.stream), "apply");
+}
+
+void Solver::stresses(const double* u, double E, double h, bool principals, float* vm, float* p1, float* p3) {
+    SolverImpl& I = *impl_;
+    const HostLevel& L0 = I.H.levels[0];
+    const int64_t nn = L0.nNodes;
+    dev::StressCoefs sc;
+    for (int a = 0; a < 8; a++)
+        for (int i = 0; i < 144; i++) sc.S[a][i] = I.H.el.cornerStress[a][i] * E / h;
+    int64_t scratch = 0;
+    DevMem out;
+    out.alloc(size_t(nn) * 4 * 3, scratch);
+    check(cudaMemcpyAsync(I.p.p, u, size_t(L0.nDof) * 8, cudaMemcpyHostToDevice, I.stream), "u upload");
+    float* o = out.as<float>();
+    I.launch(dev::k_stresses, I.nodeGrid(nn), dev::NODE_THREADS, 0, I.stream, I.L[0].view, sc, I.p.as<double>(), principals ? 1 : 0, o, o + nn, o + 2 * nn);
+    check(cudaMemcpyAsync(vm, o, size_t(nn) * 4, cudaMemcpyDeviceToHost, I.stream), "vm");
+    if (principals) {
+        check(cudaMemcpyAsync(p1, o + nn, size_t(nn) * 4, cudaMemcpyDeviceToHost, I.stream), "p1");
+        check(cudaMemcpyAsync(p3, o + 2 * nn, size_t(nn) * 4, cudaMemcpyDeviceToHost, I.stream), "p3");
+    }
+    check(cudaStreamSynchronize(I.stream), "stresses");
+}
+
+void Solver::reactions(const double* u, const double* f, double R[3]) {
+    SolverImpl& I = *impl_;
+    const HostLevel& L0 = I.H.levels[0];
+    const int64_t n = L0.nDof;
+    check(cudaMemcpyAsync(I.p.p, u, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "u upload");
+    if (f) check(cudaMemcpyAsync(I.r.p, f, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "f upload");
+    I.op64(0, I.p.as<double>(), I.q.as<double>(), true, dev::Ctl{nullptr, nullptr});
+    I.launch(dev::k_reactions, I.vecGrid(L0.nNodes), dev::VEC_THREADS, 0, I.stream, L0.nNodes, I.L[0].view.nmask, I.L[0].bc.as<uint8_t>(), I.q.as<double>(),
+                                                                               f ? I.r.as<double>() : nullptr, I.st(), I.part(), I.tick());
+    I.readState();
+    R[0] = I.hostState->alpha;
+    R[1] = I.hostState->beta;
+    R[2] = I.hostState->pq;
+}
+
+}  // namespace psfea

@@ -1,0 +1,44 @@
+// Device-resident solver for one voxel model (plain C++ interface; CUDA stays inside solver.cu).
+#pragma once
+
+#include <cstdint>
+#include <memory>
+
+#include "hierarchy.hpp"
+#include "ps_fea.h"
+
+namespace psfea {
+
+struct SolverImpl;
+
+class Solver {
+public:
+    // builds the hierarchy on the host and uploads it; throws Error
+    Solver(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsestMaxDof, const double* diagAdd);
+    ~Solver();
+
+    const Hierarchy& hierarchy() const;
+    int64_t nDof() const;
+    int64_t deviceBytes() const;
+    double levelLmax(int l) const;
+
+    // host vectors in/out; returns the outcome status
+    ps_status solve(const double* f, const ps_solve_opts& o, double* u, ps_solve_result& res);
+    // device vectors in/out (o.x0 is a device pointer)
+    ps_status solveDevice(const double* fDev, const ps_solve_opts& o, double* uDev, ps_solve_result& res);
+    void precondition(const double* r, double* z);
+    void apply(int level, const double* x, double* y, bool raw);
+    void stresses(const double* u, double E, double h, bool principals, float* vm, float* p1, float* p3);
+    void reactions(const double* u, const double* f, double R[3]);
+    // route all work to the caller's CUDA stream (nullptr = the handle's own)
+    void setStream(void* stream);
+    // mean device time (ms, CUDA events) of the finest level's operator kernel: 0 = the FP32
+    // Chebyshev step of the V-cycle, 1 = the FP64 product of the CG
+    double timeKernel(int which, int reps);
+    int64_t launches() const;
+
+private:
+    std::unique_ptr<SolverImpl> impl_;
+};
+
+}  // namespace psfea

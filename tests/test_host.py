@@ -1,0 +1,102 @@
+"""CPU-side checks of the product library: it loads, exports every symbol include/ps_fea.h
+declares, and its host-side hierarchy build (no GPU) matches the reference's golden vectors."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import psfea
+from conftest import ROOT, golden
+from psfea import workloads as W
+
+MODELS = ["cantilever_32x8x8", "cantilever_64x16x16", "lbracket_32x16x16", "simp_16x8x8", "lbracket_24x12x12_loose"]
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "ps_fea.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ps_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = declared_symbols()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(psfea.lib, n), n
+    assert set(names) == set(psfea.EXPORTS)
+
+
+@pytest.mark.parametrize("nu", [0.3, 0.33, 0.34, 0.36])
+def test_element_matrix(nu):
+    g = golden("element")
+    K, cs = psfea.element_matrix(nu)
+    Kr = g[f"K_{nu}"]
+    assert np.abs(K - Kr).max() <= 1e-14 * np.abs(Kr).max()
+    assert np.array_equal(K, K.T)
+    if nu == 0.3:
+        assert np.abs(cs - g["cornerStress_0.3"]).max() <= 1e-14 * np.abs(cs).max()
+
+
+def test_invalid_inputs_raise_like_the_reference():
+    with pytest.raises(ValueError, match="Poisson"):
+        psfea.element_matrix(0.5)
+    bc = np.zeros(3 * 5 * 2 * 2, np.uint8)
+    with pytest.raises(ValueError, match="between zero and one"):
+        psfea.Hierarchy((4, 1, 1), np.array([1, 2, 0, 1], np.float32), 0.3, bc)
+    with pytest.raises(ValueError, match="do not match"):
+        psfea.Hierarchy((4, 1, 1), np.ones(3, np.float32), 0.3, bc)
+    with pytest.raises(ValueError, match="three positive"):
+        psfea.Hierarchy((0, 1, 1), np.ones(0, np.float32), 0.3, np.zeros(12, np.uint8))
+
+
+def test_prune_matches_reference():
+    g = golden("prune")
+    o1, r1 = psfea.prune_floating((4, 1, 1), g["d1"], g["h1"])
+    assert np.array_equal(o1, g["o1"]) and r1 == 1
+    o2, r2 = psfea.prune_floating(tuple(g["dims2"]), g["d2"], g["h2"])
+    assert np.array_equal(o2, g["o2"]) and r2 == int(g["r2"])
+
+
+@pytest.mark.parametrize("name", MODELS)
+def test_hierarchy_matches_reference(name):
+    """Fixed-DOF masks, voxel/element indexing and level sizes bit-exact on every level."""
+    g = golden(name)
+    H = psfea.Hierarchy(tuple(g["dims"]), g["density"], float(g["nu"]), g["bc"], int(g["coarsest"]))
+    assert H.n_levels == int(g["levels"])
+    for l in range(H.n_levels):
+        info = H.level_info(l)
+        assert [info[k] for k in ("nx", "ny", "nz", "nNodes", "nDof", "freeDof", "nElems", "nOwn", "coarse_m")] == list(g[f"info_{l}"])
+        assert np.array_equal(np.packbits(H.fixed(l)), g[f"fixed_{l}"])
+
+
+def test_own_matrices_match_oracle():
+    import oracle
+    m = W.l_bracket(32, 16, 16, holes=3)
+    H = psfea.Hierarchy(m.dims, m.density, m.nu, m.bc)
+    P = oracle.OracleModel("port", m.dims, m.density, m.nu, m.bc)
+    for l in range(1, H.n_levels):
+        a, b = H.own(l), P.own(l)
+        assert a.shape == b.shape
+        if a.size:
+            assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max()
+        assert np.abs(H.kb(l) - P.kb(l)).max() <= 1e-13 * np.abs(P.kb(l)).max()
+
+
+def test_workloads_are_deterministic_and_loaded_as_specified():
+    c = W.cantilever()
+    assert c.dims == (64, 16, 16) and abs(c.f.sum() + 256.0) < 1e-9
+    assert c.bc.reshape(17, 17, 65, 3)[:, :, 0].all() and c.bc.sum() == 3 * 17 * 17
+    a, b = W.l_bracket(64, 32, 32, holes=8), W.l_bracket(64, 32, 32, holes=8)
+    assert np.array_equal(a.density, b.density) and np.array_equal(a.f, b.f)
+    assert abs(a.f.sum() + 500.0) < 1e-9
+    s = W.simp(16, 8, 8, nrhs=4)
+    assert s.f.shape[0] == 4 and np.allclose(np.linalg.norm(s.f.reshape(4, -1, 3).sum(axis=1), axis=1), 1.0)
+    assert s.density.min() >= 1e-9 and s.density.max() <= 1.0
+
+
+def test_no_device_is_reported_not_faked(have_gpu):
+    if have_gpu:
+        pytest.skip("a GPU is present")
+    with pytest.raises(psfea.SolverError, match="ENODEV"):
+        psfea.VoxelFEA((4, 1, 1), np.ones(4, np.float32), 0.3, np.zeros(3 * 5 * 2 * 2, np.uint8))
