@@ -132,6 +132,18 @@ ps_status ps_fea_set_stream(ps_fea_t* h, void* cuda_stream);
  * 1 the FP64 product of the CG. Diagnostics for roofline reports. */
 ps_status ps_fea_time_kernel(ps_fea_t* h, int32_t which, int32_t reps, double* ms);
 
+/* No counterpart in the reference. y = K x (FP64, held DOFs of y zero) on the finest level and
+ * *dot_dev = x . y, with x_dev, y_dev (nDof doubles) and dot_dev (one double) in device memory, for
+ * callers that cannot allocate device memory during a call: code whose device memory belongs to
+ * another allocator or a fixed budget, and loops that must not stall on the device-wide
+ * synchronisation a cudaMalloc can cause. The call allocates nothing: the reduction's scratch
+ * is a static 32.25 KiB device array in the library (at most 4096 reduction blocks; a device whose
+ * launch shape needs more gets PS_EINVAL). The first call on each device looks up that array's
+ * address and should come before any stream capture. All calls on a device share the array, so
+ * calls that overlap on the GPU race. Stream-ordered on `cuda_stream` (NULL = the handle's stream);
+ * returns without waiting for the GPU. */
+ps_status ps_fea_apply_dot_noalloc(ps_fea_t* h, const double* x_dev, double* y_dev, double* dot_dev, void* cuda_stream);
+
 /* Device kernels the handle has launched since it was created. */
 int64_t ps_fea_kernel_launches(const ps_fea_t* h);
 

@@ -167,6 +167,14 @@ ps_status ps_fea_time_kernel(ps_fea_t* h, int32_t which, int32_t reps, double* m
     });
 }
 
+ps_status ps_fea_apply_dot_noalloc(ps_fea_t* h, const double* x_dev, double* y_dev, double* dot_dev, void* cuda_stream) {
+    return guarded([&] {
+        if (!h || !x_dev || !y_dev || !dot_dev) return fail(PS_EINVAL, "NULL pointer");
+        h->solver.applyDotStatic(x_dev, y_dev, dot_dev, cuda_stream);
+        return PS_OK;
+    });
+}
+
 int64_t ps_fea_kernel_launches(const ps_fea_t* h) { return h ? h->solver.launches() : 0; }
 
 int64_t ps_fea_ndof(const ps_fea_t* h) { return h ? h->solver.nDof() : 0; }

@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1340,6 +1341,86 @@ void Solver::reactions(const double* u, const double* f, double R[3]) {
     R[0] = I.hostState->alpha;
     R[1] = I.hostState->beta;
     R[2] = I.hostState->pq;
+}
+
+// ==================================================================== allocation-free product
+//
+// For callers that must not allocate device memory during a call: code running on device memory
+// owned by another allocator (a framework's caching pool, a fixed serving budget) and loops that
+// cannot afford the implicit device synchronisation a cudaMalloc may cause. y = K x and x.y on the
+// finest level with the reduction's scratch (per-block partial sums and the last-block ticket) in
+// this file-scope device array instead of handle-owned or newly allocated memory. Its size caps the
+// kernel's grid at NOALLOC_BLOCKS blocks (grid-stride, so any model size fits); a device whose
+// launch shape would need more is refused. Every call on a device shares the array: calls that
+// overlap on the GPU race, and each call clears the ticket before use.
+
+constexpr int NOALLOC_BLOCKS = 4096;
+constexpr size_t NOALLOC_BYTES = 256 + size_t(NOALLOC_BLOCKS) * sizeof(double);  // ticket line + partials
+static __device__ __align__(256) unsigned char g_noallocScratch[NOALLOC_BYTES];
+
+namespace dev {
+
+// q = K p (FP64, held DOFs 0) and p.q into *dot, the reduction scratch in g_noallocScratch
+__global__ void __launch_bounds__(NODE_THREADS) k_apply_dot_static(LevelView L, Coefs<double> C, const double* __restrict__ p,
+                                                                   double* __restrict__ q, double* __restrict__ dot,
+                                                                   unsigned char* scratch) {
+    double v[1] = {0.0};
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < L.nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = __ldg(L.nmask + n);
+        int i, j, k;
+        nodeCoords(L, n, i, j, k);
+        double acc[3];
+        applyAt<double, false>(L, C, p, i, j, k, n, mask, acc);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const double y = fixedDof(mask, c) ? 0.0 : acc[c];
+            q[3 * n + c] = y;
+            v[0] += p[3 * n + c] * y;
+        }
+    }
+    unsigned* ticket = reinterpret_cast<unsigned*>(scratch);
+    double* partials = reinterpret_cast<double*>(scratch + 256);
+    double tot[1];
+    if (gridReduce<1>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) *dot = tot[0];
+}
+
+}  // namespace dev
+
+namespace {
+
+// device address of g_noallocScratch per device, looked up once per device with that device
+// current (the first call on a device does it, so that first call should come before any stream
+// capture)
+unsigned char* noallocScratch() {
+    static std::mutex mu;
+    static std::vector<unsigned char*> addr;
+    int devId = 0;
+    check(cudaGetDevice(&devId), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(mu);
+    if (int(addr.size()) <= devId) addr.resize(size_t(devId) + 1, nullptr);
+    if (!addr[size_t(devId)]) {
+        void* p = nullptr;
+        check(cudaGetSymbolAddress(&p, g_noallocScratch), "cudaGetSymbolAddress");
+        addr[size_t(devId)] = static_cast<unsigned char*>(p);
+    }
+    return addr[size_t(devId)];
+}
+
+}  // namespace
+
+void Solver::applyDotStatic(const double* xDev, double* yDev, double* dotDev, void* s) {
+    SolverImpl& I = *impl_;
+    const HostLevel& h = I.H.levels[0];
+    DevLevel& D = I.L[0];
+    const int grid = I.nodeGrid(h.nNodes);
+    if (grid > NOALLOC_BLOCKS)
+        throw Error(PS_EINVAL, "this device needs " + std::to_string(grid) + " reduction blocks; the static scratch holds " +
+                                   std::to_string(NOALLOC_BLOCKS));
+    cudaStream_t st = s ? static_cast<cudaStream_t>(s) : I.stream;
+    unsigned char* scratch = noallocScratch();
+    check(cudaMemsetAsync(scratch, 0, 256, st), "ticket clear");
+    I.launch(dev::k_apply_dot_static, grid, dev::NODE_THREADS, 0, st, D.view, D.c64, xDev, yDev, dotDev, scratch);
+    check(cudaGetLastError(), "apply_dot_static");
 }
 
 }  // namespace psfea

@@ -36,6 +36,9 @@ public:
     // Chebyshev step of the V-cycle, 1 = the FP64 product of the CG
     double timeKernel(int which, int reps);
     int64_t launches() const;
+    // y = K x and x.y on the finest level, device pointers, with no allocation (scratch in a
+    // static device array); stream-ordered on s (nullptr = the handle's stream), no host sync
+    void applyDotStatic(const double* xDev, double* yDev, double* dotDev, void* s);
 
 private:
     std::unique_ptr<SolverImpl> impl_;

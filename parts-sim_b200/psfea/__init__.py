@@ -69,6 +69,7 @@ _dev_bytes = _sig("ps_fea_device_bytes", C.c_int64, _P)
 _set_stream = _sig("ps_fea_set_stream", C.c_int, _P, C.c_void_p)
 _time_kernel = _sig("ps_fea_time_kernel", C.c_int, _P, C.c_int32, C.c_int32, C.POINTER(C.c_double))
 _launches = _sig("ps_fea_kernel_launches", C.c_int64, _P)
+_apply_dot_noalloc = _sig("ps_fea_apply_dot_noalloc", C.c_int, _P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
 _element = _sig("ps_element_matrix", C.c_int, C.c_double, _F64P, C.c_void_p)
 _prune = _sig("ps_prune_floating", C.c_int, _I32P, _F32P, _U8P, _F32P, C.POINTER(C.c_int32))
 _last_error = _sig("ps_last_error", C.c_char_p)
@@ -87,7 +88,7 @@ EXPORTS = ("ps_solve_opts_default", "ps_fea_create", "ps_fea_solve", "ps_fea_sol
            "ps_fea_level_fixed", "ps_fea_level_lmax", "ps_fea_device_bytes", "ps_fea_destroy", "ps_element_matrix",
            "ps_prune_floating", "ps_last_error", "ps_hierarchy_create", "ps_hierarchy_num_levels", "ps_hierarchy_level_info",
            "ps_hierarchy_level_fixed", "ps_hierarchy_level_own", "ps_hierarchy_level_kb", "ps_hierarchy_destroy",
-           "ps_fea_set_stream", "ps_fea_time_kernel", "ps_fea_kernel_launches")
+           "ps_fea_set_stream", "ps_fea_time_kernel", "ps_fea_kernel_launches", "ps_fea_apply_dot_noalloc")
 
 
 class SolverError(RuntimeError):
@@ -258,6 +259,14 @@ class VoxelFEA:
         if st != PS_OK:
             _raise(st)
         return ms.value
+
+    def apply_dot_noalloc(self, x_ptr, y_ptr, dot_ptr, stream_ptr=None):
+        """y = K x and x.y on device pointers without allocating (see ps_fea_apply_dot_noalloc);
+        stream-ordered, returns before the GPU has finished."""
+        st = _apply_dot_noalloc(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), C.c_void_p(dot_ptr),
+                                C.c_void_p(stream_ptr) if stream_ptr else None)
+        if st != PS_OK:
+            _raise(st)
 
     @property
     def kernel_launches(self):
