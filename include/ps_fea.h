@@ -67,6 +67,8 @@ typedef struct ps_solve_opts {
     const volatile int32_t* cancel;   /* polled between iteration batches; nonzero cancels (the
                                          onProgress-returns-true contract, voxel_fea.cpp:910) */
     double time_limit_s;              /* 0 = none */
+    int32_t smoother_degree;          /* Chebyshev smoother degree per V-cycle half (0 = the
+                                         reference's 2, voxel_fea.cpp:692-725); 1..8 */
 } ps_solve_opts;
 
 typedef struct ps_solve_result {
@@ -79,7 +81,8 @@ typedef struct ps_solve_result {
     int64_t kernels;      /* device kernels this call launched */
 } ps_solve_result;
 
-/* tol 1e-6, max_iter 500, PS_PREC_FP64, no warm start, no cancel flag, no time limit */
+/* tol 1e-6, max_iter 500, PS_PREC_FP64, no warm start, no cancel flag, no time limit, smoother
+ * degree 2 */
 void ps_solve_opts_default(ps_solve_opts* opts);
 
 /* Builds the multigrid hierarchy (2:1 coarsening with exact Galerkin coarse elements until the

@@ -58,6 +58,7 @@ void ps_solve_opts_default(ps_solve_opts* o) {
     o->x0 = nullptr;
     o->cancel = nullptr;
     o->time_limit_s = 0;
+    o->smoother_degree = 0;
 }
 
 const char* ps_last_error(void) { return lastError.c_str(); }
@@ -79,7 +80,8 @@ ps_status ps_fea_solve(ps_fea_t* h, const double* f, const ps_solve_opts* opts, 
     return guarded([&] {
         if (!h || !f || !u_out) return fail(PS_EINVAL, "Force or displacement vector has the wrong size.");
         const ps_solve_opts o = resolve(opts);
-        if (!(o.tol >= 0) || o.max_iter < 0 || (o.precision != PS_PREC_FP64 && o.precision != PS_PREC_MIXED))
+        if (!(o.tol >= 0) || o.max_iter < 0 || (o.precision != PS_PREC_FP64 && o.precision != PS_PREC_MIXED) || o.smoother_degree < 0 ||
+            o.smoother_degree > 8)
             return fail(PS_EINVAL, "invalid solve options");
         ps_solve_result r{};
         const ps_status s = h->solver.solve(f, o, u_out, r);
@@ -92,7 +94,8 @@ ps_status ps_fea_solve_dev(ps_fea_t* h, const double* f_dev, const ps_solve_opts
     return guarded([&] {
         if (!h || !f_dev || !u_dev) return fail(PS_EINVAL, "Force or displacement vector has the wrong size.");
         const ps_solve_opts o = resolve(opts);
-        if (!(o.tol >= 0) || o.max_iter < 0 || (o.precision != PS_PREC_FP64 && o.precision != PS_PREC_MIXED))
+        if (!(o.tol >= 0) || o.max_iter < 0 || (o.precision != PS_PREC_FP64 && o.precision != PS_PREC_MIXED) || o.smoother_degree < 0 ||
+            o.smoother_degree > 8)
             return fail(PS_EINVAL, "invalid solve options");
         ps_solve_result r{};
         const ps_status s = h->solver.solveDevice(f_dev, o, u_dev, r);

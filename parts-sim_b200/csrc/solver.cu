@@ -26,6 +26,7 @@
 #include <mutex>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -40,7 +41,8 @@ namespace dev {
 // ---------------------------------------------------------------- control
 
 struct SolveState {
-    double bnorm, rel, tol, rz, alpha, beta, rmax, scale, peak, est, pq;
+    double bnorm, rel, tol, rz, alpha, beta, rmax, scale, peak, est, pq, foldFactor;
+    double vscale;  // the scale the current FP32 right-hand side r32 was made with (r32 = r * vscale)
     int it, maxIter, done, status, fold, folds, first, mixed;
 };
 enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_BREAKDOWN = 3 };
@@ -69,7 +71,7 @@ enum { OP_APPLY = 0, OP_CHEB = 1, OP_RESID = 2 };
 //   OP_APPLY  y = K x (held DOFs 0 unless raw)
 //   OP_CHEB   d = c1 d + c2 D^-1 (r - K x); y = x + d      (Chebyshev / Jacobi step, 32-bit)
 //   OP_RESID  y = r - K x
-template <class T, int MODE, bool OWN16>
+template <class T, int MODE, bool OWN16, bool DIFF = false>
 __global__ void __launch_bounds__(NODE_THREADS) k_op(LevelView L, Coefs<T> C, const T* __restrict__ x, T* __restrict__ y,
                                                       const float* __restrict__ r, float* __restrict__ d, float c1, float c2, int raw,
                                                       Ctl ctl) {
@@ -79,7 +81,7 @@ __global__ void __launch_bounds__(NODE_THREADS) k_op(LevelView L, Coefs<T> C, co
         int i, j, k;
         nodeCoords(L, n, i, j, k);
         T acc[3];
-        applyAt<T, OWN16>(L, C, x, i, j, k, n, mask, acc);
+        applyAt<T, OWN16, DIFF>(L, C, x, i, j, k, n, mask, acc);
 #pragma unroll
         for (int q = 0; q < 3; q++) {
             const long long id = 3 * n + q;
@@ -136,6 +138,308 @@ __global__ void __launch_bounds__(NODE_THREADS) k_apply_alpha(LevelView L, Coefs
     }
 }
 
+// ---------------------------------------------------------------- coarse-level operator kernel
+
+// The same operator and epilogues (OP_APPLY / OP_CHEB / OP_RESID) with eight lanes per node, one
+// per surrounding voxel: each lane gathers its voxel's 8 corner values and applies the 3 rows of
+// its corner (Kb from shared memory, or the voxel's own matrix), and the eight partial sums meet
+// by shuffles. Coarse levels have few nodes and many own matrices; spreading a node over eight
+// lanes turns one thread's chain of eight dependent matrix reads into eight parallel ones.
+template <class T, int MODE, bool OWN16, bool DIFF>
+__global__ void __launch_bounds__(256) k_op8(LevelView L, Coefs<T> C, const T* __restrict__ x, T* __restrict__ y,
+                                             const float* __restrict__ r, float* __restrict__ d, float c1, float c2, int raw, Ctl ctl) {
+    if (skipped(ctl)) return;
+    __shared__ T kb[576];
+    for (int e = threadIdx.x; e < 576; e += blockDim.x) kb[e] = C.Kb[e];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, v = lane & 7, group = lane >> 3;
+    const int di = v & 1, dj = (v >> 1) & 1, dk = v >> 2, a = cornerOf(1 - di, 1 - dj, 1 - dk);
+    const long long NX = L.NX, NXY = (long long)L.NX * L.NY;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long nb = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4; nb < L.nNodes; nb += warps * 4) {
+        const long long n = nb + group;
+        const bool valid = n < L.nNodes;
+        const uint8_t mask = valid ? __ldg(L.nmask + n) : uint8_t(0);
+        T acc[3] = {T(0), T(0), T(0)};
+        if (mask & NM_ACTIVE) {
+            int i, j, k;
+            nodeCoords(L, n, i, j, k);
+            const int ei = i - 1 + di, ej = j - 1 + dj, ek = k - 1 + dk;
+            uint32_t w = 0;
+            if (ei >= 0 && ej >= 0 && ek >= 0 && ei < L.nx && ej < L.ny && ek < L.nz)
+                w = __ldg(L.word + (ei + (long long)L.nx * (ej + (long long)L.ny * ek)));
+            if (w) {
+                T own[3] = {T(0), T(0), T(0)};
+                if (DIFF) {
+                    own[0] = __ldg(x + 3 * n);
+                    own[1] = __ldg(x + 3 * n + 1);
+                    own[2] = __ldg(x + 3 * n + 2);
+                }
+                T xe[24];
+#pragma unroll
+                for (int b = 0; b < 8; b++) {
+                    const int bx = (b == 1 || b == 2 || b == 5 || b == 6), by = (b == 2 || b == 3 || b == 6 || b == 7), bz = b >> 2;
+                    const T* xp = x + 3 * (n + (di + bx - 1) + (dj + by - 1) * NX + (dk + bz - 1) * NXY);
+                    xe[3 * b] = __ldg(xp) - own[0];
+                    xe[3 * b + 1] = __ldg(xp + 1) - own[1];
+                    xe[3 * b + 2] = __ldg(xp + 2) - own[2];
+                }
+                if (!(w & OWN_BIT)) {
+                    const T* k0 = kb + (3 * a) * 24;
+                    T t0 = 0, t1 = 0, t2 = 0;
+#pragma unroll
+                    for (int q = 0; q < 24; q++) {
+                        t0 += k0[q] * xe[q];
+                        t1 += k0[24 + q] * xe[q];
+                        t2 += k0[48 + q] * xe[q];
+                    }
+                    const T s = T(__uint_as_float(w));
+                    acc[0] = s * t0;
+                    acc[1] = s * t1;
+                    acc[2] = s * t2;
+                } else if (OWN16) {
+                    const __half2* K2 = reinterpret_cast<const __half2*>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a);
+#pragma unroll
+                    for (int dd = 0; dd < 3; dd++) {
+                        T t = 0;
+#pragma unroll
+                        for (int q = 0; q < 12; q++) {
+                            const float2 kv = __half22float2(__ldg(K2 + dd * 12 + q));
+                            t += T(kv.x) * xe[2 * q] + T(kv.y) * xe[2 * q + 1];
+                        }
+                        acc[dd] = T(L.hs) * t;
+                    }
+                } else {
+                    const float4* K4 = reinterpret_cast<const float4*>(L.own + (long long)(w & ~OWN_BIT) * 576 + 72 * a);
+#pragma unroll
+                    for (int dd = 0; dd < 3; dd++) {
+                        T t = 0;
+#pragma unroll
+                        for (int q = 0; q < 6; q++) {
+                            const float4 kv = __ldg(K4 + dd * 6 + q);
+                            t += T(kv.x) * xe[4 * q] + T(kv.y) * xe[4 * q + 1] + T(kv.z) * xe[4 * q + 2] + T(kv.w) * xe[4 * q + 3];
+                        }
+                        acc[dd] = t;
+                    }
+                }
+            }
+            if (v == 0 && L.dadd) {
+#pragma unroll
+                for (int q = 0; q < 3; q++) acc[q] += (sizeof(T) == 8 ? T(L.dadd[3 * n + q]) : T(L.dadd32[3 * n + q])) * x[3 * n + q];
+            }
+        }
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1)
+#pragma unroll
+            for (int q = 0; q < 3; q++) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        if (valid && v < 3) {
+            const int q = v;
+            const long long id = 3 * n + q;
+            const bool fx = fixedDof(mask, q);
+            const T kx = q == 0 ? acc[0] : (q == 1 ? acc[1] : acc[2]);
+            if (MODE == OP_APPLY) {
+                y[id] = (!raw && fx) ? T(0) : kx;
+            } else if (MODE == OP_RESID) {
+                y[id] = fx ? T(0) : T(r[id]) - kx;
+            } else {
+                if (fx) {
+                    d[id] = 0.f;
+                    y[id] = T(0);
+                } else {
+                    const float dn = c1 * d[id] + c2 * L.invD[id] * (r[id] - float(kx));
+                    d[id] = dn;
+                    y[id] = x[id] + T(dn);
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- tiled operator kernel
+
+// The level's operator over its active tiles with a per-node epilogue:
+//   TOP_APPLY  y = K x (held DOFs 0 unless raw)
+//   TOP_CHEB   d = c1 d + c2 D^-1 (r - K x); y = x + d      (Chebyshev / Jacobi step, 32-bit)
+//   TOP_RESID  y = r - K x
+//   TOP_DOT    y = K x (held 0) and the CG step alpha = rz / (x . y); x . y <= 0 is a breakdown
+//              (voxel_fea.cpp:902-905)
+template <class T, int MODE, bool OWN16, bool DIFF>
+__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? 2 : 3) k_tile(LevelView L, Coefs<T> C, const uint32_t* __restrict__ tiles, TileIO<T> io,
+                                                      SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
+    if (skipped(ctl)) return;
+    using Op = TileOp<T, OWN16, DIFF>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* xs = reinterpret_cast<T*>(smem);
+    uint32_t* vs = reinterpret_cast<uint32_t*>(smem + tileOffV<T>());
+    T* ks = reinterpret_cast<T*>(smem + tileOffK<T>());  // K x per tile node, [z][y][3 x + c]
+    uint8_t* ms = smem + tileOffM<T>();
+    int* blist = reinterpret_cast<int*>(smem + tileOffB<T>());
+    int* wsum = blist + TILE_NODES;
+    const uint32_t tw = tiles[blockIdx.x];
+    const int i0 = int(tw & 2047u) * TX, j0 = int((tw >> 11) & 2047u) * TY, k0 = int(tw >> 22) * TZ;
+    const int tid = threadIdx.x, cx = tid & 31, cy = tid >> 5;
+    const int NX = L.NX, NY = L.NY, NZ = L.NZ;
+    const long long NXY = (long long)NX * NY;
+
+    // stage x (tile + halo) and the voxel words around it: asynchronous copies, all in flight; one
+    // warp per row of 34 nodes (102 contiguous values) / 33 voxel words
+    const int lane = tid & 31, warp = tid >> 5;
+    {
+        const int iLo = i0 - 1;
+        for (int row = warp; row < HZ * HY; row += TILE_THREADS / 32) {
+            const int z = row / HY, y = row - z * HY;
+            const int j = j0 - 1 + y, k = k0 - 1 + z;
+            const bool rowOk = j >= 0 && j < NY && k >= 0 && k < NZ;
+            const T* src = io.x + 3 * ((long long)iLo + (long long)NX * j + NXY * k);
+            T* dst = xs + row * PROW;
+#pragma unroll
+            for (int q = 0; q < (PROW + 31) / 32; q++) {
+                const int c3 = lane + 32 * q;
+                if (c3 >= PROW) break;
+                const int i = iLo + c3 / 3;
+                const bool ok = rowOk && i >= 0 && i < NX;
+                cpAsync<sizeof(T)>(dst + c3, ok ? src + c3 : io.x, ok);
+            }
+        }
+        for (int row = warp; row < VZ * VY; row += TILE_THREADS / 32) {
+            const int z = row / VY, y = row - z * VY;
+            const int j = j0 - 1 + y, k = k0 - 1 + z;
+            const bool rowOk = j >= 0 && j < L.ny && k >= 0 && k < L.nz;
+            const uint32_t* src = L.word + ((long long)(i0 - 1) + (long long)L.nx * (j + (long long)L.ny * k));
+#pragma unroll
+            for (int q = 0; q < (VX + 31) / 32; q++) {
+                const int c = lane + 32 * q;
+                if (c >= VX) break;
+                const int i = i0 - 1 + c;
+                const bool ok = rowOk && i >= 0 && i < L.nx;
+                cpAsync<4>(vs + row * VX + c, ok ? src + c : L.word, ok);
+            }
+        }
+    }
+    // the column's node masks meanwhile
+    const int i = i0 + cx, j = j0 + cy;
+    const bool col = i < NX && j < NY;
+    uint8_t mk[TZ];
+    bool anyUniform = false;
+#pragma unroll
+    for (int z = 0; z < TZ; z++) {
+        const int k = k0 + z;
+        mk[z] = (col && k < NZ) ? __ldg(L.nmask + i + (long long)NX * j + NXY * k) : uint8_t(0);
+        ms[(z * TY + cy) * TX + cx] = mk[z];
+        anyUniform = anyUniform || (mk[z] & NM_UNIFORM);
+    }
+    cpAsyncWaitAll();
+    __syncthreads();
+
+    // pass 1: uniform nodes of the thread's column, all four from one sweep of the planes
+    unsigned bmask = 0;
+#pragma unroll
+    for (int z = 0; z < TZ; z++)
+        if ((mk[z] & NM_ACTIVE) && !(mk[z] & NM_UNIFORM)) bmask |= 1u << z;
+    if (anyUniform) {
+        T acc[TZ][3];
+        Op::column(C, xs, cx, cy, acc);
+#pragma unroll
+        for (int z = 0; z < TZ; z++) {
+            if (!(mk[z] & NM_UNIFORM)) continue;
+            const T s = T(__uint_as_float(vs[vOff(cx, cy, z)]));
+            T* kp = ks + (z * TY + cy) * (3 * TX) + 3 * cx;
+            kp[0] = s * acc[z][0];
+            kp[1] = s * acc[z][1];
+            kp[2] = s * acc[z][2];
+        }
+    }
+    // deterministic compaction: thread order, then z
+    const int cnt = __popc(bmask);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (cx >= o) incl += v;
+    }
+    if (cx == 31) wsum[cy] = incl;
+    __syncthreads();
+    int off = incl - cnt, total = 0;
+#pragma unroll
+    for (int w = 0; w < TILE_THREADS / 32; w++) {
+        const int c = wsum[w];
+        off += (w < cy) ? c : 0;
+        total += c;
+    }
+    for (unsigned b = bmask; b; b &= b - 1) blist[off++] = (tid << 4) | (__ffs(b) - 1);
+    __syncthreads();
+    // pass 2: the listed nodes, all threads
+    for (int q = tid; q < total; q += TILE_THREADS) {
+        const int e = blist[q], bt = e >> 4, bz = e & 15, bx = bt & 31, by = bt >> 5;
+        T own[3], acc[3];
+        own[0] = own[1] = own[2] = T(0);
+        if (DIFF) {
+            const T* xn = xs + xOff(bx, by, bz);
+            own[0] = xn[0]; own[1] = xn[1]; own[2] = xn[2];
+        }
+        Op::general(L, C, xs, vs, bx, by, bz, acc, own);
+        T* kp = ks + (bz * TY + by) * (3 * TX) + 3 * bx;
+        kp[0] = acc[0];
+        kp[1] = acc[1];
+        kp[2] = acc[2];
+    }
+    __syncthreads();
+    // pass 3: the epilogue, one warp per row of 32 nodes (96 contiguous values), independent loads
+    double dot = 0.0;
+    const int nxHere = min(TX, NX - i0);
+#pragma unroll
+    for (int rr = 0; rr < TY * TZ / (TILE_THREADS / 32); rr++) {
+        const int row = warp + rr * (TILE_THREADS / 32), z = row / TY, y = row - z * TY;
+        if (j0 + y >= NY || k0 + z >= NZ) continue;
+        const long long rowBase = 3 * ((long long)i0 + (long long)NX * (j0 + y) + NXY * (k0 + z));
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const int c3 = lane + 32 * q, ex = c3 / 3, comp = c3 - 3 * ex;
+            if (ex >= nxHere) continue;
+            const uint8_t mask = ms[(z * TY + y) * TX + ex];
+            const long long id = rowBase + c3;
+            const bool act = mask & NM_ACTIVE;
+            const bool fx = fixedDof(mask, comp);
+            const T xv = xs[xOff(ex, y, z) + comp];
+            T kx = act ? ks[row * (3 * TX) + c3] : T(0);
+            if (act && L.dadd) kx += (sizeof(T) == 8 ? T(L.dadd[id]) : T(L.dadd32[id])) * xv;
+            if (MODE == TOP_APPLY) {
+                io.y[id] = (!io.raw && fx) ? T(0) : kx;
+            } else if (MODE == TOP_RESID) {
+                io.y[id] = fx ? T(0) : T(io.r[id]) - kx;
+            } else if (MODE == TOP_DOT) {
+                const T yv = fx ? T(0) : kx;
+                io.y[id] = yv;
+                dot += double(xv) * double(yv);
+            } else {
+                if (fx) {
+                    io.d[id] = 0.f;
+                    io.y[id] = T(0);
+                } else {
+                    const float dn = io.c1 * io.d[id] + io.c2 * L.invD[id] * (io.r[id] - float(kx));
+                    io.d[id] = dn;
+                    io.y[id] = xv + T(dn);
+                }
+            }
+        }
+    }
+    if (MODE == TOP_DOT) {
+        double v[1] = {dot};
+        double tot[1];
+        if (gridReduce<1>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) {
+            const double pq = tot[0];
+            st->pq = pq;
+            if (!(pq > 0)) {
+                st->status = ST_BREAKDOWN;
+                if (st->mixed) st->fold = 1;  // fold what there is, then stop
+                else st->done = 1;
+            } else {
+                st->alpha = st->rz / pq;
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------- V-cycle pieces (32-bit)
 
 // z = d = c0 D^-1 r (the first Chebyshev step from zero)
@@ -151,7 +455,8 @@ __global__ void k_cheb_first(long long nDof, const float* __restrict__ r, const 
 
 // rc = P^T rf gathered per coarse node: fine 2I (weight 1) and 2I +- 1 (weight 1/2) per axis;
 // held / inactive coarse DOFs 0
-__global__ void k_restrict(int FNX, int FNY, int FNZ, LevelView C, const float* __restrict__ rf, float* __restrict__ rc, Ctl ctl) {
+__global__ void k_restrict(int FNX, int FNY, int FNZ, LevelView C, const float* __restrict__ rf, float* __restrict__ rc, float* __restrict__ dc,
+                           float* __restrict__ zc, float c0, Ctl ctl) {
     if (skipped(ctl)) return;
     const long long FNXY = (long long)FNX * FNY;
     for (long long cn = blockIdx.x * (long long)blockDim.x + threadIdx.x; cn < C.nNodes; cn += (long long)gridDim.x * blockDim.x) {
@@ -180,9 +485,17 @@ __global__ void k_restrict(int FNX, int FNY, int FNZ, LevelView C, const float* 
                 }
             }
         }
-        rc[3 * cn] = fixedDof(mask, 0) ? 0.f : s0;
-        rc[3 * cn + 1] = fixedDof(mask, 1) ? 0.f : s1;
-        rc[3 * cn + 2] = fixedDof(mask, 2) ? 0.f : s2;
+        const float sv[3] = {s0, s1, s2};
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const float v = fixedDof(mask, q) ? 0.f : sv[q];
+            rc[3 * cn + q] = v;
+            if (dc) {  // the coarse level's first smoothing step, d = z = c0 D^-1 r
+                const float dv = c0 * C.invD[3 * cn + q] * v;
+                dc[3 * cn + q] = dv;
+                zc[3 * cn + q] = dv;
+            }
+        }
     }
 }
 
@@ -281,15 +594,20 @@ __global__ void k_cg_init(long long nNodes, const uint8_t* __restrict__ nmask, c
     (void)r32;
 }
 
-// x += alpha p, r -= alpha q at free DOFs; rel = ||r|| / bnorm; stop on rel <= tol or the cap
+// x += alpha p, r -= alpha q at free DOFs; rel = ||r|| / bnorm; stop on rel <= tol or the cap.
+// Fused: the preconditioner's FP32 input r32 = r * s (s = 1 / max|r_free| of the previous iterate;
+// the V-cycle is linear, so any order-one scale serves, voxel_fea.cpp:843-857) and the first
+// Chebyshev step of the finest level, d = z = c0 D^-1 r32.
 __global__ void k_cg_update(long long nNodes, const uint8_t* __restrict__ nmask, double* __restrict__ x, double* __restrict__ r,
-                            const double* __restrict__ p, const double* __restrict__ q, SolveState* st, double* partials, unsigned* ticket,
+                            const double* __restrict__ p, const double* __restrict__ q, float* __restrict__ r32, const float* __restrict__ invD,
+                            float* __restrict__ d, float* __restrict__ z, float c0, SolveState* st, double* partials, unsigned* ticket,
                             Ctl ctl) {
     if (skipped(ctl)) return;
-    const double alpha = st->alpha;
+    const double alpha = st->alpha, s = st->scale;
     double v[2] = {0, 0};
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
         const uint8_t mask = nmask[n];
+        if ((mask & 7) == 7) continue;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             if (fixedDof(mask, c)) continue;
@@ -299,11 +617,19 @@ __global__ void k_cg_update(long long nNodes, const uint8_t* __restrict__ nmask,
             r[id] = rv;
             v[0] += rv * rv;
             v[1] = fmax(v[1], fabs(rv));
+            if (r32) {
+                const float rs = float(rv * s);
+                r32[id] = rs;
+                const float dv = c0 * invD[id] * rs;
+                d[id] = dv;
+                z[id] = dv;
+            }
         }
     }
     double tot[2];
     if (gridReduce<2>(v, 2u, partials, ticket, tot) && threadIdx.x == 0) {
         st->rel = sqrt(tot[0]) / st->bnorm;
+        st->vscale = s;
         st->rmax = tot[1];
         st->scale = tot[1] > 0 ? 1.0 / tot[1] : 1.0;
         st->it += 1;
@@ -317,30 +643,51 @@ __global__ void k_cg_update(long long nNodes, const uint8_t* __restrict__ nmask,
     }
 }
 
-// the preconditioner's input: r32 = float(r / max|r_free|) at free DOFs (voxel_fea.cpp:856-857)
+// the preconditioner's input: r32 = float(r / max|r_free|) at free DOFs (voxel_fea.cpp:856-857),
+// and (d non-null) the first Chebyshev step d = z = c0 D^-1 r32
 __global__ void k_vc_load(long long nNodes, const uint8_t* __restrict__ nmask, const double* __restrict__ r, float* __restrict__ r32,
-                          const SolveState* st, Ctl ctl) {
+                          const float* __restrict__ invD, float* __restrict__ d, float* __restrict__ z, float c0, SolveState* st, Ctl ctl) {
     if (skipped(ctl)) return;
     const double s = st->scale;
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
         const uint8_t mask = nmask[n];
+        if ((mask & 7) == 7) continue;
 #pragma unroll
-        for (int c = 0; c < 3; c++) r32[3 * n + c] = fixedDof(mask, c) ? 0.f : float(r[3 * n + c] * s);
+        for (int c = 0; c < 3; c++) {
+            if (fixedDof(mask, c)) continue;
+            const long long id = 3 * n + c;
+            const float rs = float(r[id] * s);
+            r32[id] = rs;
+            if (d) {
+                const float dv = c0 * invD[id] * rs;
+                d[id] = dv;
+                z[id] = dv;
+            }
+        }
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->vscale = s;
 }
 
-// z = z32 * rmax (or z64); rzNew = r.z, zq = z.q; beta = max(0, -alpha zq / rz) (voxel_fea.cpp:913-917);
-// on the first pass beta = 0
-__global__ void k_cg_dots(long long nDof, const double* __restrict__ r, const float* __restrict__ z32, const double* __restrict__ z64,
-                          const double* __restrict__ q, SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
+// z = z32 / vscale (or z64); rzNew = r.z, zq = z.q; beta = max(0, -alpha zq / rz)
+// (voxel_fea.cpp:913-917); on the first pass beta = 0. Held DOFs carry zeros and are skipped.
+__global__ void k_cg_dots(long long nNodes, const uint8_t* __restrict__ nmask, const double* __restrict__ r, const float* __restrict__ z32,
+                          const double* __restrict__ z64, const double* __restrict__ q, SolveState* st, double* partials, unsigned* ticket,
+                          Ctl ctl) {
     if (skipped(ctl)) return;
-    const double rmax = st->rmax;
+    const double inv = 1.0 / st->vscale;
     const bool first = st->first;
     double v[2] = {0, 0};
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x) {
-        const double z = z64 ? z64[i] : double(z32[i]) * rmax;
-        v[0] += r[i] * z;
-        if (!first) v[1] += z * q[i];
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+        if ((mask & 7) == 7) continue;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            if (fixedDof(mask, c)) continue;
+            const long long i = 3 * n + c;
+            const double z = z64 ? z64[i] : double(z32[i]) * inv;
+            v[0] += r[i] * z;
+            if (!first) v[1] += z * q[i];
+        }
     }
     double tot[2];
     if (gridReduce<2>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) {
@@ -349,15 +696,22 @@ __global__ void k_cg_dots(long long nDof, const double* __restrict__ r, const fl
     }
 }
 
-// p = z + beta p
-__global__ void k_cg_p(long long nDof, const float* __restrict__ z32, const double* __restrict__ z64, double* __restrict__ p, SolveState* st,
-                       Ctl ctl) {
+// p = z + beta p at free DOFs
+__global__ void k_cg_p(long long nNodes, const uint8_t* __restrict__ nmask, const float* __restrict__ z32, const double* __restrict__ z64,
+                       double* __restrict__ p, SolveState* st, Ctl ctl) {
     if (skipped(ctl)) return;
-    const double rmax = st->rmax, beta = st->beta;
+    const double inv = 1.0 / st->vscale, beta = st->beta;
     const bool first = st->first;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x) {
-        const double z = z64 ? z64[i] : double(z32[i]) * rmax;
-        p[i] = first ? z : z + beta * p[i];
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+        if ((mask & 7) == 7) continue;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            if (fixedDof(mask, c)) continue;
+            const long long i = 3 * n + c;
+            const double z = z64 ? z64[i] : double(z32[i]) * inv;
+            p[i] = first ? z : z + beta * p[i];
+        }
     }
 }
 
@@ -407,7 +761,7 @@ __global__ void k_mx_update(long long nNodes, const uint8_t* __restrict__ nmask,
         st->est = sqrt(tot[0]) / st->scale / st->bnorm;
         st->it += 1;
         st->peak = fmax(st->peak, st->est);
-        if (st->est <= st->tol || st->est <= 0.1 * st->peak || st->it >= st->maxIter || !(st->est == st->est)) st->fold = 1;
+        if (st->est <= st->tol || st->est <= st->foldFactor * st->peak || st->it >= st->maxIter || !(st->est == st->est)) st->fold = 1;
     }
 }
 
@@ -511,11 +865,11 @@ __global__ void k_rmax(long long nNodes, const uint8_t* __restrict__ nmask, cons
 // z = z32 * rmax on active nodes, 0 elsewhere (voxel_fea.cpp:859-860)
 __global__ void k_vc_store(long long nNodes, const uint8_t* __restrict__ nmask, const float* __restrict__ z32, double* __restrict__ z,
                            const SolveState* st) {
-    const double rmax = st->rmax;
+    const double inv = 1.0 / st->vscale, rmax = st->rmax;
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
         const bool act = nmask[n] & NM_ACTIVE;
 #pragma unroll
-        for (int c = 0; c < 3; c++) z[3 * n + c] = (act && rmax > 0) ? double(z32[3 * n + c]) * rmax : 0.0;
+        for (int c = 0; c < 3; c++) z[3 * n + c] = (act && rmax > 0) ? double(z32[3 * n + c]) * inv : 0.0;
     }
 }
 
@@ -760,7 +1114,12 @@ struct DevLevel {
     dev::Coefs<float> c32{};
     DevMem word, nmask, own, own16, invD, invD64, dadd, dadd32, bc;
     DevMem r, z, t, d;
+    DevMem tiles;      // packed (tx, ty, tz) of the 32 x 8 x 4 node tiles with an active node
+    int nTiles = 0;
+    bool useTiles = false;  // tiled kernel (large levels) or one thread per node (small ones)
+    bool use8 = false;      // eight lanes per node (the smallest levels)
     float cf0 = 0, cf1 = 0, cf2 = 0, omega = 0.5f;
+    std::vector<float> chebC1, chebC2;  // steps 1 .. degree-1 of the Chebyshev smoother: d = c1 d + c2 D^-1 (r - K z)
     bool hasOwn = false;
 };
 
@@ -780,7 +1139,14 @@ struct SolverImpl {
     cudaStream_t stream = nullptr;      // the stream every kernel goes to (own, or the caller's)
     cudaStream_t ownStream = nullptr;
     bool smoothersReady = false;
+    int degree = 2;  // Chebyshev smoother degree (the reference's is 2)
     int64_t launches = 0;     // kernels launched by this handle (graph replays add their kernel count)
+    // FP16 own matrices (mixed precision) are applied to neighbour differences, which keeps rigid
+    // translations in their null space exactly despite the rounding of the entries; the mixed form
+    // may also keep the 32-bit matrices. Tuning knobs: PSFEA_OWN16_DIFF=0, PSFEA_MIXED_OWN32=1.
+    bool ownDiff = false;
+    bool mixedOwn16 = true;
+    double foldFactor = 0.1;  // fold when the FP32 residual is this fraction of its peak (PSFEA_FOLD)
     int64_t graphKernels[2] = {0, 0};
 
     template <class... KArgs, class... Args>
@@ -800,6 +1166,17 @@ struct SolverImpl {
     void build(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsest, const double* diagAdd);
     void uploadLevel(int l);
     void prepareSmoothers();
+    void setDegree(int want) {
+        if (want == degree) return;
+        // new smoother coefficients: the recorded iteration graphs hold the old ones
+        degree = want;
+        smoothersReady = false;
+        for (auto& gg : graph)
+            if (gg) {
+                cudaGraphExecDestroy(gg);
+                gg = nullptr;
+            }
+    }
     double lanczos(int l);
 
     // operator launches
@@ -807,7 +1184,8 @@ struct SolverImpl {
     template <int MODE>
     void op32(int l, const float* x, float* y, float c1, float c2, dev::Ctl ctl, bool own16 = false);
     // V-cycle on level l from L[l].r; returns the buffer holding the result
-    float* vcycle(int l, dev::Ctl ctl, bool own16);
+    // firstDone: L[l].d and L[l].z already hold the first smoothing step (fused upstream)
+    float* vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone = false);
     bool exactOneLevel() const { return L.size() == 1 && H.hasFactor(); }
 
     void recordPlainIteration(dev::Ctl ctl);
@@ -831,9 +1209,25 @@ void SolverImpl::build(const int32_t dims[3], const float* density, double nu, c
     int devId = 0;
     check(cudaGetDevice(&devId), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, devId), "attribute");
+    if (const char* e = std::getenv("PSFEA_OWN16_DIFF")) ownDiff = std::atoi(e) != 0;
+    if (const char* e = std::getenv("PSFEA_FOLD")) foldFactor = std::atof(e);
+    if (const char* e = std::getenv("PSFEA_MIXED_OWN32")) mixedOwn16 = std::atoi(e) == 0;
     check(cudaStreamCreateWithFlags(&ownStream, cudaStreamNonBlocking), "stream");
     stream = ownStream;
     check(cudaMallocHost(&hostState, sizeof(dev::SolveState)), "cudaMallocHost");
+    {
+        // the tiled operator stages more than the default 48 KB of shared memory
+        const int s32 = int(dev::tileSmemBytes<float>()), s64 = int(dev::tileSmemBytes<double>());
+        check(cudaFuncSetAttribute(dev::k_tile<double, dev::TOP_APPLY, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64), "attr");
+        check(cudaFuncSetAttribute(dev::k_tile<double, dev::TOP_DOT, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64), "attr");
+        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_DOT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
+        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_CHEB, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
+        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_CHEB, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
+        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_RESID, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
+        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_RESID, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
+        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_CHEB, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
+        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_RESID, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
+    }
     L.resize(H.levels.size());
     for (int l = 0; l < int(H.levels.size()); l++) uploadLevel(l);
     const HostLevel& L0 = H.levels[0];
@@ -853,7 +1247,9 @@ void SolverImpl::build(const int32_t dims[3], const float* density, double nu, c
         upload(cInv, H.coarseInv, bytes);
     }
     state.alloc(sizeof(dev::SolveState), bytes);
-    partials.alloc(size_t(smCount) * 16 * 4 * sizeof(double) + 4096, bytes);
+    int maxTiles = 0;
+    for (auto& D : L) maxTiles = std::max(maxTiles, D.nTiles);
+    partials.alloc(size_t(std::max(smCount * 16, maxTiles)) * 4 * sizeof(double) + 4096, bytes);
     ticket.alloc(64, bytes);
 }
 
@@ -885,6 +1281,31 @@ void SolverImpl::uploadLevel(int l) {
         upload(D.dadd32, d32, bytes);
     }
     if (l == 0) upload(D.bc, h.bc, bytes);
+    {
+        const int ntx = (h.NX + dev::TX - 1) / dev::TX, nty = (h.NY + dev::TY - 1) / dev::TY, ntz = (h.NZ + dev::TZ - 1) / dev::TZ;
+        if (ntx > 2047 || nty > 2047 || ntz > 1023) throw Error(PS_EINVAL, "grid too large for the tile index");
+        std::vector<uint8_t> act(size_t(ntx) * nty * ntz, 0);
+        for (int k = 0; k < h.NZ; k++)
+            for (int j = 0; j < h.NY; j++) {
+                const uint8_t* row = h.nmask.data() + h.node(0, j, k);
+                for (int i = 0; i < h.NX; i++)
+                    if (row[i] & NM_ACTIVE) act[size_t((i / dev::TX) + ntx * ((j / dev::TY) + size_t(nty) * (k / dev::TZ)))] = 1;
+            }
+        std::vector<uint32_t> list;
+        for (int tz = 0; tz < ntz; tz++)
+            for (int ty = 0; ty < nty; ty++)
+                for (int tx = 0; tx < ntx; tx++)
+                    if (act[size_t(tx + ntx * (ty + size_t(nty) * tz))]) list.push_back(dev::packTile(tx, ty, tz));
+        D.nTiles = int(list.size());
+        upload(D.tiles, list, bytes);
+        // small levels have too few tiles to fill the GPU: one thread per node instead
+        int64_t minNodes = 400000;
+        if (const char* e = std::getenv("PSFEA_TILE_MIN_NODES")) minNodes = std::atoll(e);
+        D.useTiles = h.nNodes >= minNodes;
+        int64_t max8 = 30000;
+        if (const char* e = std::getenv("PSFEA_OP8_MAX_NODES")) max8 = std::atoll(e);
+        D.use8 = !D.useTiles && l > 0 && h.nNodes <= max8;
+    }
     const size_t n = size_t(h.nDof);
     D.r.alloc(n * 4, bytes);
     D.z.alloc(n * 4, bytes);
@@ -913,27 +1334,70 @@ void SolverImpl::uploadLevel(int l) {
 
 void SolverImpl::op64(int l, const double* xin, double* y, bool raw, dev::Ctl ctl) {
     DevLevel& D = L[size_t(l)];
-    launch(dev::k_op<double, dev::OP_APPLY, false>, nodeGrid(D.view.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c64, xin, y, nullptr, nullptr, 0.f,
-                                                                                                         0.f, raw ? 1 : 0, ctl);
+    if (!D.nTiles) return;
+    if (!D.useTiles) {
+        if (D.use8)
+            launch(dev::k_op8<double, dev::OP_APPLY, false, false>, gridFor(D.view.nNodes * 8, 256, smCount * 32), 256, 0, stream, D.view, D.c64, xin,
+                   y, nullptr, nullptr, 0.f, 0.f, raw ? 1 : 0, ctl);
+        else
+            launch(dev::k_op<double, dev::OP_APPLY, false>, nodeGrid(D.view.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c64, xin, y, nullptr,
+                   nullptr, 0.f, 0.f, raw ? 1 : 0, ctl);
+        return;
+    }
+    dev::TileIO<double> io{xin, y, nullptr, nullptr, 0.f, 0.f, raw ? 1 : 0};
+    launch(dev::k_tile<double, dev::TOP_APPLY, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double>(), stream, D.view, D.c64, D.tiles.as<uint32_t>(), io,
+           st(), part(), tick(), ctl);
 }
 
 template <int MODE>
 void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev::Ctl ctl, bool own16) {
     DevLevel& D = L[size_t(l)];
-    const int g = nodeGrid(D.view.nNodes);
-    if (own16 && D.hasOwn)
-        launch(dev::k_op<float, MODE, true>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, D.r.as<float>(), D.d.as<float>(), c1, c2, 0, ctl);
+    if (!D.nTiles) return;
+    if (D.use8) {
+        const int g = gridFor(D.view.nNodes * 8, 256, smCount * 32);
+        float* rr = D.r.as<float>();
+        float* dd = D.d.as<float>();
+        if (own16 && D.hasOwn && ownDiff)
+            launch(dev::k_op8<float, MODE, true, true>, g, 256, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
+        else if (own16 && D.hasOwn)
+            launch(dev::k_op8<float, MODE, true, false>, g, 256, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
+        else
+            launch(dev::k_op8<float, MODE, false, false>, g, 256, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
+        return;
+    }
+    if (!D.useTiles) {
+        const int g = nodeGrid(D.view.nNodes);
+        if (own16 && D.hasOwn && ownDiff)
+            launch(dev::k_op<float, MODE, true, true>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, D.r.as<float>(), D.d.as<float>(), c1,
+                   c2, 0, ctl);
+        else if (own16 && D.hasOwn)
+            launch(dev::k_op<float, MODE, true>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, D.r.as<float>(), D.d.as<float>(), c1, c2, 0,
+                   ctl);
+        else
+            launch(dev::k_op<float, MODE, false>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, D.r.as<float>(), D.d.as<float>(), c1, c2,
+                   0, ctl);
+        return;
+    }
+    dev::TileIO<float> io{xin, y, D.r.as<float>(), D.d.as<float>(), c1, c2, 0};
+    if (own16 && D.hasOwn && ownDiff)
+        launch(dev::k_tile<float, MODE, true, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float>(), stream, D.view, D.c32,
+               D.tiles.as<uint32_t>(), io, st(), part(), tick(), ctl);
+    else if (own16 && D.hasOwn)
+        launch(dev::k_tile<float, MODE, true, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float>(), stream, D.view, D.c32, D.tiles.as<uint32_t>(), io, st(), part(),
+               tick(), ctl);
     else
-        launch(dev::k_op<float, MODE, false>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, D.r.as<float>(), D.d.as<float>(), c1, c2, 0, ctl);
+        launch(dev::k_tile<float, MODE, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float>(), stream, D.view, D.c32, D.tiles.as<uint32_t>(), io, st(), part(),
+               tick(), ctl);
 }
 
 // pre-smoothing from zero, residual, restriction, coarse correction, prolongation, post-smoothing
 // (voxel_fea.cpp:817-828); buffers alternate between the level's z and t
-float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16) {
+float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
     DevLevel& D = L[size_t(l)];
     const HostLevel& h = H.levels[size_t(l)];
     float *z = D.z.as<float>(), *t = D.t.as<float>(), *r = D.r.as<float>(), *d = D.d.as<float>();
-    if (l == int(L.size()) - 1) {
+    const int last = int(L.size()) - 1;
+    if (l == last) {
         if (H.hasFactor()) {
             const int threads = 256, warps = threads / 32;
             const int grid = std::max(1, std::min(smCount * 2, (m + warps - 1) / warps));
@@ -941,7 +1405,8 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16) {
             return z;
         }
         // no factor: 40 damped Jacobi sweeps with the default weight (voxel_fea.cpp:676-678)
-        launch(dev::k_cheb_first, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, r, D.invD.as<float>(), d, z, D.omega, ctl);
+        if (!firstDone)
+            launch(dev::k_cheb_first, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, r, D.invD.as<float>(), d, z, D.omega, ctl);
         float* a = z;
         float* b = t;
         for (int s = 1; s < 40; s++) {
@@ -952,15 +1417,29 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16) {
     }
     DevLevel& C = L[size_t(l + 1)];
     const HostLevel& hc = H.levels[size_t(l + 1)];
-    launch(dev::k_cheb_first, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, r, D.invD.as<float>(), d, z, D.cf0, ctl);
-    op32<dev::OP_CHEB>(l, z, t, D.cf1, D.cf2, ctl, own16);    // t = smoothed
-    op32<dev::OP_RESID>(l, t, z, 0.f, 0.f, ctl, own16);       // z = r - K t
-    launch(dev::k_restrict, gridFor(hc.nNodes, 256, smCount * 16), 256, 0, stream, h.NX, h.NY, h.NZ, C.view, z, C.r.as<float>(), ctl);
-    float* zc = vcycle(l + 1, ctl, own16);
-    launch(dev::k_prolong, gridFor(h.nNodes, 256, smCount * 16), 256, 0, stream, D.view, hc.NX, hc.NY, zc, t, ctl);
-    op32<dev::OP_CHEB>(l, t, z, 0.f, D.cf0, ctl, own16);      // d = c0 D^-1 (r - K t); z = t + d
-    op32<dev::OP_CHEB>(l, z, t, D.cf1, D.cf2, ctl, own16);    // second step
-    return t;
+    if (!firstDone)
+        launch(dev::k_cheb_first, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, r, D.invD.as<float>(), d, z, D.cf0, ctl);
+    float* a = z;  // the current iterate
+    float* b = t;
+    for (size_t k = 0; k < D.chebC1.size(); k++) {  // pre-smoothing from zero
+        op32<dev::OP_CHEB>(l, a, b, D.chebC1[k], D.chebC2[k], ctl, own16);
+        std::swap(a, b);
+    }
+    op32<dev::OP_RESID>(l, a, b, 0.f, 0.f, ctl, own16);  // b = r - K a
+    // restriction, with the coarse level's first smoothing step fused in (unless it is the dense solve)
+    const bool fuse = !(l + 1 == last && H.hasFactor());
+    const float c0c = (l + 1 == last) ? C.omega : C.cf0;
+    launch(dev::k_restrict, gridFor(hc.nNodes, 256, smCount * 16), 256, 0, stream, h.NX, h.NY, h.NZ, C.view, b, C.r.as<float>(),
+           fuse ? C.d.as<float>() : nullptr, fuse ? C.z.as<float>() : nullptr, c0c, ctl);
+    float* zc = vcycle(l + 1, ctl, own16, fuse);
+    launch(dev::k_prolong, gridFor(h.nNodes, 256, smCount * 16), 256, 0, stream, D.view, hc.NX, hc.NY, zc, a, ctl);
+    op32<dev::OP_CHEB>(l, a, b, 0.f, D.cf0, ctl, own16);  // post-smoothing: d = c0 D^-1 (r - K a); b = a + d
+    std::swap(a, b);
+    for (size_t k = 0; k < D.chebC1.size(); k++) {
+        op32<dev::OP_CHEB>(l, a, b, D.chebC1[k], D.chebC2[k], ctl, own16);
+        std::swap(a, b);
+    }
+    return a;
 }
 
 double SolverImpl::lanczos(int l) {
@@ -1004,12 +1483,25 @@ void SolverImpl::prepareSmoothers() {
     for (int l = 0; l + 1 < int(L.size()); l++) {
         HostLevel& h = H.levels[size_t(l)];
         if (!(h.lmax > 0)) h.lmax = lanczos(l);
+        DevLevel& D = L[size_t(l)];
         double c0, c1, c2;
         chebyshevCoefficients(h.lmax, c0, c1, c2);
-        L[size_t(l)].cf0 = float(c0);
-        L[size_t(l)].cf1 = float(c1);
-        L[size_t(l)].cf2 = float(c2);
-        L[size_t(l)].omega = float(1.2 / (h.lmax * 1.05));
+        D.cf0 = float(c0);
+        D.cf1 = float(c1);
+        D.cf2 = float(c2);
+        D.omega = float(1.2 / (h.lmax * 1.05));
+        // the Chebyshev recurrence on [0.1, 1.15] lmax continued to `degree` steps (Adams et al.
+        // 2003); step 1 is the reference's second step (voxel_fea.cpp:692-701)
+        const double b = 1.15 * h.lmax, a = 0.1 * h.lmax, theta = (b + a) / 2, delta = (b - a) / 2, sigma = theta / delta;
+        double rho = 1 / sigma;
+        D.chebC1.clear();
+        D.chebC2.clear();
+        for (int k = 1; k < degree; k++) {
+            const double rn = 1 / (2 * sigma - rho);
+            D.chebC1.push_back(float(rn * rho));
+            D.chebC2.push_back(float(2 * rn / delta));
+            rho = rn;
+        }
     }
     // the coarsest level keeps the default Jacobi weight 0.5 (its eigenvalue is never estimated)
     smoothersReady = true;
@@ -1019,23 +1511,29 @@ void SolverImpl::prepareSmoothers() {
 void SolverImpl::recordPlainIteration(dev::Ctl ctl) {
     const HostLevel& h = H.levels[0];
     DevLevel& D = L[0];
-    launch(dev::k_apply_alpha<double, false>, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c64, p.as<double>(), q.as<double>(), st(),
-                                                                                            part(), tick(), ctl);
+    if (!D.useTiles) {
+        launch(dev::k_apply_alpha<double, false>, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c64, p.as<double>(), q.as<double>(),
+               st(), part(), tick(), ctl);
+    } else {
+        dev::TileIO<double> io{p.as<double>(), q.as<double>(), nullptr, nullptr, 0.f, 0.f, 0};
+        launch(dev::k_tile<double, dev::TOP_DOT, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double>(), stream, D.view, D.c64, D.tiles.as<uint32_t>(), io,
+               st(), part(), tick(), ctl);
+    }
+    const bool one = exactOneLevel();
     launch(dev::k_cg_update, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x.as<double>(), r.as<double>(), p.as<double>(),
-                                                                         q.as<double>(), st(), part(), tick(), ctl);
+           q.as<double>(), one ? nullptr : D.r.as<float>(), D.invD.as<float>(), D.d.as<float>(), D.z.as<float>(), D.cf0, st(), part(), tick(), ctl);
     float* z32 = nullptr;
-    if (exactOneLevel()) {
+    if (one) {
         const int threads = 256, warps = threads / 32;
         const int grid = std::max(1, std::min(smCount * 2, (m + warps - 1) / warps));
         launch(dev::k_coarse<double, double>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(), r.as<double>(),
                                                                                            z64.as<double>(), ctl);
     } else {
-        launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), D.r.as<float>(), st(), ctl);
-        z32 = vcycle(0, ctl, false);
+        z32 = vcycle(0, ctl, false, true);  // r32 and the first smoothing step came with the update
     }
-    launch(dev::k_cg_dots, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, r.as<double>(), z32, z64.as<double>(), q.as<double>(), st(), part(),
-                                                                     tick(), ctl);
-    launch(dev::k_cg_p, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, z32, z64.as<double>(), p.as<double>(), st(), ctl);
+    launch(dev::k_cg_dots, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), z32, z64.as<double>(),
+           q.as<double>(), st(), part(), tick(), ctl);
+    launch(dev::k_cg_p, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, z32, z64.as<double>(), p.as<double>(), st(), ctl);
 }
 
 // one FP32 CG iteration with the FP64 fold (runs only when due)
@@ -1043,8 +1541,14 @@ void SolverImpl::recordMixedIteration(dev::Ctl ctl) {
     const HostLevel& h = H.levels[0];
     DevLevel& D = L[0];
     const int* foldFlag = &st()->fold;
-    launch(dev::k_apply_alpha<float, true>, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c32, p32.as<float>(), q32.as<float>(), st(),
-                                                                                          part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
+    if (!D.useTiles) {
+        launch(dev::k_apply_alpha<float, true>, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c32, p32.as<float>(), q32.as<float>(),
+               st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
+    } else {
+        dev::TileIO<float> io{p32.as<float>(), q32.as<float>(), nullptr, nullptr, 0.f, 0.f, 0};
+        launch(dev::k_tile<float, dev::TOP_DOT, false, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float>(), stream, D.view, D.c32, D.tiles.as<uint32_t>(), io,
+               st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
+    }
     launch(dev::k_mx_update, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x32.as<float>(), D.r.as<float>(), p32.as<float>(),
                                                                          q32.as<float>(), st(), part(), tick(), ctl);
     const dev::Ctl foldCtl{ctl.skipIf, foldFlag};
@@ -1052,7 +1556,7 @@ void SolverImpl::recordMixedIteration(dev::Ctl ctl) {
     op64(0, x.as<double>(), q.as<double>(), false, foldCtl);
     launch(dev::k_mx_fold2, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), D.r.as<float>(),
                                                                         st(), part(), tick(), foldCtl);
-    float* z32 = vcycle(0, ctl, true);
+    float* z32 = vcycle(0, ctl, mixedOwn16);
     launch(dev::k_mx_dots, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, D.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
     launch(dev::k_mx_p, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, z32, p32.as<float>(), st(), ctl);
 }
@@ -1064,6 +1568,7 @@ ps_status SolverImpl::runSolve(const double* fDev, const double* x0Dev, const ps
     DevLevel& D = L[0];
     const bool mixed = o.precision == PS_PREC_MIXED && !exactOneLevel();
     const int64_t n = h.nDof;
+    setDegree(o.smoother_degree > 0 ? o.smoother_degree : 2);
     prepareSmoothers();
     // state
     dev::SolveState s{};
@@ -1071,6 +1576,7 @@ ps_status SolverImpl::runSolve(const double* fDev, const double* x0Dev, const ps
     s.maxIter = o.max_iter;
     s.first = 1;
     s.mixed = mixed ? 1 : 0;
+    s.foldFactor = foldFactor;
     check(cudaMemcpyAsync(state.p, &s, sizeof s, cudaMemcpyHostToDevice, stream), "state");
     if (fDev != f.p) check(cudaMemcpyAsync(f.p, fDev, size_t(n) * 8, cudaMemcpyDeviceToDevice, stream), "f copy");
     launch(dev::k_mask_copy, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x0Dev, x.as<double>());
@@ -1082,8 +1588,9 @@ ps_status SolverImpl::runSolve(const double* fDev, const double* x0Dev, const ps
     // first preconditioned direction
     if (mixed) {
         check(cudaMemsetAsync(x32.p, 0, size_t(n) * 4, stream), "memset");
-        launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), D.r.as<float>(), st(), ctl);
-        float* z32 = vcycle(0, ctl, true);
+        launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), D.r.as<float>(),
+               D.invD.as<float>(), D.d.as<float>(), D.z.as<float>(), D.cf0, st(), ctl);
+        float* z32 = vcycle(0, ctl, mixedOwn16, true);
         launch(dev::k_mx_dots, vecGrid(n), dev::VEC_THREADS, 0, stream, n, D.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
         launch(dev::k_mx_p, vecGrid(n), dev::VEC_THREADS, 0, stream, n, z32, p32.as<float>(), st(), ctl);
     } else {
@@ -1095,12 +1602,13 @@ ps_status SolverImpl::runSolve(const double* fDev, const double* x0Dev, const ps
             launch(dev::k_coarse<double, double>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(),
                                                                                                r.as<double>(), z64.as<double>(), ctl);
         } else {
-            launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), D.r.as<float>(), st(), ctl);
-            z32 = vcycle(0, ctl, false);
+            launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), D.r.as<float>(),
+                   D.invD.as<float>(), D.d.as<float>(), D.z.as<float>(), D.cf0, st(), ctl);
+            z32 = vcycle(0, ctl, false, true);
         }
-        launch(dev::k_cg_dots, vecGrid(n), dev::VEC_THREADS, 0, stream, n, r.as<double>(), z32, z64.as<double>(), q.as<double>(), st(), part(), tick(),
-                                                                    ctl);
-        launch(dev::k_cg_p, vecGrid(n), dev::VEC_THREADS, 0, stream, n, z32, z64.as<double>(), p.as<double>(), st(), ctl);
+        launch(dev::k_cg_dots, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), z32, z64.as<double>(),
+               q.as<double>(), st(), part(), tick(), ctl);
+        launch(dev::k_cg_p, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, z32, z64.as<double>(), p.as<double>(), st(), ctl);
     }
     launch(dev::k_clear_first, 1, 1, 0, stream, st());
     check(cudaGetLastError(), "solve setup");
@@ -1239,6 +1747,7 @@ void Solver::precondition(const double* rHost, double* zHost) {
     const HostLevel& h = I.H.levels[0];
     DevLevel& D = I.L[0];
     const int64_t n = h.nDof;
+    I.setDegree(2);  // the reference's preconditioner
     I.prepareSmoothers();
     check(cudaMemcpyAsync(I.r.p, rHost, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "r upload");
     const dev::Ctl none{nullptr, nullptr};
@@ -1252,9 +1761,9 @@ void Solver::precondition(const double* rHost, double* zHost) {
         check(cudaMemcpyAsync(zHost, I.z64.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "z download");
     } else {
         I.launch(dev::k_rmax, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, I.r.as<double>(), I.st(), I.part(), I.tick());
-        I.launch(dev::k_vc_load, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, I.r.as<double>(), D.r.as<float>(), I.st(),
-                                                                               none);
-        float* z32 = I.vcycle(0, none, false);
+        I.launch(dev::k_vc_load, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, I.r.as<double>(), D.r.as<float>(),
+                 D.invD.as<float>(), D.d.as<float>(), D.z.as<float>(), D.cf0, I.st(), none);
+        float* z32 = I.vcycle(0, none, false, true);
         I.launch(dev::k_vc_store, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, z32, I.q.as<double>(), I.st());
         check(cudaMemcpyAsync(zHost, I.q.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "z download");
     }
@@ -1302,6 +1811,7 @@ void Solver::apply(int level, const double* xHost, double* yHost, bool raw) {
     if (level < 0 || level >= int(I.L.size())) throw Error(PS_EINVAL, "level out of range");
     const int64_t n = I.H.levels[size_t(level)].nDof;
     check(cudaMemcpyAsync(I.p.p, xHost, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "x upload");
+    check(cudaMemsetAsync(I.q.p, 0, size_t(n) * 8, I.stream), "memset");  // inactive tiles are not written
     I.op64(level, I.p.as<double>(), I.q.as<double>(), raw, dev::Ctl{nullptr, nullptr});
     check(cudaMemcpyAsync(yHost, I.q.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "y download");
     check(cudaStreamSynchronize(I.stream), "apply");
@@ -1334,6 +1844,7 @@ void Solver::reactions(const double* u, const double* f, double R[3]) {
     const int64_t n = L0.nDof;
     check(cudaMemcpyAsync(I.p.p, u, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "u upload");
     if (f) check(cudaMemcpyAsync(I.r.p, f, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "f upload");
+    check(cudaMemsetAsync(I.q.p, 0, size_t(n) * 8, I.stream), "memset");
     I.op64(0, I.p.as<double>(), I.q.as<double>(), true, dev::Ctl{nullptr, nullptr});
     I.launch(dev::k_reactions, I.vecGrid(L0.nNodes), dev::VEC_THREADS, 0, I.stream, L0.nNodes, I.L[0].view.nmask, I.L[0].bc.as<uint8_t>(), I.q.as<double>(),
                                                                                f ? I.r.as<double>() : nullptr, I.st(), I.part(), I.tick());

@@ -24,7 +24,7 @@ STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "CANCELLED", 4: 
 
 class SolveOpts(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iter", C.c_int32), ("precision", C.c_int32), ("x0", C.c_void_p),
-                ("cancel", C.c_void_p), ("time_limit_s", C.c_double)]
+                ("cancel", C.c_void_p), ("time_limit_s", C.c_double), ("smoother_degree", C.c_int32)]
 
 
 class SolveResultC(C.Structure):
@@ -127,7 +127,7 @@ class SolveResult:
         return self.status == PS_CANCELLED
 
 
-def make_opts(tol=1e-6, max_iter=500, precision="fp64", x0=None, cancel=None, time_limit_s=0.0):
+def make_opts(tol=1e-6, max_iter=500, precision="fp64", x0=None, cancel=None, time_limit_s=0.0, smoother_degree=0):
     o = SolveOpts()
     _opts_default(C.byref(o))
     o.tol = float(tol)
@@ -136,6 +136,7 @@ def make_opts(tol=1e-6, max_iter=500, precision="fp64", x0=None, cancel=None, ti
     o.x0 = x0
     o.cancel = cancel
     o.time_limit_s = float(time_limit_s)
+    o.smoother_degree = int(smoother_degree)
     return o
 
 
@@ -210,11 +211,11 @@ class VoxelFEA:
             raise ValueError("Force or displacement vector has the wrong size.")
         return v
 
-    def solve(self, f, tol=1e-6, max_iter=500, x0=None, precision="fp64", cancel=None, time_limit_s=0.0):
+    def solve(self, f, tol=1e-6, max_iter=500, x0=None, precision="fp64", cancel=None, time_limit_s=0.0, smoother_degree=0):
         """K u = f; returns a SolveResult (u in normalised units: u_phys = u / (E h))."""
         f = self._check_vec(f, "f")
         x0a = None if x0 is None else self._check_vec(x0, "x0")
-        o = make_opts(tol, max_iter, precision, _ptr(x0a), None if cancel is None else C.addressof(cancel), time_limit_s)
+        o = make_opts(tol, max_iter, precision, _ptr(x0a), None if cancel is None else C.addressof(cancel), time_limit_s, smoother_degree)
         u = np.zeros(self.n_dof, np.float64)
         r = SolveResultC()
         st = _solve(self.h, f, C.byref(o), u, C.byref(r))
@@ -222,9 +223,9 @@ class VoxelFEA:
             _raise(st)
         return SolveResult(u, r.iterations, r.residual, bool(r.converged), st, r.folds, r.seconds, r.kernels)
 
-    def solve_dev(self, f_ptr, u_ptr, tol=1e-6, max_iter=500, precision="fp64", x0_ptr=None):
+    def solve_dev(self, f_ptr, u_ptr, tol=1e-6, max_iter=500, precision="fp64", x0_ptr=None, smoother_degree=0):
         """The solve on device pointers (e.g. ``tensor.data_ptr()`` of CUDA float64 tensors)."""
-        o = make_opts(tol, max_iter, precision, x0_ptr)
+        o = make_opts(tol, max_iter, precision, x0_ptr, smoother_degree=smoother_degree)
         r = SolveResultC()
         st = _solve_dev(self.h, C.c_void_p(f_ptr), C.byref(o), C.c_void_p(u_ptr), C.byref(r))
         if st >= PS_EINVAL:
