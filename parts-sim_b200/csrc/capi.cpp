@@ -1,6 +1,7 @@
 // The C ABI of include/ps_fea.h: validation with the reference's messages, exceptions mapped to
 // status codes, and the per-thread last-error string.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -108,17 +109,13 @@ ps_status ps_fea_solve_batch(ps_fea_t* h, int32_t nrhs, const double* f, const p
     return guarded([&] {
         if (!h || !f || !u_out || nrhs < 0) return fail(PS_EINVAL, "Force or displacement vector has the wrong size.");
         const ps_solve_opts base = resolve(opts);
-        const int64_t n = h->solver.nDof();
-        ps_status worst = PS_OK;
-        for (int32_t q = 0; q < nrhs; q++) {
-            ps_solve_opts o = base;
-            if (base.x0) o.x0 = base.x0 + q * n;
-            ps_solve_result r{};
-            const ps_status s = h->solver.solve(f + q * n, o, u_out + q * n, r);
-            if (results) results[q] = r;
-            if (s > worst) worst = s;
-        }
-        return worst;
+        if (!(base.tol >= 0) || base.max_iter < 0 || (base.precision != PS_PREC_FP64 && base.precision != PS_PREC_MIXED) ||
+            base.smoother_degree < 0 || base.smoother_degree > 8)
+            return fail(PS_EINVAL, "invalid solve options");
+        if (nrhs == 0) return PS_OK;
+        int concurrency = 8;
+        if (const char* e = std::getenv("PSFEA_BATCH_CONCURRENCY")) concurrency = std::max(1, std::atoi(e));
+        return h->solver.solveBatch(nrhs, f, base, u_out, results, concurrency);
     });
 }
 

@@ -23,7 +23,9 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <memory>
 #include <mutex>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -916,9 +918,10 @@ __global__ void k_lz_x(long long n, const double* __restrict__ invD, const doubl
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) x[i] = sqrt(invD[i]) * v[i];
 }
 
-// w = sq w - b vp; alpha = w . v
+// w = sq w - b vp (b = |w| of the previous step, 0 on the first); alpha = w . v into *aOut
 __global__ void k_lz_w(long long n, const double* __restrict__ invD, double* __restrict__ w, const double* __restrict__ v,
-                       const double* __restrict__ vp, double b, SolveState* st, double* partials, unsigned* ticket) {
+                       const double* __restrict__ vp, const double* bPrev, double* aOut, SolveState* st, double* partials, unsigned* ticket) {
+    const double b = bPrev ? *bPrev : 0.0;
     double acc[1] = {0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const double wv = sqrt(invD[i]) * w[i] - b * vp[i];
@@ -926,13 +929,13 @@ __global__ void k_lz_w(long long n, const double* __restrict__ invD, double* __r
         acc[0] += wv * v[i];
     }
     double tot[1];
-    if (gridReduce<1>(acc, 0u, partials, ticket, tot) && threadIdx.x == 0) st->alpha = tot[0];
+    if (gridReduce<1>(acc, 0u, partials, ticket, tot) && threadIdx.x == 0) *aOut = tot[0];
 }
 
-// w -= alpha v; beta^2 = w . w
-__global__ void k_lz_axpy(long long n, double* __restrict__ w, const double* __restrict__ v, SolveState* st, double* partials,
-                          unsigned* ticket) {
-    const double a = st->alpha;
+// w -= alpha v; |w| into *bOut
+__global__ void k_lz_axpy(long long n, double* __restrict__ w, const double* __restrict__ v, const double* aIn, double* bOut, SolveState* st,
+                          double* partials, unsigned* ticket) {
+    const double a = *aIn;
     double acc[1] = {0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const double wv = w[i] - a * v[i];
@@ -940,10 +943,12 @@ __global__ void k_lz_axpy(long long n, double* __restrict__ w, const double* __r
         acc[0] += wv * wv;
     }
     double tot[1];
-    if (gridReduce<1>(acc, 0u, partials, ticket, tot) && threadIdx.x == 0) st->beta = tot[0];
+    if (gridReduce<1>(acc, 0u, partials, ticket, tot) && threadIdx.x == 0) *bOut = sqrt(tot[0]);
 }
 
-__global__ void k_lz_next(long long n, const double* __restrict__ w, double* __restrict__ v, double* __restrict__ vp, double b) {
+// vp = v; v = w / b (after the sequence has stopped these values are never used)
+__global__ void k_lz_next(long long n, const double* __restrict__ w, double* __restrict__ v, double* __restrict__ vp, const double* bIn) {
+    const double b = *bIn;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         vp[i] = v[i];
         v[i] = w[i] / b;
@@ -1108,12 +1113,12 @@ int gridFor(int64_t n, int threads, int cap) {
 
 }  // namespace
 
+// Read-only device data of one level, shared by every solve context of a handle.
 struct DevLevel {
     dev::LevelView view{};
     dev::Coefs<double> c64{};
     dev::Coefs<float> c32{};
-    DevMem word, nmask, own, own16, invD, invD64, dadd, dadd32, bc;
-    DevMem r, z, t, d;
+    DevMem word, nmask, own, own16, invD, dadd, dadd32, bc;
     DevMem tiles;      // packed (tx, ty, tz) of the 32 x 8 x 4 node tiles with an active node
     int nTiles = 0;
     bool useTiles = false;  // tiled kernel (large levels) or one thread per node (small ones)
@@ -1123,88 +1128,37 @@ struct DevLevel {
     bool hasOwn = false;
 };
 
-struct SolverImpl {
+// The V-cycle work vectors of one level in one solve context.
+struct LevelWork {
+    DevMem r, z, t, d;
+};
+
+// The hierarchy on the device: built once per handle, shared by its solve contexts.
+struct SharedModel {
     Hierarchy H;
     std::vector<DevLevel> L;
+    DevMem cDof, cInv;  // coarsest level: free DOF list, dense FP64 inverse
+    int m = 0;
     int64_t bytes = 0;
     int smCount = 148;
-    // coarsest
-    DevMem cDof, cInv;
-    int m = 0;
-    // finest-level FP64 work vectors and FP32 mixed-precision ones
-    DevMem f, x, r, p, q, z64, x32, p32, q32, tmp;
-    // control
-    DevMem state, partials, ticket;
-    dev::SolveState* hostState = nullptr;  // pinned mirror
-    cudaStream_t stream = nullptr;      // the stream every kernel goes to (own, or the caller's)
-    cudaStream_t ownStream = nullptr;
+    int maxTiles = 0;
+    // smoother coefficients (shared; `version` changes whenever they do, so contexts re-record)
     bool smoothersReady = false;
     int degree = 2;  // Chebyshev smoother degree (the reference's is 2)
-    int64_t launches = 0;     // kernels launched by this handle (graph replays add their kernel count)
-    // FP16 own matrices (mixed precision) are applied to neighbour differences, which keeps rigid
+    int64_t version = 0;
+    // FP16 own matrices (mixed precision) may be applied to neighbour differences, keeping rigid
     // translations in their null space exactly despite the rounding of the entries; the mixed form
-    // may also keep the 32-bit matrices. Tuning knobs: PSFEA_OWN16_DIFF=0, PSFEA_MIXED_OWN32=1.
+    // may also keep the 32-bit matrices. Tuning knobs: PSFEA_OWN16_DIFF, PSFEA_MIXED_OWN32, PSFEA_FOLD.
     bool ownDiff = false;
     bool mixedOwn16 = true;
-    double foldFactor = 0.1;  // fold when the FP32 residual is this fraction of its peak (PSFEA_FOLD)
-    int64_t graphKernels[2] = {0, 0};
-
-    template <class... KArgs, class... Args>
-    void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
-        kernel<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
-        ++launches;
-    }
-    // graphs of one iteration, per precision
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-
-    int nodeGrid(int64_t nNodes) const { return gridFor(nNodes, dev::NODE_THREADS, smCount * 16); }
-    int vecGrid(int64_t n) const { return gridFor(n, dev::VEC_THREADS, smCount * 8); }
-    dev::SolveState* st() const { return state.as<dev::SolveState>(); }
-    double* part() const { return partials.as<double>(); }
-    unsigned* tick() const { return ticket.as<unsigned>(); }
+    double foldFactor = 0.1;  // fold when the FP32 residual is this fraction of its peak
 
     void build(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsest, const double* diagAdd);
     void uploadLevel(int l);
-    void prepareSmoothers();
-    void setDegree(int want) {
-        if (want == degree) return;
-        // new smoother coefficients: the recorded iteration graphs hold the old ones
-        degree = want;
-        smoothersReady = false;
-        for (auto& gg : graph)
-            if (gg) {
-                cudaGraphExecDestroy(gg);
-                gg = nullptr;
-            }
-    }
-    double lanczos(int l);
-
-    // operator launches
-    void op64(int l, const double* x, double* y, bool raw, dev::Ctl ctl);
-    template <int MODE>
-    void op32(int l, const float* x, float* y, float c1, float c2, dev::Ctl ctl, bool own16 = false);
-    // V-cycle on level l from L[l].r; returns the buffer holding the result
-    // firstDone: L[l].d and L[l].z already hold the first smoothing step (fused upstream)
-    float* vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone = false);
     bool exactOneLevel() const { return L.size() == 1 && H.hasFactor(); }
-
-    void recordPlainIteration(dev::Ctl ctl);
-    void recordMixedIteration(dev::Ctl ctl);
-    ps_status runSolve(const double* fDev, const double* x0Dev, const ps_solve_opts& o, double* uDev, ps_solve_result& res);
-    void readState() {
-        check(cudaMemcpyAsync(hostState, state.p, sizeof(dev::SolveState), cudaMemcpyDeviceToHost, stream), "state read");
-        check(cudaStreamSynchronize(stream), "sync");
-    }
-
-    ~SolverImpl() {
-        for (auto& g : graph)
-            if (g) cudaGraphExecDestroy(g);
-        if (hostState) cudaFreeHost(hostState);
-        if (ownStream) cudaStreamDestroy(ownStream);
-    }
 };
 
-void SolverImpl::build(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsest, const double* diagAdd) {
+void SharedModel::build(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsest, const double* diagAdd) {
     H = buildHierarchy(dims, density, nu, bc, coarsest, diagAdd);
     int devId = 0;
     check(cudaGetDevice(&devId), "cudaGetDevice");
@@ -1212,9 +1166,6 @@ void SolverImpl::build(const int32_t dims[3], const float* density, double nu, c
     if (const char* e = std::getenv("PSFEA_OWN16_DIFF")) ownDiff = std::atoi(e) != 0;
     if (const char* e = std::getenv("PSFEA_FOLD")) foldFactor = std::atof(e);
     if (const char* e = std::getenv("PSFEA_MIXED_OWN32")) mixedOwn16 = std::atoi(e) == 0;
-    check(cudaStreamCreateWithFlags(&ownStream, cudaStreamNonBlocking), "stream");
-    stream = ownStream;
-    check(cudaMallocHost(&hostState, sizeof(dev::SolveState)), "cudaMallocHost");
     {
         // the tiled operator stages more than the default 48 KB of shared memory
         const int s32 = int(dev::tileSmemBytes<float>()), s64 = int(dev::tileSmemBytes<double>());
@@ -1230,30 +1181,15 @@ void SolverImpl::build(const int32_t dims[3], const float* density, double nu, c
     }
     L.resize(H.levels.size());
     for (int l = 0; l < int(H.levels.size()); l++) uploadLevel(l);
-    const HostLevel& L0 = H.levels[0];
-    const size_t n = size_t(L0.nDof);
-    f.alloc(n * 8, bytes);
-    x.alloc(n * 8, bytes);
-    r.alloc(n * 8, bytes);
-    p.alloc(n * 8, bytes);
-    q.alloc(n * 8, bytes);
-    if (exactOneLevel()) z64.alloc(n * 8, bytes);
-    x32.alloc(n * 4, bytes);
-    p32.alloc(n * 4, bytes);
-    q32.alloc(n * 4, bytes);
     m = int(H.coarseM);
     if (H.hasFactor()) {
         upload(cDof, H.coarseDof, bytes);
         upload(cInv, H.coarseInv, bytes);
     }
-    state.alloc(sizeof(dev::SolveState), bytes);
-    int maxTiles = 0;
     for (auto& D : L) maxTiles = std::max(maxTiles, D.nTiles);
-    partials.alloc(size_t(std::max(smCount * 16, maxTiles)) * 4 * sizeof(double) + 4096, bytes);
-    ticket.alloc(64, bytes);
 }
 
-void SolverImpl::uploadLevel(int l) {
+void SharedModel::uploadLevel(int l) {
     const HostLevel& h = H.levels[size_t(l)];
     DevLevel& D = L[size_t(l)];
     upload(D.word, h.word, bytes);
@@ -1298,7 +1234,8 @@ void SolverImpl::uploadLevel(int l) {
                     if (act[size_t(tx + ntx * (ty + size_t(nty) * tz))]) list.push_back(dev::packTile(tx, ty, tz));
         D.nTiles = int(list.size());
         upload(D.tiles, list, bytes);
-        // small levels have too few tiles to fill the GPU: one thread per node instead
+        // small levels have too few tiles to fill the GPU: one thread per node instead, or eight
+        // lanes per node on the smallest ones
         int64_t minNodes = 400000;
         if (const char* e = std::getenv("PSFEA_TILE_MIN_NODES")) minNodes = std::atoll(e);
         D.useTiles = h.nNodes >= minNodes;
@@ -1306,11 +1243,6 @@ void SolverImpl::uploadLevel(int l) {
         if (const char* e = std::getenv("PSFEA_OP8_MAX_NODES")) max8 = std::atoll(e);
         D.use8 = !D.useTiles && l > 0 && h.nNodes <= max8;
     }
-    const size_t n = size_t(h.nDof);
-    D.r.alloc(n * 4, bytes);
-    D.z.alloc(n * 4, bytes);
-    D.t.alloc(n * 4, bytes);
-    D.d.alloc(n * 4, bytes);
     dev::LevelView& v = D.view;
     v.nx = h.nx; v.ny = h.ny; v.nz = h.nz; v.NX = h.NX; v.NY = h.NY; v.NZ = h.NZ;
     v.nNodes = h.nNodes;
@@ -1332,6 +1264,140 @@ void SolverImpl::uploadLevel(int l) {
         }
 }
 
+// One solve context: work vectors, control state, stream and recorded iteration graphs over a
+// shared hierarchy. A handle has one; concurrent batch solves add more.
+struct SolverImpl {
+    std::shared_ptr<SharedModel> M;
+    Hierarchy& H;
+    std::vector<DevLevel>& L;
+    DevMem& cDof;
+    DevMem& cInv;
+    const int& m;
+    int smCount;
+    std::vector<LevelWork> W;
+    // finest-level FP64 work vectors and FP32 mixed-precision ones
+    DevMem f, x, r, p, q, z64, x32, p32, q32;
+    // control
+    DevMem state, partials, ticket;
+    int64_t bytes = 0;
+    dev::SolveState* hostState = nullptr;  // pinned mirror
+    cudaStream_t stream = nullptr;      // the stream every kernel goes to (own, or the caller's)
+    cudaStream_t ownStream = nullptr;
+    cudaEvent_t ev = nullptr;           // recorded after each asynchronous state read
+    int64_t launches = 0;     // kernels launched by this context (graph replays add their kernel count)
+    // graphs of one iteration, per precision, and the coefficient version they were recorded with
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int64_t graphKernels[2] = {0, 0};
+    int64_t graphVersion[2] = {-1, -1};
+
+    // the solve in progress (a resumable state machine, so one host thread can drive many)
+    struct Pending {
+        bool active = false, finishing = false, mixed = false;
+        ps_solve_opts o{};
+        double* uDev = nullptr;
+        double* uHost = nullptr;
+        std::chrono::steady_clock::time_point t0;
+        int batch = 2;
+        double lastRel = 0;
+        int lastIt = 0;
+        ps_status outcome = PS_OK;
+        int64_t launches0 = 0;
+    } pend;
+
+    explicit SolverImpl(std::shared_ptr<SharedModel> model)
+        : M(std::move(model)), H(M->H), L(M->L), cDof(M->cDof), cInv(M->cInv), m(M->m), smCount(M->smCount) {}
+    void allocate();
+
+    template <class... KArgs, class... Args>
+    void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+        kernel<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+        ++launches;
+    }
+
+    int nodeGrid(int64_t nNodes) const { return gridFor(nNodes, dev::NODE_THREADS, smCount * 16); }
+    int vecGrid(int64_t n) const { return gridFor(n, dev::VEC_THREADS, smCount * 8); }
+    dev::SolveState* st() const { return state.as<dev::SolveState>(); }
+    double* part() const { return partials.as<double>(); }
+    unsigned* tick() const { return ticket.as<unsigned>(); }
+
+    void prepareSmoothers();
+    void setDegree(int want) {
+        if (want == M->degree) return;
+        M->degree = want;
+        M->smoothersReady = false;
+    }
+    double lanczos(int l);
+
+    // operator launches
+    void op64(int l, const double* x, double* y, bool raw, dev::Ctl ctl);
+    template <int MODE>
+    void op32(int l, const float* x, float* y, float c1, float c2, dev::Ctl ctl, bool own16 = false);
+    // V-cycle on level l from W[l].r; returns the buffer holding the result
+    // firstDone: W[l].d and W[l].z already hold the first smoothing step (fused upstream)
+    float* vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone = false);
+    bool exactOneLevel() const { return M->exactOneLevel(); }
+
+    void recordPlainIteration(dev::Ctl ctl);
+    void recordMixedIteration(dev::Ctl ctl);
+    // enqueue a solve (f, x0, u in device memory; uHost, if set, receives u as well)
+    void startSolve(const double* fDev, const double* x0Dev, const ps_solve_opts& o, double* uDev, double* uHost);
+    // move the solve on; returns true (and fills res) once it has finished. block: wait for the
+    // GPU instead of returning when it is still busy.
+    bool advance(bool block, ps_solve_result& res);
+    ps_status runSolve(const double* fDev, const double* x0Dev, const ps_solve_opts& o, double* uDev, ps_solve_result& res) {
+        startSolve(fDev, x0Dev, o, uDev, nullptr);
+        while (!advance(true, res)) {
+        }
+        return ps_status(res.status);
+    }
+    void enqueueStateRead() {
+        check(cudaMemcpyAsync(hostState, state.p, sizeof(dev::SolveState), cudaMemcpyDeviceToHost, stream), "state read");
+        check(cudaEventRecord(ev, stream), "event");
+    }
+    void readState() {
+        enqueueStateRead();
+        check(cudaEventSynchronize(ev), "sync");
+    }
+
+    ~SolverImpl() {
+        // a caller's stream (setStream) may already be gone: wait for this context's own one only
+        if (ownStream) cudaStreamSynchronize(ownStream);
+        for (auto& g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        if (ev) cudaEventDestroy(ev);
+        if (hostState) cudaFreeHost(hostState);
+        if (ownStream) cudaStreamDestroy(ownStream);
+    }
+};
+
+void SolverImpl::allocate() {
+    check(cudaStreamCreateWithFlags(&ownStream, cudaStreamNonBlocking), "stream");
+    stream = ownStream;
+    check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+    check(cudaMallocHost(&hostState, sizeof(dev::SolveState)), "cudaMallocHost");
+    W.resize(H.levels.size());
+    for (size_t l = 0; l < W.size(); l++) {
+        const size_t n = size_t(H.levels[l].nDof);
+        W[l].r.alloc(n * 4, bytes);
+        W[l].z.alloc(n * 4, bytes);
+        W[l].t.alloc(n * 4, bytes);
+        W[l].d.alloc(n * 4, bytes);
+    }
+    const size_t n = size_t(H.levels[0].nDof);
+    f.alloc(n * 8, bytes);
+    x.alloc(n * 8, bytes);
+    r.alloc(n * 8, bytes);
+    p.alloc(n * 8, bytes);
+    q.alloc(n * 8, bytes);
+    if (exactOneLevel()) z64.alloc(n * 8, bytes);
+    x32.alloc(n * 4, bytes);
+    p32.alloc(n * 4, bytes);
+    q32.alloc(n * 4, bytes);
+    state.alloc(sizeof(dev::SolveState), bytes);
+    partials.alloc(size_t(std::max(smCount * 16, M->maxTiles)) * 4 * sizeof(double) + 4096, bytes);
+    ticket.alloc(64, bytes);
+}
+
 void SolverImpl::op64(int l, const double* xin, double* y, bool raw, dev::Ctl ctl) {
     DevLevel& D = L[size_t(l)];
     if (!D.nTiles) return;
@@ -1345,49 +1411,37 @@ void SolverImpl::op64(int l, const double* xin, double* y, bool raw, dev::Ctl ct
         return;
     }
     dev::TileIO<double> io{xin, y, nullptr, nullptr, 0.f, 0.f, raw ? 1 : 0};
-    launch(dev::k_tile<double, dev::TOP_APPLY, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double>(), stream, D.view, D.c64, D.tiles.as<uint32_t>(), io,
-           st(), part(), tick(), ctl);
+    launch(dev::k_tile<double, dev::TOP_APPLY, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double>(), stream, D.view, D.c64,
+           D.tiles.as<uint32_t>(), io, st(), part(), tick(), ctl);
 }
 
 template <int MODE>
 void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev::Ctl ctl, bool own16) {
     DevLevel& D = L[size_t(l)];
     if (!D.nTiles) return;
+    float* rr = W[size_t(l)].r.as<float>();
+    float* dd = W[size_t(l)].d.as<float>();
+    const bool o16 = own16 && D.hasOwn, diff = o16 && M->ownDiff;
     if (D.use8) {
         const int g = gridFor(D.view.nNodes * 8, 256, smCount * 32);
-        float* rr = D.r.as<float>();
-        float* dd = D.d.as<float>();
-        if (own16 && D.hasOwn && ownDiff)
-            launch(dev::k_op8<float, MODE, true, true>, g, 256, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
-        else if (own16 && D.hasOwn)
-            launch(dev::k_op8<float, MODE, true, false>, g, 256, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
-        else
-            launch(dev::k_op8<float, MODE, false, false>, g, 256, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
+        if (diff) launch(dev::k_op8<float, MODE, true, true>, g, 256, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
+        else if (o16) launch(dev::k_op8<float, MODE, true, false>, g, 256, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
+        else launch(dev::k_op8<float, MODE, false, false>, g, 256, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
         return;
     }
     if (!D.useTiles) {
         const int g = nodeGrid(D.view.nNodes);
-        if (own16 && D.hasOwn && ownDiff)
-            launch(dev::k_op<float, MODE, true, true>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, D.r.as<float>(), D.d.as<float>(), c1,
-                   c2, 0, ctl);
-        else if (own16 && D.hasOwn)
-            launch(dev::k_op<float, MODE, true>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, D.r.as<float>(), D.d.as<float>(), c1, c2, 0,
-                   ctl);
-        else
-            launch(dev::k_op<float, MODE, false>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, D.r.as<float>(), D.d.as<float>(), c1, c2,
-                   0, ctl);
+        if (diff) launch(dev::k_op<float, MODE, true, true>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
+        else if (o16) launch(dev::k_op<float, MODE, true>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
+        else launch(dev::k_op<float, MODE, false>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
         return;
     }
-    dev::TileIO<float> io{xin, y, D.r.as<float>(), D.d.as<float>(), c1, c2, 0};
-    if (own16 && D.hasOwn && ownDiff)
-        launch(dev::k_tile<float, MODE, true, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float>(), stream, D.view, D.c32,
-               D.tiles.as<uint32_t>(), io, st(), part(), tick(), ctl);
-    else if (own16 && D.hasOwn)
-        launch(dev::k_tile<float, MODE, true, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float>(), stream, D.view, D.c32, D.tiles.as<uint32_t>(), io, st(), part(),
-               tick(), ctl);
-    else
-        launch(dev::k_tile<float, MODE, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float>(), stream, D.view, D.c32, D.tiles.as<uint32_t>(), io, st(), part(),
-               tick(), ctl);
+    dev::TileIO<float> io{xin, y, rr, dd, c1, c2, 0};
+    const size_t sm = dev::tileSmemBytes<float>();
+    const uint32_t* tl = D.tiles.as<uint32_t>();
+    if (diff) launch(dev::k_tile<float, MODE, true, true>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, io, st(), part(), tick(), ctl);
+    else if (o16) launch(dev::k_tile<float, MODE, true, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, io, st(), part(), tick(), ctl);
+    else launch(dev::k_tile<float, MODE, false, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, io, st(), part(), tick(), ctl);
 }
 
 // pre-smoothing from zero, residual, restriction, coarse correction, prolongation, post-smoothing
@@ -1395,7 +1449,8 @@ void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev
 float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
     DevLevel& D = L[size_t(l)];
     const HostLevel& h = H.levels[size_t(l)];
-    float *z = D.z.as<float>(), *t = D.t.as<float>(), *r = D.r.as<float>(), *d = D.d.as<float>();
+    LevelWork& Wl = W[size_t(l)];
+    float *z = Wl.z.as<float>(), *t = Wl.t.as<float>(), *r = Wl.r.as<float>(), *d = Wl.d.as<float>();
     const int last = int(L.size()) - 1;
     if (l == last) {
         if (H.hasFactor()) {
@@ -1416,6 +1471,7 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
         return a;
     }
     DevLevel& C = L[size_t(l + 1)];
+    LevelWork& Wc = W[size_t(l + 1)];
     const HostLevel& hc = H.levels[size_t(l + 1)];
     if (!firstDone)
         launch(dev::k_cheb_first, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, r, D.invD.as<float>(), d, z, D.cf0, ctl);
@@ -1429,8 +1485,8 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
     // restriction, with the coarse level's first smoothing step fused in (unless it is the dense solve)
     const bool fuse = !(l + 1 == last && H.hasFactor());
     const float c0c = (l + 1 == last) ? C.omega : C.cf0;
-    launch(dev::k_restrict, gridFor(hc.nNodes, 256, smCount * 16), 256, 0, stream, h.NX, h.NY, h.NZ, C.view, b, C.r.as<float>(),
-           fuse ? C.d.as<float>() : nullptr, fuse ? C.z.as<float>() : nullptr, c0c, ctl);
+    launch(dev::k_restrict, gridFor(hc.nNodes, 256, smCount * 16), 256, 0, stream, h.NX, h.NY, h.NZ, C.view, b, Wc.r.as<float>(),
+           fuse ? Wc.d.as<float>() : nullptr, fuse ? Wc.z.as<float>() : nullptr, c0c, ctl);
     float* zc = vcycle(l + 1, ctl, own16, fuse);
     launch(dev::k_prolong, gridFor(h.nNodes, 256, smCount * 16), 256, 0, stream, D.view, hc.NX, hc.NY, zc, a, ctl);
     op32<dev::OP_CHEB>(l, a, b, 0.f, D.cf0, ctl, own16);  // post-smoothing: d = c0 D^-1 (r - K a); b = a + d
@@ -1442,36 +1498,43 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
     return a;
 }
 
+// 10 Lanczos steps on D^-1/2 K D^-1/2 from the reference's LCG start vector (voxel_fea.cpp:579-610),
+// all on the device; the scalars come back once at the end and the host applies the reference's
+// stop rule (b <= 1e-12 |a| ends the sequence; later steps are ignored)
 double SolverImpl::lanczos(int l) {
     DevLevel& D = L[size_t(l)];
     const HostLevel& h = H.levels[size_t(l)];
     const int64_t n = h.nDof;
     int64_t scratch = 0;
-    DevMem v, vp, w, xx, invD;
+    DevMem v, vp, w, xx, invD, ab;
     v.alloc(size_t(n) * 8, scratch);
     vp.alloc(size_t(n) * 8, scratch);
     w.alloc(size_t(n) * 8, scratch);
     xx.alloc(size_t(n) * 8, scratch);
+    ab.alloc(20 * sizeof(double), scratch);
     upload(invD, h.invDiag, scratch);
     const int vg = vecGrid(n);
     launch(dev::k_lz_start, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, h.nNodes, D.view.nmask, v.as<double>(), part(), tick(), st());
     launch(dev::k_scale, vg, dev::VEC_THREADS, 0, stream, n, v.as<double>(), st());
-    std::vector<double> alpha, beta;
-    double b = 0;
     const dev::Ctl none{nullptr, nullptr};
+    double* abp = ab.as<double>();
     for (int s = 0; s < 10; s++) {
         launch(dev::k_lz_x, vg, dev::VEC_THREADS, 0, stream, n, invD.as<double>(), v.as<double>(), xx.as<double>());
         op64(l, xx.as<double>(), w.as<double>(), false, none);
-        launch(dev::k_lz_w, vg, dev::VEC_THREADS, 0, stream, n, invD.as<double>(), w.as<double>(), v.as<double>(), vp.as<double>(), b, st(), part(),
-                                                          tick());
-        launch(dev::k_lz_axpy, vg, dev::VEC_THREADS, 0, stream, n, w.as<double>(), v.as<double>(), st(), part(), tick());
-        readState();
-        const double a = hostState->alpha;
+        launch(dev::k_lz_w, vg, dev::VEC_THREADS, 0, stream, n, invD.as<double>(), w.as<double>(), v.as<double>(), vp.as<double>(),
+               s == 0 ? nullptr : abp + 10 + s - 1, abp + s, st(), part(), tick());
+        launch(dev::k_lz_axpy, vg, dev::VEC_THREADS, 0, stream, n, w.as<double>(), v.as<double>(), abp + s, abp + 10 + s, st(), part(), tick());
+        launch(dev::k_lz_next, vg, dev::VEC_THREADS, 0, stream, n, w.as<double>(), v.as<double>(), vp.as<double>(), abp + 10 + s);
+    }
+    double hab[20];
+    check(cudaMemcpyAsync(hab, abp, sizeof hab, cudaMemcpyDeviceToHost, stream), "lanczos read");
+    check(cudaStreamSynchronize(stream), "lanczos");
+    std::vector<double> alpha, beta;
+    for (int s = 0; s < 10; s++) {
+        const double a = hab[s], b = hab[10 + s];  // hab[10 + s] holds |w| after step s
         alpha.push_back(a);
-        b = std::sqrt(hostState->beta);
         if (!(b > 1e-12 * std::fabs(a))) break;
         beta.push_back(b);
-        launch(dev::k_lz_next, vg, dev::VEC_THREADS, 0, stream, n, w.as<double>(), v.as<double>(), vp.as<double>(), b);
     }
     beta.resize(alpha.size() - 1);
     check(cudaGetLastError(), "lanczos");
@@ -1479,7 +1542,7 @@ double SolverImpl::lanczos(int l) {
 }
 
 void SolverImpl::prepareSmoothers() {
-    if (smoothersReady) return;
+    if (M->smoothersReady) return;
     for (int l = 0; l + 1 < int(L.size()); l++) {
         HostLevel& h = H.levels[size_t(l)];
         if (!(h.lmax > 0)) h.lmax = lanczos(l);
@@ -1496,7 +1559,7 @@ void SolverImpl::prepareSmoothers() {
         double rho = 1 / sigma;
         D.chebC1.clear();
         D.chebC2.clear();
-        for (int k = 1; k < degree; k++) {
+        for (int k = 1; k < M->degree; k++) {
             const double rn = 1 / (2 * sigma - rho);
             D.chebC1.push_back(float(rn * rho));
             D.chebC2.push_back(float(2 * rn / delta));
@@ -1504,30 +1567,33 @@ void SolverImpl::prepareSmoothers() {
         }
     }
     // the coarsest level keeps the default Jacobi weight 0.5 (its eigenvalue is never estimated)
-    smoothersReady = true;
+    M->smoothersReady = true;
+    M->version++;
 }
 
 // one FP64 CG iteration (voxel_fea.cpp:901-919)
 void SolverImpl::recordPlainIteration(dev::Ctl ctl) {
     const HostLevel& h = H.levels[0];
     DevLevel& D = L[0];
+    LevelWork& W0 = W[0];
     if (!D.useTiles) {
         launch(dev::k_apply_alpha<double, false>, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c64, p.as<double>(), q.as<double>(),
                st(), part(), tick(), ctl);
     } else {
         dev::TileIO<double> io{p.as<double>(), q.as<double>(), nullptr, nullptr, 0.f, 0.f, 0};
-        launch(dev::k_tile<double, dev::TOP_DOT, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double>(), stream, D.view, D.c64, D.tiles.as<uint32_t>(), io,
-               st(), part(), tick(), ctl);
+        launch(dev::k_tile<double, dev::TOP_DOT, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double>(), stream, D.view, D.c64,
+               D.tiles.as<uint32_t>(), io, st(), part(), tick(), ctl);
     }
     const bool one = exactOneLevel();
     launch(dev::k_cg_update, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x.as<double>(), r.as<double>(), p.as<double>(),
-           q.as<double>(), one ? nullptr : D.r.as<float>(), D.invD.as<float>(), D.d.as<float>(), D.z.as<float>(), D.cf0, st(), part(), tick(), ctl);
+           q.as<double>(), one ? nullptr : W0.r.as<float>(), D.invD.as<float>(), W0.d.as<float>(), W0.z.as<float>(), D.cf0, st(), part(), tick(),
+           ctl);
     float* z32 = nullptr;
     if (one) {
         const int threads = 256, warps = threads / 32;
         const int grid = std::max(1, std::min(smCount * 2, (m + warps - 1) / warps));
         launch(dev::k_coarse<double, double>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(), r.as<double>(),
-                                                                                           z64.as<double>(), ctl);
+               z64.as<double>(), ctl);
     } else {
         z32 = vcycle(0, ctl, false, true);  // r32 and the first smoothing step came with the update
     }
@@ -1540,33 +1606,40 @@ void SolverImpl::recordPlainIteration(dev::Ctl ctl) {
 void SolverImpl::recordMixedIteration(dev::Ctl ctl) {
     const HostLevel& h = H.levels[0];
     DevLevel& D = L[0];
+    LevelWork& W0 = W[0];
     const int* foldFlag = &st()->fold;
     if (!D.useTiles) {
         launch(dev::k_apply_alpha<float, true>, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c32, p32.as<float>(), q32.as<float>(),
                st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
     } else {
         dev::TileIO<float> io{p32.as<float>(), q32.as<float>(), nullptr, nullptr, 0.f, 0.f, 0};
-        launch(dev::k_tile<float, dev::TOP_DOT, false, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float>(), stream, D.view, D.c32, D.tiles.as<uint32_t>(), io,
-               st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
+        launch(dev::k_tile<float, dev::TOP_DOT, false, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float>(), stream, D.view, D.c32,
+               D.tiles.as<uint32_t>(), io, st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
     }
-    launch(dev::k_mx_update, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x32.as<float>(), D.r.as<float>(), p32.as<float>(),
-                                                                         q32.as<float>(), st(), part(), tick(), ctl);
+    launch(dev::k_mx_update, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x32.as<float>(), W0.r.as<float>(),
+           p32.as<float>(), q32.as<float>(), st(), part(), tick(), ctl);
     const dev::Ctl foldCtl{ctl.skipIf, foldFlag};
     launch(dev::k_mx_fold1, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, x.as<double>(), x32.as<float>(), st(), foldCtl);
     op64(0, x.as<double>(), q.as<double>(), false, foldCtl);
-    launch(dev::k_mx_fold2, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), D.r.as<float>(),
-                                                                        st(), part(), tick(), foldCtl);
-    float* z32 = vcycle(0, ctl, mixedOwn16);
-    launch(dev::k_mx_dots, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, D.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
+    launch(dev::k_mx_fold2, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(),
+           W0.r.as<float>(), st(), part(), tick(), foldCtl);
+    float* z32 = vcycle(0, ctl, M->mixedOwn16);
+    launch(dev::k_mx_dots, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, W0.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
     launch(dev::k_mx_p, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, z32, p32.as<float>(), st(), ctl);
 }
 
-ps_status SolverImpl::runSolve(const double* fDev, const double* x0Dev, const ps_solve_opts& o, double* uDev, ps_solve_result& res) {
-    const auto t0 = std::chrono::steady_clock::now();
-    const int64_t launches0 = launches;
+void SolverImpl::startSolve(const double* fDev, const double* x0Dev, const ps_solve_opts& o, double* uDev, double* uHost) {
+    pend = Pending{};
+    pend.t0 = std::chrono::steady_clock::now();
+    pend.launches0 = launches;
+    pend.o = o;
+    pend.uDev = uDev;
+    pend.uHost = uHost;
     const HostLevel& h = H.levels[0];
     DevLevel& D = L[0];
+    LevelWork& W0 = W[0];
     const bool mixed = o.precision == PS_PREC_MIXED && !exactOneLevel();
+    pend.mixed = mixed;
     const int64_t n = h.nDof;
     setDegree(o.smoother_degree > 0 ? o.smoother_degree : 2);
     prepareSmoothers();
@@ -1576,22 +1649,23 @@ ps_status SolverImpl::runSolve(const double* fDev, const double* x0Dev, const ps
     s.maxIter = o.max_iter;
     s.first = 1;
     s.mixed = mixed ? 1 : 0;
-    s.foldFactor = foldFactor;
-    check(cudaMemcpyAsync(state.p, &s, sizeof s, cudaMemcpyHostToDevice, stream), "state");
+    s.foldFactor = M->foldFactor;
+    *hostState = s;
+    check(cudaMemcpyAsync(state.p, hostState, sizeof s, cudaMemcpyHostToDevice, stream), "state");
     if (fDev != f.p) check(cudaMemcpyAsync(f.p, fDev, size_t(n) * 8, cudaMemcpyDeviceToDevice, stream), "f copy");
     launch(dev::k_mask_copy, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x0Dev, x.as<double>());
     const dev::Ctl none{nullptr, nullptr};
     const dev::Ctl ctl{&st()->done, nullptr};
     op64(0, x.as<double>(), q.as<double>(), false, none);
     launch(dev::k_cg_init, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), r.as<double>(),
-                                                                       nullptr, st(), part(), tick());
+           nullptr, st(), part(), tick());
     // first preconditioned direction
     if (mixed) {
         check(cudaMemsetAsync(x32.p, 0, size_t(n) * 4, stream), "memset");
-        launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), D.r.as<float>(),
-               D.invD.as<float>(), D.d.as<float>(), D.z.as<float>(), D.cf0, st(), ctl);
-        float* z32 = vcycle(0, ctl, mixedOwn16, true);
-        launch(dev::k_mx_dots, vecGrid(n), dev::VEC_THREADS, 0, stream, n, D.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
+        launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), W0.r.as<float>(),
+               D.invD.as<float>(), W0.d.as<float>(), W0.z.as<float>(), D.cf0, st(), ctl);
+        float* z32 = vcycle(0, ctl, M->mixedOwn16, true);
+        launch(dev::k_mx_dots, vecGrid(n), dev::VEC_THREADS, 0, stream, n, W0.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
         launch(dev::k_mx_p, vecGrid(n), dev::VEC_THREADS, 0, stream, n, z32, p32.as<float>(), st(), ctl);
     } else {
         float* z32 = nullptr;
@@ -1600,21 +1674,26 @@ ps_status SolverImpl::runSolve(const double* fDev, const double* x0Dev, const ps
             const int grid = std::max(1, std::min(smCount * 2, (m + warps - 1) / warps));
             check(cudaMemsetAsync(z64.p, 0, size_t(n) * 8, stream), "memset");
             launch(dev::k_coarse<double, double>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(),
-                                                                                               r.as<double>(), z64.as<double>(), ctl);
+                   r.as<double>(), z64.as<double>(), ctl);
         } else {
-            launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), D.r.as<float>(),
-                   D.invD.as<float>(), D.d.as<float>(), D.z.as<float>(), D.cf0, st(), ctl);
+            launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), W0.r.as<float>(),
+                   D.invD.as<float>(), W0.d.as<float>(), W0.z.as<float>(), D.cf0, st(), ctl);
             z32 = vcycle(0, ctl, false, true);
         }
         launch(dev::k_cg_dots, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), z32, z64.as<double>(),
                q.as<double>(), st(), part(), tick(), ctl);
-        launch(dev::k_cg_p, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, z32, z64.as<double>(), p.as<double>(), st(), ctl);
+        launch(dev::k_cg_p, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, z32, z64.as<double>(), p.as<double>(), st(),
+               ctl);
     }
     launch(dev::k_clear_first, 1, 1, 0, stream, st());
     check(cudaGetLastError(), "solve setup");
-    // the iteration graph (recorded once per precision)
-    cudaGraphExec_t& g = graph[mixed ? 1 : 0];
-    if (!g) {
+    // the iteration graph (recorded once per precision and smoother version)
+    const int gi = mixed ? 1 : 0;
+    if (graph[gi] && graphVersion[gi] != M->version) {
+        cudaGraphExecDestroy(graph[gi]);
+        graph[gi] = nullptr;
+    }
+    if (!graph[gi]) {
         cudaGraph_t gr;
         check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
         if (mixed) recordMixedIteration(ctl);
@@ -1622,58 +1701,82 @@ ps_status SolverImpl::runSolve(const double* fDev, const double* x0Dev, const ps
         check(cudaStreamEndCapture(stream, &gr), "capture end");
         size_t nodes = 0;
         check(cudaGraphGetNodes(gr, nullptr, &nodes), "graph nodes");
-        graphKernels[mixed ? 1 : 0] = int64_t(nodes);
+        graphKernels[gi] = int64_t(nodes);
         launches -= int64_t(nodes);  // captured, not run
-        check(cudaGraphInstantiate(&g, gr, 0), "instantiate");
+        check(cudaGraphInstantiate(&graph[gi], gr, 0), "instantiate");
         cudaGraphDestroy(gr);
+        graphVersion[gi] = M->version;
     }
-    // batches of iterations, sized from the observed convergence rate
-    int batch = 2;
-    double lastRel = 0;
-    int lastIt = 0;
-    ps_status outcome = PS_OK;
-    for (;;) {
-        readState();
+    enqueueStateRead();
+    pend.active = true;
+}
+
+bool SolverImpl::advance(bool block, ps_solve_result& res) {
+    if (!pend.active) return true;
+    if (block) check(cudaEventSynchronize(ev), "sync");
+    else {
+        const cudaError_t qe = cudaEventQuery(ev);
+        if (qe == cudaErrorNotReady) return false;
+        check(qe, "event query");
+    }
+    const HostLevel& h = H.levels[0];
+    DevLevel& D = L[0];
+    const int64_t n = h.nDof;
+    const ps_solve_opts& o = pend.o;
+    const bool mixed = pend.mixed;
+    const dev::Ctl none{nullptr, nullptr};
+    if (!pend.finishing) {
         const dev::SolveState& hs = *hostState;
-        if (hs.done) break;
-        if (o.cancel && *o.cancel) { outcome = PS_CANCELLED; break; }
-        if (o.time_limit_s > 0 && std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o.time_limit_s) {
-            outcome = PS_TIMEOUT;
-            break;
+        bool stop = hs.done != 0;
+        if (!stop && o.cancel && *o.cancel) {
+            pend.outcome = PS_CANCELLED;
+            stop = true;
         }
-        const double rel = mixed ? std::max(hs.est, 0.0) : hs.rel;
-        if (lastIt > 0 && hs.it > lastIt && rel > 0 && lastRel > 0) {
-            const double rate = std::pow(rel / lastRel, 1.0 / (hs.it - lastIt));
-            int need = 32;
-            if (rate < 0.999) need = int(std::ceil(std::log(o.tol / rel) / std::log(rate)));
-            batch = std::max(1, std::min({need, 32, 2 * batch}));
+        if (!stop && o.time_limit_s > 0 &&
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - pend.t0).count() > o.time_limit_s) {
+            pend.outcome = PS_TIMEOUT;
+            stop = true;
         }
-        lastRel = rel;
-        lastIt = hs.it;
-        batch = std::max(1, std::min(batch, o.max_iter - hs.it + 1));
-        for (int b = 0; b < batch; b++) check(cudaGraphLaunch(g, stream), "graph launch");
-        launches += int64_t(batch) * graphKernels[mixed ? 1 : 0];
-    }
-    // the result
-    if (!mixed) {
-        if (hostState->done == 2) check(cudaMemsetAsync(x.p, 0, size_t(n) * 8, stream), "memset");
-        op64(0, x.as<double>(), q.as<double>(), false, none);
-        launch(dev::k_final, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), st(), part(),
-                                                                         tick());
-    } else {
-        if (hostState->done == 2) check(cudaMemsetAsync(x.p, 0, size_t(n) * 8, stream), "memset");
-        if (outcome == PS_CANCELLED || outcome == PS_TIMEOUT) {
+        if (!stop) {
+            // the next batch of iterations, sized from the observed convergence rate
+            const double rel = mixed ? std::max(hs.est, 0.0) : hs.rel;
+            if (pend.lastIt > 0 && hs.it > pend.lastIt && rel > 0 && pend.lastRel > 0) {
+                const double rate = std::pow(rel / pend.lastRel, 1.0 / (hs.it - pend.lastIt));
+                int need = 32;
+                if (rate < 0.999) need = int(std::ceil(std::log(o.tol / rel) / std::log(rate)));
+                pend.batch = std::max(1, std::min({need, 32, 2 * pend.batch}));
+            }
+            pend.lastRel = rel;
+            pend.lastIt = hs.it;
+            const int batch = std::max(1, std::min(pend.batch, o.max_iter - hs.it + 1));
+            const int gi = mixed ? 1 : 0;
+            for (int b = 0; b < batch; b++) check(cudaGraphLaunch(graph[gi], stream), "graph launch");
+            launches += int64_t(batch) * graphKernels[gi];
+            enqueueStateRead();
+            return false;
+        }
+        // the result: true residual, u to its destinations
+        if (hs.done == 2) check(cudaMemsetAsync(x.p, 0, size_t(n) * 8, stream), "memset");
+        if (!mixed) {
+            op64(0, x.as<double>(), q.as<double>(), false, none);
+            launch(dev::k_final, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), st(), part(),
+                   tick());
+        } else if (pend.outcome == PS_CANCELLED || pend.outcome == PS_TIMEOUT) {
             // fold what the FP32 iterate holds and report the true residual
             launch(dev::k_mx_fold1, vecGrid(n), dev::VEC_THREADS, 0, stream, n, x.as<double>(), x32.as<float>(), st(), none);
             op64(0, x.as<double>(), q.as<double>(), false, none);
             launch(dev::k_final, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), st(), part(),
-                                                                             tick());
+                   tick());
         }
+        if (pend.uDev && pend.uDev != x.p) check(cudaMemcpyAsync(pend.uDev, x.p, size_t(n) * 8, cudaMemcpyDeviceToDevice, stream), "u copy");
+        if (pend.uHost) check(cudaMemcpyAsync(pend.uHost, x.p, size_t(n) * 8, cudaMemcpyDeviceToHost, stream), "u download");
+        enqueueStateRead();
+        pend.finishing = true;
+        return false;
     }
-    if (uDev != x.p) check(cudaMemcpyAsync(uDev, x.p, size_t(n) * 8, cudaMemcpyDeviceToDevice, stream), "u copy");
-    readState();
     check(cudaGetLastError(), "solve");
     const dev::SolveState& hs = *hostState;
+    ps_status outcome = pend.outcome;
     res.iterations = hs.it;
     res.residual = hs.rel;
     res.folds = hs.folds;
@@ -1683,33 +1786,59 @@ ps_status SolverImpl::runSolve(const double* fDev, const double* x0Dev, const ps
         else if (!res.converged) outcome = PS_NOT_CONVERGED;
     }
     res.status = outcome;
-    res.kernels = launches - launches0;
-    res.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    return outcome;
+    res.kernels = launches - pend.launches0;
+    res.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - pend.t0).count();
+    pend.active = false;
+    return true;
 }
 
 // ==================================================================== Solver
 
-Solver::Solver(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsestMaxDof, const double* diagAdd)
-    : impl_(new SolverImpl) {
+struct SolverHandle {
+    std::shared_ptr<SharedModel> model;
+    std::unique_ptr<SolverImpl> main;
+    std::vector<std::unique_ptr<SolverImpl>> extra;  // batch contexts, created on demand
+};
+
+Solver::Solver(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsestMaxDof, const double* diagAdd) {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
         cudaGetLastError();
         throw Error(PS_ENODEV, "no CUDA device is available");
     }
-    impl_->build(dims, density, nu, bc, coarsestMaxDof, diagAdd);
+    auto model = std::make_shared<SharedModel>();
+    model->build(dims, density, nu, bc, coarsestMaxDof, diagAdd);
+    auto* I = new SolverImpl(model);
+    impl_.reset(I);
+    I->allocate();
+    handle_.reset(new SolverHandle{model, nullptr, {}});
 }
 
-Solver::~Solver() = default;
+Solver::~Solver() {
+    handle_.reset();
+    impl_.reset();
+}
 
 const Hierarchy& Solver::hierarchy() const { return impl_->H; }
 int64_t Solver::nDof() const { return impl_->H.levels[0].nDof; }
-int64_t Solver::deviceBytes() const { return impl_->bytes; }
+int64_t Solver::deviceBytes() const {
+    int64_t b = impl_->M->bytes + impl_->bytes;
+    for (auto& c : handle_->extra) b += c->bytes;
+    return b;
+}
+int64_t Solver::contextBytes() const { return impl_->bytes; }
 double Solver::levelLmax(int l) const { return impl_->H.levels[size_t(l)].lmax; }
 
 static void validateF(const double* f, const double* x0, int64_t n) {
-    for (int64_t i = 0; i < n; i++)
-        if (!std::isfinite(f[i]) || (x0 && !std::isfinite(x0[i]))) throw Error(PS_ENONFINITE, "Forces and displacements must be finite numbers.");
+    bool bad = false;
+    parallelFor(n, [&](int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; i++)
+            if (!std::isfinite(f[i]) || (x0 && !std::isfinite(x0[i]))) {
+                bad = true;
+                return;
+            }
+    }, 1 << 20);
+    if (bad) throw Error(PS_ENONFINITE, "Forces and displacements must be finite numbers.");
 }
 
 ps_status Solver::solve(const double* f, const ps_solve_opts& o, double* u, ps_solve_result& res) {
@@ -1723,11 +1852,11 @@ ps_status Solver::solve(const double* f, const ps_solve_opts& o, double* u, ps_s
         check(cudaMemcpyAsync(I.p.p, o.x0, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "x0 upload");
         x0 = I.p.as<double>();
     }
-    const ps_status s = I.runSolve(I.f.as<double>(), x0, o, I.x.as<double>(), res);
-    check(cudaMemcpyAsync(u, I.x.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "u download");
-    check(cudaStreamSynchronize(I.stream), "sync");
+    I.startSolve(I.f.as<double>(), x0, o, nullptr, u);
+    while (!I.advance(true, res)) {
+    }
     res.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    return s;
+    return ps_status(res.status);
 }
 
 ps_status Solver::solveDevice(const double* fDev, const ps_solve_opts& o, double* uDev, ps_solve_result& res) {
@@ -1737,15 +1866,85 @@ ps_status Solver::solveDevice(const double* fDev, const ps_solve_opts& o, double
         check(cudaMemcpyAsync(I.p.p, x0, size_t(nDof()) * 8, cudaMemcpyDeviceToDevice, I.stream), "x0 copy");
         x0 = I.p.as<double>();
     }
-    const ps_status s = I.runSolve(fDev, x0, o, uDev, res);
-    check(cudaStreamSynchronize(I.stream), "sync");
-    return s;
+    return I.runSolve(fDev, x0, o, uDev, res);
+}
+
+void Solver::begin(const double* fHost, const ps_solve_opts& o, double* uHost) {
+    SolverImpl& I = *impl_;
+    const int64_t n = nDof();
+    check(cudaMemcpyAsync(I.f.p, fHost, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "f upload");
+    const double* x0 = nullptr;
+    if (o.x0) {
+        check(cudaMemcpyAsync(I.p.p, o.x0, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "x0 upload");
+        x0 = I.p.as<double>();
+    }
+    I.startSolve(I.f.as<double>(), x0, o, nullptr, uHost);
+}
+
+bool Solver::poll(ps_solve_result& res) { return impl_->advance(false, res); }
+
+ps_status Solver::solveBatch(int32_t nrhs, const double* f, const ps_solve_opts& base, double* u, ps_solve_result* results, int concurrency) {
+    const int64_t n = nDof();
+    validateF(f, nullptr, n * nrhs);
+    if (base.x0) validateF(base.x0, nullptr, n * nrhs);
+    // contexts: the handle's own plus extra ones, as many as free memory allows
+    size_t freeB = 0, totalB = 0;
+    check(cudaMemGetInfo(&freeB, &totalB), "cudaMemGetInfo");
+    const int64_t per = impl_->bytes + (64 << 20);
+    const int fit = int(std::max<int64_t>(0, (int64_t(freeB) - (int64_t(1) << 30)) / per));
+    const int K = std::max(1, std::min({concurrency, int(nrhs), 1 + fit}));
+    SolverHandle& Hd = *handle_;
+    while (int(Hd.extra.size()) < K - 1) {
+        auto c = std::make_unique<SolverImpl>(impl_->M);
+        c->allocate();
+        Hd.extra.push_back(std::move(c));
+    }
+    std::vector<SolverImpl*> ctx{impl_.get()};
+    for (int k = 0; k + 1 < K; k++) ctx.push_back(Hd.extra[size_t(k)].get());
+    std::vector<int> job(size_t(K), -1);
+    int next = 0, left = nrhs;
+    ps_status worst = PS_OK;
+    auto startOn = [&](int k, int q) {
+        SolverImpl& I = *ctx[size_t(k)];
+        ps_solve_opts o = base;
+        check(cudaMemcpyAsync(I.f.p, f + int64_t(q) * n, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "f upload");
+        const double* x0 = nullptr;
+        if (base.x0) {
+            check(cudaMemcpyAsync(I.p.p, base.x0 + int64_t(q) * n, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "x0 upload");
+            x0 = I.p.as<double>();
+        }
+        o.x0 = nullptr;
+        I.startSolve(I.f.as<double>(), x0, o, nullptr, u + int64_t(q) * n);
+        job[size_t(k)] = q;
+    };
+    // the smoothers are estimated once, before the contexts run side by side
+    impl_->setDegree(base.smoother_degree > 0 ? base.smoother_degree : 2);
+    impl_->prepareSmoothers();
+    for (int k = 0; k < K && next < nrhs; k++) startOn(k, next++);
+    while (left > 0) {
+        bool progressed = false;
+        for (int k = 0; k < K; k++) {
+            if (job[size_t(k)] < 0) continue;
+            ps_solve_result r{};
+            if (!ctx[size_t(k)]->advance(false, r)) continue;
+            progressed = true;
+            const int q = job[size_t(k)];
+            if (results) results[q] = r;
+            if (r.status > worst) worst = ps_status(r.status);
+            left--;
+            job[size_t(k)] = -1;
+            if (next < nrhs) startOn(k, next++);
+        }
+        if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+    return worst;
 }
 
 void Solver::precondition(const double* rHost, double* zHost) {
     SolverImpl& I = *impl_;
     const HostLevel& h = I.H.levels[0];
     DevLevel& D = I.L[0];
+    LevelWork& W0 = I.W[0];
     const int64_t n = h.nDof;
     I.setDegree(2);  // the reference's preconditioner
     I.prepareSmoothers();
@@ -1757,12 +1956,12 @@ void Solver::precondition(const double* rHost, double* zHost) {
         const int grid = std::max(1, std::min(I.smCount * 2, (I.m + warps - 1) / warps));
         check(cudaMemsetAsync(I.z64.p, 0, size_t(n) * 8, I.stream), "memset");
         I.launch(dev::k_coarse<double, double>, grid, threads, size_t(I.m) * sizeof(double), I.stream, I.m, I.cDof.as<int>(), I.cInv.as<double>(),
-                                                                                               I.r.as<double>(), I.z64.as<double>(), none);
+                 I.r.as<double>(), I.z64.as<double>(), none);
         check(cudaMemcpyAsync(zHost, I.z64.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "z download");
     } else {
         I.launch(dev::k_rmax, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, I.r.as<double>(), I.st(), I.part(), I.tick());
-        I.launch(dev::k_vc_load, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, I.r.as<double>(), D.r.as<float>(),
-                 D.invD.as<float>(), D.d.as<float>(), D.z.as<float>(), D.cf0, I.st(), none);
+        I.launch(dev::k_vc_load, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, I.r.as<double>(), W0.r.as<float>(),
+                 D.invD.as<float>(), W0.d.as<float>(), W0.z.as<float>(), D.cf0, I.st(), none);
         float* z32 = I.vcycle(0, none, false, true);
         I.launch(dev::k_vc_store, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, z32, I.q.as<double>(), I.st());
         check(cudaMemcpyAsync(zHost, I.q.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "z download");
@@ -1785,11 +1984,12 @@ double Solver::timeKernel(int which, int reps) {
     I.prepareSmoothers();
     const dev::Ctl none{nullptr, nullptr};
     DevLevel& D = I.L[0];
+    LevelWork& W0 = I.W[0];
     cudaEvent_t e0, e1;
     check(cudaEventCreate(&e0), "event");
     check(cudaEventCreate(&e1), "event");
     auto once = [&] {
-        if (which == 0) I.op32<dev::OP_CHEB>(0, D.z.as<float>(), D.t.as<float>(), D.cf1, D.cf2, none, true);
+        if (which == 0) I.op32<dev::OP_CHEB>(0, W0.z.as<float>(), W0.t.as<float>(), D.cf1, D.cf2, none, true);
         else I.op64(0, I.p.as<double>(), I.q.as<double>(), false, none);
     };
     once();
@@ -1804,7 +2004,11 @@ double Solver::timeKernel(int which, int reps) {
     return double(ms) / reps;
 }
 
-int64_t Solver::launches() const { return impl_->launches; }
+int64_t Solver::launches() const {
+    int64_t n = impl_->launches;
+    for (auto& c : handle_->extra) n += c->launches;
+    return n;
+}
 
 void Solver::apply(int level, const double* xHost, double* yHost, bool raw) {
     SolverImpl& I = *impl_;
@@ -1829,7 +2033,8 @@ void Solver::stresses(const double* u, double E, double h, bool principals, floa
     out.alloc(size_t(nn) * 4 * 3, scratch);
     check(cudaMemcpyAsync(I.p.p, u, size_t(L0.nDof) * 8, cudaMemcpyHostToDevice, I.stream), "u upload");
     float* o = out.as<float>();
-    I.launch(dev::k_stresses, I.nodeGrid(nn), dev::NODE_THREADS, 0, I.stream, I.L[0].view, sc, I.p.as<double>(), principals ? 1 : 0, o, o + nn, o + 2 * nn);
+    I.launch(dev::k_stresses, I.nodeGrid(nn), dev::NODE_THREADS, 0, I.stream, I.L[0].view, sc, I.p.as<double>(), principals ? 1 : 0, o, o + nn,
+             o + 2 * nn);
     check(cudaMemcpyAsync(vm, o, size_t(nn) * 4, cudaMemcpyDeviceToHost, I.stream), "vm");
     if (principals) {
         check(cudaMemcpyAsync(p1, o + nn, size_t(nn) * 4, cudaMemcpyDeviceToHost, I.stream), "p1");
@@ -1846,8 +2051,8 @@ void Solver::reactions(const double* u, const double* f, double R[3]) {
     if (f) check(cudaMemcpyAsync(I.r.p, f, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "f upload");
     check(cudaMemsetAsync(I.q.p, 0, size_t(n) * 8, I.stream), "memset");
     I.op64(0, I.p.as<double>(), I.q.as<double>(), true, dev::Ctl{nullptr, nullptr});
-    I.launch(dev::k_reactions, I.vecGrid(L0.nNodes), dev::VEC_THREADS, 0, I.stream, L0.nNodes, I.L[0].view.nmask, I.L[0].bc.as<uint8_t>(), I.q.as<double>(),
-                                                                               f ? I.r.as<double>() : nullptr, I.st(), I.part(), I.tick());
+    I.launch(dev::k_reactions, I.vecGrid(L0.nNodes), dev::VEC_THREADS, 0, I.stream, L0.nNodes, I.L[0].view.nmask, I.L[0].bc.as<uint8_t>(),
+             I.q.as<double>(), f ? I.r.as<double>() : nullptr, I.st(), I.part(), I.tick());
     I.readState();
     R[0] = I.hostState->alpha;
     R[1] = I.hostState->beta;

@@ -10,6 +10,7 @@
 namespace psfea {
 
 struct SolverImpl;
+struct SolverHandle;
 
 class Solver {
 public:
@@ -20,12 +21,20 @@ public:
     const Hierarchy& hierarchy() const;
     int64_t nDof() const;
     int64_t deviceBytes() const;
+    int64_t contextBytes() const;  // device bytes of one solve context (work vectors and state)
     double levelLmax(int l) const;
 
     // host vectors in/out; returns the outcome status
     ps_status solve(const double* f, const ps_solve_opts& o, double* u, ps_solve_result& res);
     // device vectors in/out (o.x0 is a device pointer)
     ps_status solveDevice(const double* fDev, const ps_solve_opts& o, double* uDev, ps_solve_result& res);
+    // nrhs solves on this hierarchy, up to `concurrency` at once on separate streams (each solve its
+    // own context), refilled as solves finish
+    ps_status solveBatch(int32_t nrhs, const double* f, const ps_solve_opts& o, double* u, ps_solve_result* results, int concurrency);
+    // non-blocking solve for a serving loop: begin() enqueues it (f and u stay valid until poll()
+    // returns true), poll() moves it on without waiting for the GPU
+    void begin(const double* fHost, const ps_solve_opts& o, double* uHost);
+    bool poll(ps_solve_result& res);
     void precondition(const double* r, double* z);
     void apply(int level, const double* x, double* y, bool raw);
     void stresses(const double* u, double E, double h, bool principals, float* vm, float* p1, float* p3);
@@ -42,6 +51,7 @@ public:
 
 private:
     std::unique_ptr<SolverImpl> impl_;
+    std::unique_ptr<SolverHandle> handle_;
 };
 
 }  // namespace psfea
