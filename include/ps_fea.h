@@ -39,6 +39,7 @@ typedef enum ps_status {
     PS_BREAKDOWN = 2,       /* p.Kp <= 0 (a mechanism; voxel_fea.cpp:904); u is returned */
     PS_CANCELLED = 3,       /* the cancel flag was raised; u is returned */
     PS_TIMEOUT = 4,         /* the time limit ran out; u is returned */
+    PS_PENDING = 5,         /* a served request has not finished yet */
     PS_EINVAL = 10,         /* bad dims, sizes, density or nu (voxel_fea.cpp:141-146, hex8.cpp:9) */
     PS_ENONFINITE = 11,     /* non-finite f or x0 (voxel_fea.cpp:866-868) */
     PS_EOOM = 12,           /* device memory or admission budget exhausted */
@@ -186,6 +187,59 @@ ps_status ps_element_matrix(double nu, double K[576], double* corner_stress);
  * (pruneFloating, voxel_fea.cpp:1086-1119). held_node: NX*NY*NZ bytes. */
 ps_status ps_prune_floating(const int32_t dims[3], const float* density, const uint8_t* held_node,
                             float* out, int32_t* removed);
+
+/* ---- Serving: many independent solves on one GPU with continuous batching (no counterpart in the
+ * reference, which runs one job at a time behind a GPU lock, native/src/gpu/gpu.hpp:43).
+ * Requests are submitted at any time; host threads build their hierarchies; a scheduler admits
+ * them in arrival order as device memory (estimated footprint against the budget) and active
+ * slots allow, runs them concurrently on separate streams, retires finished ones and back-fills. */
+typedef struct ps_server ps_server_t;
+
+typedef struct ps_request {
+    int32_t dims[3];
+    const float* density;      /* copied at submit */
+    double nu;
+    const uint8_t* bc;         /* copied at submit */
+    const double* f;           /* copied at submit */
+    int64_t coarsest_max_dof;  /* 0 = 300 */
+    double tol;                /* 0 = 1e-8 */
+    int32_t max_iter;          /* 0 = 5000 */
+    int32_t precision;         /* ps_precision */
+    int32_t smoother_degree;   /* 0 = 2 */
+} ps_request;
+
+typedef struct ps_request_result {
+    int64_t id;
+    int32_t status;            /* ps_status of the solve (or the error that ended the request) */
+    int32_t iterations;
+    int32_t converged;
+    double residual;
+    int64_t n_dof;
+    const double* u;           /* n_dof displacements, valid until ps_server_release */
+    double build_s;            /* submit -> hierarchy built (host) */
+    double wait_s;             /* built -> admitted to the GPU */
+    double solve_s;            /* admitted -> finished */
+    double total_s;            /* submit -> finished */
+} ps_request_result;
+
+typedef struct ps_server_stats {
+    int64_t queued, active, completed;
+    int64_t device_bytes_in_use, peak_device_bytes, budget_bytes;
+    int64_t peak_active;
+} ps_server_stats;
+
+/* budget_bytes 0 = 80 % of the free device memory; max_active 0 = 4 (measured best for the
+ * serving stream: each small-grid solve already spreads over the whole GPU); build_threads 0 = half
+ * the host cores. */
+ps_status ps_server_create(int64_t device_budget_bytes, int32_t max_active, int32_t build_threads, ps_server_t** out);
+ps_status ps_server_submit(ps_server_t* s, const ps_request* req, int64_t* id);
+/* PS_PENDING until the request has finished, then PS_OK with *out filled */
+ps_status ps_server_poll(ps_server_t* s, int64_t id, ps_request_result* out);
+ps_status ps_server_wait(ps_server_t* s, int64_t id, ps_request_result* out);
+/* frees a finished request's result */
+ps_status ps_server_release(ps_server_t* s, int64_t id);
+ps_status ps_server_get_stats(ps_server_t* s, ps_server_stats* out);
+void ps_server_destroy(ps_server_t* s);
 
 /* Message of the calling thread's last error ("" if none). */
 const char* ps_last_error(void);

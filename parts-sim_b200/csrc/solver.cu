@@ -1072,28 +1072,41 @@ void check(cudaError_t e, const char* what) {
     }
 }
 
+// Device buffer. With a stream it is allocated and freed stream-ordered (cudaMallocAsync /
+// cudaFreeAsync), which never waits for the rest of the device: handles come and go while other
+// solves run (serving). Without one it uses cudaMalloc / cudaFree.
 struct DevMem {
     void* p = nullptr;
     size_t bytes = 0;
+    cudaStream_t s = nullptr;
     DevMem() = default;
     DevMem(const DevMem&) = delete;
     DevMem& operator=(const DevMem&) = delete;
-    DevMem(DevMem&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevMem(DevMem&& o) noexcept : p(o.p), bytes(o.bytes), s(o.s) { o.p = nullptr; o.bytes = 0; }
     DevMem& operator=(DevMem&& o) noexcept {
-        if (this != &o) { release(); p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0; }
+        if (this != &o) { release(); p = o.p; bytes = o.bytes; s = o.s; o.p = nullptr; o.bytes = 0; }
         return *this;
     }
     ~DevMem() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (s) cudaFreeAsync(p, s);
+            else cudaFree(p);
+        }
         p = nullptr;
         bytes = 0;
     }
-    void alloc(size_t n, int64_t& total) {
+    void alloc(size_t n, int64_t& total, cudaStream_t stream = nullptr) {
         release();
+        s = stream;
         if (n == 0) return;
-        check(cudaMalloc(&p, n), "cudaMalloc");
-        check(cudaMemset(p, 0, n), "cudaMemset");
+        if (s) {
+            check(cudaMallocAsync(&p, n, s), "cudaMallocAsync");
+            check(cudaMemsetAsync(p, 0, n, s), "cudaMemsetAsync");
+        } else {
+            check(cudaMalloc(&p, n), "cudaMalloc");
+            check(cudaMemset(p, 0, n), "cudaMemset");
+        }
         bytes = n;
         total += int64_t(n);
     }
@@ -1101,9 +1114,12 @@ struct DevMem {
 };
 
 template <class T>
-void upload(DevMem& m, const std::vector<T>& v, int64_t& total) {
-    m.alloc(v.size() * sizeof(T), total);
-    if (!v.empty()) check(cudaMemcpy(m.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+void upload(DevMem& m, const std::vector<T>& v, int64_t& total, cudaStream_t s = nullptr) {
+    m.alloc(v.size() * sizeof(T), total, s);
+    if (!v.empty()) {
+        if (s) check(cudaMemcpyAsync(m.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
+        else check(cudaMemcpy(m.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    }
 }
 
 int gridFor(int64_t n, int threads, int cap) {
@@ -1126,11 +1142,17 @@ struct DevLevel {
     float cf0 = 0, cf1 = 0, cf2 = 0, omega = 0.5f;
     std::vector<float> chebC1, chebC2;  // steps 1 .. degree-1 of the Chebyshev smoother: d = c1 d + c2 D^-1 (r - K z)
     bool hasOwn = false;
+    void release() {
+        for (DevMem* b : {&word, &nmask, &own, &own16, &invD, &dadd, &dadd32, &bc, &tiles}) b->release();
+    }
 };
 
 // The V-cycle work vectors of one level in one solve context.
 struct LevelWork {
     DevMem r, z, t, d;
+    void release() {
+        for (DevMem* b : {&r, &z, &t, &d}) b->release();
+    }
 };
 
 // The hierarchy on the device: built once per handle, shared by its solve contexts.
@@ -1152,21 +1174,42 @@ struct SharedModel {
     bool ownDiff = false;
     bool mixedOwn16 = true;
     double foldFactor = 0.1;  // fold when the FP32 residual is this fraction of its peak
+    cudaStream_t ms = nullptr;     // allocation / upload stream of the shared data
+    cudaEvent_t readyEv = nullptr; // recorded when the uploads are done; contexts wait on it
+
+    ~SharedModel() {
+        for (auto& D : L) D.release();
+        cDof.release();
+        cInv.release();
+        if (ms) {
+            cudaStreamSynchronize(ms);
+            cudaStreamDestroy(ms);
+        }
+        if (readyEv) cudaEventDestroy(readyEv);
+    }
 
     void build(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsest, const double* diagAdd);
+    void adopt(Hierarchy&& h);  // upload a hierarchy built on the host beforehand
     void uploadLevel(int l);
     bool exactOneLevel() const { return L.size() == 1 && H.hasFactor(); }
 };
 
 void SharedModel::build(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsest, const double* diagAdd) {
-    H = buildHierarchy(dims, density, nu, bc, coarsest, diagAdd);
+    adopt(buildHierarchy(dims, density, nu, bc, coarsest, diagAdd));
+}
+
+void SharedModel::adopt(Hierarchy&& h) {
+    H = std::move(h);
     int devId = 0;
     check(cudaGetDevice(&devId), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, devId), "attribute");
     if (const char* e = std::getenv("PSFEA_OWN16_DIFF")) ownDiff = std::atoi(e) != 0;
     if (const char* e = std::getenv("PSFEA_FOLD")) foldFactor = std::atof(e);
     if (const char* e = std::getenv("PSFEA_MIXED_OWN32")) mixedOwn16 = std::atoi(e) == 0;
-    {
+    check(cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking), "stream");
+    check(cudaEventCreateWithFlags(&readyEv, cudaEventDisableTiming), "event");
+    static std::once_flag attrOnce;
+    std::call_once(attrOnce, [] {
         // the tiled operator stages more than the default 48 KB of shared memory
         const int s32 = int(dev::tileSmemBytes<float>()), s64 = int(dev::tileSmemBytes<double>());
         check(cudaFuncSetAttribute(dev::k_tile<double, dev::TOP_APPLY, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64), "attr");
@@ -1178,25 +1221,26 @@ void SharedModel::build(const int32_t dims[3], const float* density, double nu, 
         check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_RESID, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
         check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_CHEB, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
         check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_RESID, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
-    }
+    });
     L.resize(H.levels.size());
     for (int l = 0; l < int(H.levels.size()); l++) uploadLevel(l);
     m = int(H.coarseM);
     if (H.hasFactor()) {
-        upload(cDof, H.coarseDof, bytes);
-        upload(cInv, H.coarseInv, bytes);
+        upload(cDof, H.coarseDof, bytes, ms);
+        upload(cInv, H.coarseInv, bytes, ms);
     }
     for (auto& D : L) maxTiles = std::max(maxTiles, D.nTiles);
+    check(cudaEventRecord(readyEv, ms), "event");
 }
 
 void SharedModel::uploadLevel(int l) {
     const HostLevel& h = H.levels[size_t(l)];
     DevLevel& D = L[size_t(l)];
-    upload(D.word, h.word, bytes);
-    upload(D.nmask, h.nmask, bytes);
+    upload(D.word, h.word, bytes, ms);
+    upload(D.nmask, h.nmask, bytes, ms);
     D.hasOwn = h.nOwn > 0;
     if (D.hasOwn) {
-        upload(D.own, h.own, bytes);
+        upload(D.own, h.own, bytes, ms);
         // halves with a power-of-two level scale keeping the largest entry near 2^14
         double kmax = 0;
         for (float v : h.own) kmax = std::max(kmax, double(std::fabs(v)));
@@ -1206,17 +1250,17 @@ void SharedModel::uploadLevel(int l) {
         parallelFor(int64_t(h.own.size()), [&](int64_t lo, int64_t hi) {
             for (int64_t i = lo; i < hi; i++) h16[size_t(i)] = __float2half_rn(h.own[size_t(i)] * inv);
         });
-        upload(D.own16, h16, bytes);
+        upload(D.own16, h16, bytes, ms);
         D.view.hs = hs;
     }
     std::vector<float> invD(h.invDiag.begin(), h.invDiag.end());
-    upload(D.invD, invD, bytes);
+    upload(D.invD, invD, bytes, ms);
     if (!h.diagAdd.empty()) {
-        upload(D.dadd, h.diagAdd, bytes);
+        upload(D.dadd, h.diagAdd, bytes, ms);
         std::vector<float> d32(h.diagAdd.begin(), h.diagAdd.end());
-        upload(D.dadd32, d32, bytes);
+        upload(D.dadd32, d32, bytes, ms);
     }
-    if (l == 0) upload(D.bc, h.bc, bytes);
+    if (l == 0) upload(D.bc, h.bc, bytes, ms);
     {
         const int ntx = (h.NX + dev::TX - 1) / dev::TX, nty = (h.NY + dev::TY - 1) / dev::TY, ntz = (h.NZ + dev::TZ - 1) / dev::TZ;
         if (ntx > 2047 || nty > 2047 || ntz > 1023) throw Error(PS_EINVAL, "grid too large for the tile index");
@@ -1233,7 +1277,7 @@ void SharedModel::uploadLevel(int l) {
                 for (int tx = 0; tx < ntx; tx++)
                     if (act[size_t(tx + ntx * (ty + size_t(nty) * tz))]) list.push_back(dev::packTile(tx, ty, tz));
         D.nTiles = int(list.size());
-        upload(D.tiles, list, bytes);
+        upload(D.tiles, list, bytes, ms);
         // small levels have too few tiles to fill the GPU: one thread per node instead, or eight
         // lanes per node on the smallest ones
         int64_t minNodes = 400000;
@@ -1290,9 +1334,16 @@ struct SolverImpl {
     int64_t graphKernels[2] = {0, 0};
     int64_t graphVersion[2] = {-1, -1};
 
+    // smoother estimation in flight: its scratch (stream-ordered, freed as soon as the kernels
+    // have run) and the Lanczos scalars of every level, copied to pinned host memory
+    double* lzHost = nullptr;  // [12 levels][20]
+    bool lzPending = false;
+
     // the solve in progress (a resumable state machine, so one host thread can drive many)
     struct Pending {
-        bool active = false, finishing = false, mixed = false;
+        bool active = false, finishing = false, mixed = false, lanczos = false;
+        const double* fDev = nullptr;
+        const double* x0Dev = nullptr;
         ps_solve_opts o{};
         double* uDev = nullptr;
         double* uHost = nullptr;
@@ -1326,7 +1377,11 @@ struct SolverImpl {
         M->degree = want;
         M->smoothersReady = false;
     }
-    double lanczos(int l);
+    void enqueueLanczos(int l);       // 10 Lanczos steps of level l, scalars to lzHost[l]
+    bool enqueueAllLanczos();         // every level without an estimate; false if none
+    void finishLanczos();             // lmax of those levels from lzHost (after the event)
+    void computeCoefficients();
+    void startIterations();
 
     // operator launches
     void op64(int l, const double* x, double* y, bool raw, dev::Ctl ctl);
@@ -1364,9 +1419,15 @@ struct SolverImpl {
         if (ownStream) cudaStreamSynchronize(ownStream);
         for (auto& g : graph)
             if (g) cudaGraphExecDestroy(g);
+        for (auto& w : W) w.release();
+        for (DevMem* b : {&f, &x, &r, &p, &q, &z64, &x32, &p32, &q32, &state, &partials, &ticket}) b->release();
         if (ev) cudaEventDestroy(ev);
         if (hostState) cudaFreeHost(hostState);
-        if (ownStream) cudaStreamDestroy(ownStream);
+        if (lzHost) cudaFreeHost(lzHost);
+        if (ownStream) {
+            cudaStreamSynchronize(ownStream);
+            cudaStreamDestroy(ownStream);
+        }
     }
 };
 
@@ -1375,27 +1436,31 @@ void SolverImpl::allocate() {
     stream = ownStream;
     check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
     check(cudaMallocHost(&hostState, sizeof(dev::SolveState)), "cudaMallocHost");
+    check(cudaMallocHost(&lzHost, 12 * 20 * sizeof(double)), "cudaMallocHost");
+    cudaStream_t s = ownStream;
     W.resize(H.levels.size());
     for (size_t l = 0; l < W.size(); l++) {
         const size_t n = size_t(H.levels[l].nDof);
-        W[l].r.alloc(n * 4, bytes);
-        W[l].z.alloc(n * 4, bytes);
-        W[l].t.alloc(n * 4, bytes);
-        W[l].d.alloc(n * 4, bytes);
+        W[l].r.alloc(n * 4, bytes, s);
+        W[l].z.alloc(n * 4, bytes, s);
+        W[l].t.alloc(n * 4, bytes, s);
+        W[l].d.alloc(n * 4, bytes, s);
     }
     const size_t n = size_t(H.levels[0].nDof);
-    f.alloc(n * 8, bytes);
-    x.alloc(n * 8, bytes);
-    r.alloc(n * 8, bytes);
-    p.alloc(n * 8, bytes);
-    q.alloc(n * 8, bytes);
-    if (exactOneLevel()) z64.alloc(n * 8, bytes);
-    x32.alloc(n * 4, bytes);
-    p32.alloc(n * 4, bytes);
-    q32.alloc(n * 4, bytes);
-    state.alloc(sizeof(dev::SolveState), bytes);
-    partials.alloc(size_t(std::max(smCount * 16, M->maxTiles)) * 4 * sizeof(double) + 4096, bytes);
-    ticket.alloc(64, bytes);
+    f.alloc(n * 8, bytes, s);
+    x.alloc(n * 8, bytes, s);
+    r.alloc(n * 8, bytes, s);
+    p.alloc(n * 8, bytes, s);
+    q.alloc(n * 8, bytes, s);
+    if (exactOneLevel()) z64.alloc(n * 8, bytes, s);
+    x32.alloc(n * 4, bytes, s);
+    p32.alloc(n * 4, bytes, s);
+    q32.alloc(n * 4, bytes, s);
+    state.alloc(sizeof(dev::SolveState), bytes, s);
+    partials.alloc(size_t(std::max(smCount * 16, M->maxTiles)) * 4 * sizeof(double) + 4096, bytes, s);
+    ticket.alloc(64, bytes, s);
+    // the shared data is uploaded on the model's stream: this context's work starts after it
+    check(cudaStreamWaitEvent(s, M->readyEv, 0), "wait");
 }
 
 void SolverImpl::op64(int l, const double* xin, double* y, bool raw, dev::Ctl ctl) {
@@ -1499,20 +1564,21 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
 }
 
 // 10 Lanczos steps on D^-1/2 K D^-1/2 from the reference's LCG start vector (voxel_fea.cpp:579-610),
-// all on the device; the scalars come back once at the end and the host applies the reference's
-// stop rule (b <= 1e-12 |a| ends the sequence; later steps are ignored)
-double SolverImpl::lanczos(int l) {
+// all on the device and stream-ordered (scratch freed behind the kernels); the 20 scalars go to
+// pinned host memory and finishLanczos applies the reference's stop rule (b <= 1e-12 |a| ends the
+// sequence; later steps are ignored)
+void SolverImpl::enqueueLanczos(int l) {
     DevLevel& D = L[size_t(l)];
     const HostLevel& h = H.levels[size_t(l)];
     const int64_t n = h.nDof;
     int64_t scratch = 0;
     DevMem v, vp, w, xx, invD, ab;
-    v.alloc(size_t(n) * 8, scratch);
-    vp.alloc(size_t(n) * 8, scratch);
-    w.alloc(size_t(n) * 8, scratch);
-    xx.alloc(size_t(n) * 8, scratch);
-    ab.alloc(20 * sizeof(double), scratch);
-    upload(invD, h.invDiag, scratch);
+    v.alloc(size_t(n) * 8, scratch, stream);
+    vp.alloc(size_t(n) * 8, scratch, stream);
+    w.alloc(size_t(n) * 8, scratch, stream);
+    xx.alloc(size_t(n) * 8, scratch, stream);
+    ab.alloc(20 * sizeof(double), scratch, stream);
+    upload(invD, h.invDiag, scratch, stream);
     const int vg = vecGrid(n);
     launch(dev::k_lz_start, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, h.nNodes, D.view.nmask, v.as<double>(), part(), tick(), st());
     launch(dev::k_scale, vg, dev::VEC_THREADS, 0, stream, n, v.as<double>(), st());
@@ -1526,26 +1592,43 @@ double SolverImpl::lanczos(int l) {
         launch(dev::k_lz_axpy, vg, dev::VEC_THREADS, 0, stream, n, w.as<double>(), v.as<double>(), abp + s, abp + 10 + s, st(), part(), tick());
         launch(dev::k_lz_next, vg, dev::VEC_THREADS, 0, stream, n, w.as<double>(), v.as<double>(), vp.as<double>(), abp + 10 + s);
     }
-    double hab[20];
-    check(cudaMemcpyAsync(hab, abp, sizeof hab, cudaMemcpyDeviceToHost, stream), "lanczos read");
-    check(cudaStreamSynchronize(stream), "lanczos");
-    std::vector<double> alpha, beta;
-    for (int s = 0; s < 10; s++) {
-        const double a = hab[s], b = hab[10 + s];  // hab[10 + s] holds |w| after step s
-        alpha.push_back(a);
-        if (!(b > 1e-12 * std::fabs(a))) break;
-        beta.push_back(b);
-    }
-    beta.resize(alpha.size() - 1);
+    check(cudaMemcpyAsync(lzHost + 20 * l, abp, 20 * sizeof(double), cudaMemcpyDeviceToHost, stream), "lanczos read");
     check(cudaGetLastError(), "lanczos");
-    return tridiagonalMax(alpha, beta);
+}  // the scratch buffers are released here, stream-ordered behind the kernels
+
+bool SolverImpl::enqueueAllLanczos() {
+    bool any = false;
+    for (int l = 0; l + 1 < int(L.size()); l++)
+        if (!(H.levels[size_t(l)].lmax > 0)) {
+            enqueueLanczos(l);
+            any = true;
+        }
+    if (any) check(cudaEventRecord(ev, stream), "event");
+    lzPending = any;
+    return any;
 }
 
-void SolverImpl::prepareSmoothers() {
-    if (M->smoothersReady) return;
+void SolverImpl::finishLanczos() {
     for (int l = 0; l + 1 < int(L.size()); l++) {
         HostLevel& h = H.levels[size_t(l)];
-        if (!(h.lmax > 0)) h.lmax = lanczos(l);
+        if (h.lmax > 0) continue;
+        const double* hab = lzHost + 20 * l;
+        std::vector<double> alpha, beta;
+        for (int s = 0; s < 10; s++) {
+            const double a = hab[s], b = hab[10 + s];  // hab[10 + s] holds |w| after step s
+            alpha.push_back(a);
+            if (!(b > 1e-12 * std::fabs(a))) break;
+            beta.push_back(b);
+        }
+        beta.resize(alpha.size() - 1);
+        h.lmax = tridiagonalMax(alpha, beta);
+    }
+    lzPending = false;
+}
+
+void SolverImpl::computeCoefficients() {
+    for (int l = 0; l + 1 < int(L.size()); l++) {
+        HostLevel& h = H.levels[size_t(l)];
         DevLevel& D = L[size_t(l)];
         double c0, c1, c2;
         chebyshevCoefficients(h.lmax, c0, c1, c2);
@@ -1569,6 +1652,15 @@ void SolverImpl::prepareSmoothers() {
     // the coarsest level keeps the default Jacobi weight 0.5 (its eigenvalue is never estimated)
     M->smoothersReady = true;
     M->version++;
+}
+
+void SolverImpl::prepareSmoothers() {
+    if (M->smoothersReady) return;
+    if (enqueueAllLanczos()) {
+        check(cudaEventSynchronize(ev), "lanczos");
+        finishLanczos();
+    }
+    computeCoefficients();
 }
 
 // one FP64 CG iteration (voxel_fea.cpp:901-919)
@@ -1635,14 +1727,31 @@ void SolverImpl::startSolve(const double* fDev, const double* x0Dev, const ps_so
     pend.o = o;
     pend.uDev = uDev;
     pend.uHost = uHost;
+    pend.fDev = fDev;
+    pend.x0Dev = x0Dev;
+    pend.active = true;
+    setDegree(o.smoother_degree > 0 ? o.smoother_degree : 2);
+    if (!M->smoothersReady) {
+        // the smoother bounds first: their scalars come back with an event (advance() waits for it)
+        if (enqueueAllLanczos()) {
+            pend.lanczos = true;
+            return;
+        }
+        computeCoefficients();
+    }
+    startIterations();
+}
+
+void SolverImpl::startIterations() {
+    const double* fDev = pend.fDev;
+    const double* x0Dev = pend.x0Dev;
+    const ps_solve_opts& o = pend.o;
     const HostLevel& h = H.levels[0];
     DevLevel& D = L[0];
     LevelWork& W0 = W[0];
     const bool mixed = o.precision == PS_PREC_MIXED && !exactOneLevel();
     pend.mixed = mixed;
     const int64_t n = h.nDof;
-    setDegree(o.smoother_degree > 0 ? o.smoother_degree : 2);
-    prepareSmoothers();
     // state
     dev::SolveState s{};
     s.tol = o.tol;
@@ -1708,7 +1817,6 @@ void SolverImpl::startSolve(const double* fDev, const double* x0Dev, const ps_so
         graphVersion[gi] = M->version;
     }
     enqueueStateRead();
-    pend.active = true;
 }
 
 bool SolverImpl::advance(bool block, ps_solve_result& res) {
@@ -1718,6 +1826,13 @@ bool SolverImpl::advance(bool block, ps_solve_result& res) {
         const cudaError_t qe = cudaEventQuery(ev);
         if (qe == cudaErrorNotReady) return false;
         check(qe, "event query");
+    }
+    if (pend.lanczos) {
+        pend.lanczos = false;
+        if (lzPending) finishLanczos();
+        computeCoefficients();
+        startIterations();
+        return false;
     }
     const HostLevel& h = H.levels[0];
     DevLevel& D = L[0];
@@ -1812,6 +1927,38 @@ Solver::Solver(const int32_t dims[3], const float* density, double nu, const uin
     impl_.reset(I);
     I->allocate();
     handle_.reset(new SolverHandle{model, nullptr, {}});
+}
+
+Solver::Solver(Hierarchy&& hier) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        throw Error(PS_ENODEV, "no CUDA device is available");
+    }
+    auto model = std::make_shared<SharedModel>();
+    model->adopt(std::move(hier));
+    auto* I = new SolverImpl(model);
+    impl_.reset(I);
+    I->allocate();
+    handle_.reset(new SolverHandle{model, nullptr, {}});
+}
+
+int64_t estimateDeviceBytes(const Hierarchy& H) {
+    // what SharedModel::adopt and one SolverImpl::allocate take, plus allocation slack
+    int64_t b = 0, allocs = 0;
+    for (size_t l = 0; l < H.levels.size(); l++) {
+        const HostLevel& h = H.levels[l];
+        b += 4 * h.nVox + h.nNodes + 6 * 576 * h.nOwn + 4 * h.nDof + (h.diagAdd.empty() ? 0 : 12 * h.nDof) + 4 * (h.nNodes / 1024 + 1);
+        if (l == 0) b += h.nDof;
+        b += 16 * h.nDof;  // V-cycle vectors r, z, t, d
+        allocs += 12;
+    }
+    const int64_t n = H.levels[0].nDof;
+    b += 40 * n + 12 * n + (H.levels.size() == 1 ? 8 * n : 0);
+    b += 4 * H.coarseM + 8 * H.coarseM * H.coarseM;
+    b += 4096 * 32 + 64 * 1024;
+    allocs += 16;
+    return b + allocs * (64 << 10);
 }
 
 Solver::~Solver() {

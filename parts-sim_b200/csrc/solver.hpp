@@ -16,6 +16,8 @@ class Solver {
 public:
     // builds the hierarchy on the host and uploads it; throws Error
     Solver(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsestMaxDof, const double* diagAdd);
+    // uploads a hierarchy built beforehand (buildHierarchy may run on any host thread)
+    explicit Solver(Hierarchy&& hier);
     ~Solver();
 
     const Hierarchy& hierarchy() const;
@@ -53,5 +55,8 @@ private:
     std::unique_ptr<SolverImpl> impl_;
     std::unique_ptr<SolverHandle> handle_;
 };
+
+// device bytes a Solver over this hierarchy takes (its data and one solve context), for admission
+int64_t estimateDeviceBytes(const Hierarchy& H);
 
 }  // namespace psfea

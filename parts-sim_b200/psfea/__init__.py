@@ -15,10 +15,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpsfea.so")
 
-PS_OK, PS_NOT_CONVERGED, PS_BREAKDOWN, PS_CANCELLED, PS_TIMEOUT = 0, 1, 2, 3, 4
+PS_OK, PS_NOT_CONVERGED, PS_BREAKDOWN, PS_CANCELLED, PS_TIMEOUT, PS_PENDING = 0, 1, 2, 3, 4, 5
 PS_EINVAL, PS_ENONFINITE, PS_EOOM, PS_ECUDA, PS_ENODEV = 10, 11, 12, 13, 14
 PREC = {"fp64": 0, "mixed": 1}
-STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "CANCELLED", 4: "TIMEOUT", 10: "EINVAL", 11: "ENONFINITE",
+STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "CANCELLED", 4: "TIMEOUT", 5: "PENDING", 10: "EINVAL", 11: "ENONFINITE",
                 12: "EOOM", 13: "ECUDA", 14: "ENODEV"}
 
 
@@ -30,6 +30,23 @@ class SolveOpts(C.Structure):
 class SolveResultC(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("status", C.c_int32), ("folds", C.c_int32),
                 ("residual", C.c_double), ("seconds", C.c_double), ("kernels", C.c_int64)]
+
+
+class PsRequest(C.Structure):
+    _fields_ = [("dims", C.c_int32 * 3), ("density", C.c_void_p), ("nu", C.c_double), ("bc", C.c_void_p), ("f", C.c_void_p),
+                ("coarsest_max_dof", C.c_int64), ("tol", C.c_double), ("max_iter", C.c_int32), ("precision", C.c_int32),
+                ("smoother_degree", C.c_int32)]
+
+
+class PsRequestResult(C.Structure):
+    _fields_ = [("id", C.c_int64), ("status", C.c_int32), ("iterations", C.c_int32), ("converged", C.c_int32), ("residual", C.c_double),
+                ("n_dof", C.c_int64), ("u", C.c_void_p), ("build_s", C.c_double), ("wait_s", C.c_double), ("solve_s", C.c_double),
+                ("total_s", C.c_double)]
+
+
+class PsServerStats(C.Structure):
+    _fields_ = [("queued", C.c_int64), ("active", C.c_int64), ("completed", C.c_int64), ("device_bytes_in_use", C.c_int64),
+                ("peak_device_bytes", C.c_int64), ("budget_bytes", C.c_int64), ("peak_active", C.c_int64)]
 
 
 if not os.path.exists(LIB_PATH):
@@ -69,6 +86,13 @@ _dev_bytes = _sig("ps_fea_device_bytes", C.c_int64, _P)
 _set_stream = _sig("ps_fea_set_stream", C.c_int, _P, C.c_void_p)
 _time_kernel = _sig("ps_fea_time_kernel", C.c_int, _P, C.c_int32, C.c_int32, C.POINTER(C.c_double))
 _launches = _sig("ps_fea_kernel_launches", C.c_int64, _P)
+_srv_create = _sig("ps_server_create", C.c_int, C.c_int64, C.c_int32, C.c_int32, C.POINTER(C.c_void_p))
+_srv_submit = _sig("ps_server_submit", C.c_int, _P, C.POINTER(PsRequest), C.POINTER(C.c_int64))
+_srv_poll = _sig("ps_server_poll", C.c_int, _P, C.c_int64, C.POINTER(PsRequestResult))
+_srv_wait = _sig("ps_server_wait", C.c_int, _P, C.c_int64, C.POINTER(PsRequestResult))
+_srv_release = _sig("ps_server_release", C.c_int, _P, C.c_int64)
+_srv_stats = _sig("ps_server_get_stats", C.c_int, _P, C.POINTER(PsServerStats))
+_srv_destroy = _sig("ps_server_destroy", None, _P)
 _apply_dot_noalloc = _sig("ps_fea_apply_dot_noalloc", C.c_int, _P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
 _element = _sig("ps_element_matrix", C.c_int, C.c_double, _F64P, C.c_void_p)
 _prune = _sig("ps_prune_floating", C.c_int, _I32P, _F32P, _U8P, _F32P, C.POINTER(C.c_int32))
@@ -88,7 +112,9 @@ EXPORTS = ("ps_solve_opts_default", "ps_fea_create", "ps_fea_solve", "ps_fea_sol
            "ps_fea_level_fixed", "ps_fea_level_lmax", "ps_fea_device_bytes", "ps_fea_destroy", "ps_element_matrix",
            "ps_prune_floating", "ps_last_error", "ps_hierarchy_create", "ps_hierarchy_num_levels", "ps_hierarchy_level_info",
            "ps_hierarchy_level_fixed", "ps_hierarchy_level_own", "ps_hierarchy_level_kb", "ps_hierarchy_destroy",
-           "ps_fea_set_stream", "ps_fea_time_kernel", "ps_fea_kernel_launches", "ps_fea_apply_dot_noalloc")
+           "ps_fea_set_stream", "ps_fea_time_kernel", "ps_fea_kernel_launches", "ps_fea_apply_dot_noalloc",
+           "ps_server_create", "ps_server_submit", "ps_server_poll", "ps_server_wait", "ps_server_release", "ps_server_get_stats",
+           "ps_server_destroy")
 
 
 class SolverError(RuntimeError):
@@ -381,3 +407,80 @@ def prune_floating(dims, density, held_node):
     if st != PS_OK:
         _raise(st)
     return out, int(removed.value)
+
+
+class Server:
+    """Continuous-batching request loop (ps_server_*): submit solves at any time, each is built on
+    host threads, admitted to the GPU by memory footprint and run concurrently with the others."""
+
+    def __init__(self, budget_bytes=0, max_active=0, build_threads=0):
+        h = C.c_void_p()
+        st = _srv_create(int(budget_bytes), int(max_active), int(build_threads), C.byref(h))
+        if st != PS_OK:
+            _raise(st)
+        self.h = h
+
+    def submit(self, dims, density, nu, bc, f, tol=1e-8, max_iter=5000, precision="mixed", coarsest_max_dof=300, smoother_degree=0):
+        density = np.ascontiguousarray(density, np.float32).ravel()
+        bc = np.ascontiguousarray(bc, np.uint8).ravel()
+        f = np.ascontiguousarray(f, np.float64).ravel()
+        q = PsRequest()
+        q.dims[:] = [int(v) for v in dims]
+        q.density, q.bc, q.f = _ptr(density), _ptr(bc), _ptr(f)
+        q.nu = float(nu)
+        q.coarsest_max_dof = int(coarsest_max_dof)
+        q.tol = float(tol)
+        q.max_iter = int(max_iter)
+        q.precision = PREC[precision] if isinstance(precision, str) else int(precision)
+        q.smoother_degree = int(smoother_degree)
+        rid = C.c_int64()
+        st = _srv_submit(self.h, C.byref(q), C.byref(rid))
+        if st != PS_OK:
+            _raise(st)
+        return int(rid.value)
+
+    @staticmethod
+    def _result(r, keep_u=True):
+        u = None
+        if keep_u and r.u:
+            u = np.ctypeslib.as_array(C.cast(r.u, C.POINTER(C.c_double)), shape=(r.n_dof,)).copy()
+        return {"id": r.id, "status": r.status, "iterations": r.iterations, "converged": bool(r.converged), "residual": r.residual,
+                "n_dof": r.n_dof, "u": u, "build_s": r.build_s, "wait_s": r.wait_s, "solve_s": r.solve_s, "total_s": r.total_s}
+
+    def wait(self, rid, keep_u=True, release=True):
+        r = PsRequestResult()
+        st = _srv_wait(self.h, int(rid), C.byref(r))
+        if st != PS_OK:
+            _raise(st)
+        out = self._result(r, keep_u)
+        if release:
+            _srv_release(self.h, int(rid))
+        return out
+
+    def poll(self, rid, keep_u=True, release=True):
+        r = PsRequestResult()
+        st = _srv_poll(self.h, int(rid), C.byref(r))
+        if st == PS_PENDING:
+            return None
+        if st != PS_OK:
+            _raise(st)
+        out = self._result(r, keep_u)
+        if release:
+            _srv_release(self.h, int(rid))
+        return out
+
+    def stats(self):
+        s = PsServerStats()
+        _srv_stats(self.h, C.byref(s))
+        return {k: getattr(s, k) for k, _ in PsServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            _srv_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

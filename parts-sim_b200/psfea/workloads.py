@@ -275,22 +275,30 @@ def box_with_voids(rng, lo=24, hi=160, solid_target=0.6, h=1e-3):
     radius U[2, 10] voxels placed until the solid fraction reaches ``solid_target``, material
     drawn from MATERIALS, one random face held and a uniform traction with a random direction and
     log-uniform magnitude in [0.1, 10] MPa on the opposite face; floating fragments pruned."""
+    from . import prune_floating as _prune  # the library's breadth-first search
     u = rng.uniform(3)
     dims = tuple(int(round(np.exp(np.log(lo) + (np.log(hi) - np.log(lo)) * v))) for v in u)
     nx, ny, nz = dims
     solid = np.ones((nz, ny, nx), bool)
-    zz, yy, xx = np.meshgrid(np.arange(nz) + 0.5, np.arange(ny) + 0.5, np.arange(nx) + 0.5, indexing="ij")
     total = nx * ny * nz
-    tries = 0
-    while solid.sum() > solid_target * total and tries < 2000:
-        c = rng.uniform(4)
-        cx, cy, cz, r = c[0] * nx, c[1] * ny, c[2] * nz, 2 + 8 * c[3]
-        lo_ = [max(0, int(v - r)) for v in (cz, cy, cx)]
-        hi_ = [min(n, int(v + r) + 1) for v, n in zip((cz, cy, cx), (nz, ny, nx))]
-        sl = tuple(slice(a, b) for a, b in zip(lo_, hi_))
-        m = (xx[sl] - cx) ** 2 + (yy[sl] - cy) ** 2 + (zz[sl] - cz) ** 2 < r * r
-        solid[sl] &= ~m
-        tries += 1
+    removed = 0
+    # voids in rounds (each round's centres drawn at once); a round stops at the target
+    while total - removed > solid_target * total:
+        c = rng.uniform(4 * 32).reshape(32, 4)
+        for cx, cy, cz, cr in c:
+            cx, cy, cz, r = cx * nx, cy * ny, cz * nz, 2 + 8 * cr
+            k0, k1 = max(0, int(cz - r)), min(nz, int(cz + r) + 1)
+            j0, j1 = max(0, int(cy - r)), min(ny, int(cy + r) + 1)
+            i0, i1 = max(0, int(cx - r)), min(nx, int(cx + r) + 1)
+            zz = (np.arange(k0, k1) + 0.5 - cz)[:, None, None] ** 2
+            yy = (np.arange(j0, j1) + 0.5 - cy)[None, :, None] ** 2
+            xx = (np.arange(i0, i1) + 0.5 - cx)[None, None, :] ** 2
+            m = zz + yy + xx < r * r
+            sub = solid[k0:k1, j0:j1, i0:i1]
+            removed += int((sub & m).sum())
+            sub &= ~m
+            if total - removed <= solid_target * total:
+                break
     mat = MATERIALS[int(rng.uniform(1)[0] * 3) % 3]
     face = int(rng.uniform(1)[0] * 6) % 6
     axis, side = face // 2, face % 2
@@ -299,19 +307,21 @@ def box_with_voids(rng, lo=24, hi=160, solid_target=0.6, h=1e-3):
     sl = [slice(None)] * 3
     sl[2 - axis] = 0 if side == 0 else dims[axis]
     bc[tuple(sl)] = 1
-    density = solid.astype(np.float32).ravel()
-    density, removed = prune_floating(dims, density, bc.ravel())
+    held = bc.reshape(-1, 3).max(axis=1)
+    density, nrem = _prune(dims, solid.astype(np.float32).ravel(), held)
     d = rng.normal(3)
     d /= np.linalg.norm(d)
     mag = np.exp(np.log(0.1e6) + (np.log(10e6) - np.log(0.1e6)) * rng.uniform(1)[0])
     f, nface = _face_load(dims, density, axis, 1 - side, d * mag * h * h)
-    return Model("request", dims, density, bc.ravel(), f, mat[1], mat[0], h, 1100,
-                 {"face": face, "traction_Pa": mag, "removed": removed})
+    return Model("request", dims, density, bc.ravel(), f, mat[1], mat[0], h, 300,
+                 {"face": face, "traction_Pa": mag, "removed": nrem})
 
 
 def serving_stream(n=512, rate=200.0, seed=5):
-    """``n`` requests with Poisson arrival times at ``rate`` per second: list of (t_arrival, Model)."""
+    """``n`` requests with Poisson arrival times at ``rate`` per second: a generator of
+    (t_arrival, Model), each request from its own sub-seed (so any prefix is reproducible)."""
     rng = Rng(seed)
     gaps = -np.log1p(-rng.uniform(n)) / rate
     t = np.cumsum(gaps)
-    return [(float(t[q]), box_with_voids(rng)) for q in range(n)]
+    for q in range(n):
+        yield float(t[q]), box_with_voids(Rng(seed * 1000003 + q))

@@ -100,3 +100,10 @@ def test_no_device_is_reported_not_faked(have_gpu):
         pytest.skip("a GPU is present")
     with pytest.raises(psfea.SolverError, match="ENODEV"):
         psfea.VoxelFEA((4, 1, 1), np.ones(4, np.float32), 0.3, np.zeros(3 * 5 * 2 * 2, np.uint8))
+
+
+def test_server_needs_a_device(have_gpu):
+    if have_gpu:
+        pytest.skip("a GPU is present")
+    with pytest.raises(psfea.SolverError, match="ENODEV"):
+        psfea.Server()
