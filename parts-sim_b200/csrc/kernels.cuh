@@ -1,12 +1,17 @@
 // Device code of the voxel solve (sm_100a). Included by solver.cu only.
 //
-// Data layout in HBM, per level: xyz-interleaved DOF vectors (DOF 3n + d, node n = i + NX (j + NY k),
-// the reference's layout), one 32-bit word per voxel (0 empty, float bits of s for s * Kb,
-// OWN_BIT | index of an own 24x24 matrix), one mask byte per node (fixed DOFs, active, uniform).
+// Data layout in HBM, per level: xyz-interleaved DOF vectors (DOF 3n + d) over pitched node rows,
+// node n = i + PX (j + NY k) with the row pitch PX = NX rounded up to a multiple of 4, so that every
+// row of 3 PX values starts on a 16-byte boundary (the rule of tensor-memory-access copies); the
+// padding nodes i >= NX are inactive with all DOFs held, and stay 0 in every vector. One 32-bit word
+// per voxel (0 empty, float bits of s for s * Kb, OWN_BIT | index of an own 24x24 matrix) over rows
+// of px = nx rounded up to a multiple of 4 words (padding words 0), one mask byte per node (fixed
+// DOFs, active, uniform). The reference's dense layout (pitch NX) exists only at the C ABI.
 // The level's Kb (576) and its assembled 27-point stencil (243) travel as kernel parameters, so
 // every coefficient is a constant-bank operand of the FMA that uses it.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cstdint>
 
@@ -17,8 +22,9 @@ constexpr uint32_t OWN_BIT = 0x80000000u;
 constexpr uint8_t NM_ACTIVE = 8, NM_UNIFORM = 16;
 
 struct LevelView {
-    int nx, ny, nz, NX, NY, NZ;
-    long long nNodes;
+    int nx, ny, nz, NX, NY, NZ;  // voxel and node counts per axis
+    int PX, px;                  // row pitches: nodes (PX >= NX) and voxel words (px >= nx), multiples of 4
+    long long nNodes;            // PX NY NZ: the length of every per-node array
     const uint32_t* word;
     const uint8_t* nmask;
     const float* own;       // own matrices, 32-bit
@@ -27,6 +33,7 @@ struct LevelView {
     const double* dadd;     // diagonal shift per DOF, or null
     const float* dadd32;
     const float* invD;      // 1 / diag per DOF (0 where fixed), 32-bit
+    __host__ __device__ long long wi(int i, int j, int k) const { return i + (long long)px * (j + (long long)ny * k); }
 };
 
 template <class T>
@@ -49,12 +56,15 @@ __host__ __device__ constexpr int cornerOf(int x, int y, int z) { return (y ? (x
 // the FP32 CG accurate on smooth search directions. (The reference's WGSL kernel forms its
 // products the same way, native/shaders/fea.wgsl:91-92.) The diagonal shift is not a
 // translation-free term and always uses x_n itself.
+//
+// x is read at node index n with row pitch XP (L.PX for the level's own vectors); the diagonal
+// shift at the level's node index nm.
 template <class T, bool OWN16, bool DIFF = false>
 __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, const T* __restrict__ x, int i, int j, int k,
-                                        long long n, uint8_t mask, T acc[3]) {
+                                        long long n, uint8_t mask, T acc[3], long long XP, long long nm) {
     acc[0] = acc[1] = acc[2] = T(0);
     if (!(mask & NM_ACTIVE)) return;
-    const long long NX = L.NX, NXY = (long long)L.NX * L.NY;
+    const long long NX = XP, NXY = XP * L.NY;
     T own0 = 0, own1 = 0, own2 = 0;
     if (DIFF) {
         own0 = __ldg(x + 3 * n);
@@ -62,7 +72,7 @@ __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, c
         own2 = __ldg(x + 3 * n + 2);
     }
     if (mask & NM_UNIFORM) {
-        const float s = __uint_as_float(__ldg(L.word + ((i - 1) + (long long)L.nx * ((j - 1) + (long long)L.ny * (k - 1)))));
+        const float s = __uint_as_float(__ldg(L.word + L.wi(i - 1, j - 1, k - 1)));
         T a0 = 0, a1 = 0, a2 = 0;
 #pragma unroll
         for (int m = 0; m < 27; m++) {
@@ -86,7 +96,7 @@ __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, c
             const int di = v & 1, dj = (v >> 1) & 1, dk = v >> 2;
             const int ei = i - 1 + di, ej = j - 1 + dj, ek = k - 1 + dk;
             if (ei < 0 || ej < 0 || ek < 0 || ei >= L.nx || ej >= L.ny || ek >= L.nz) continue;
-            const uint32_t w = __ldg(L.word + (ei + (long long)L.nx * (ej + (long long)L.ny * ek)));
+            const uint32_t w = __ldg(L.word + L.wi(ei, ej, ek));
             if (w == 0) continue;
             const int a = cornerOf(1 - di, 1 - dj, 1 - dk);
             // the voxel's 8 corner values
@@ -138,13 +148,13 @@ __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, c
     }
     if (L.dadd) {
 #pragma unroll
-        for (int d = 0; d < 3; d++) acc[d] += (sizeof(T) == 8 ? T(L.dadd[3 * n + d]) : T(L.dadd32[3 * n + d])) * x[3 * n + d];
+        for (int d = 0; d < 3; d++) acc[d] += (sizeof(T) == 8 ? T(L.dadd[3 * nm + d]) : T(L.dadd32[3 * nm + d])) * x[3 * n + d];
     }
 }
 
 __device__ __forceinline__ void nodeCoords(const LevelView& L, long long n, int& i, int& j, int& k) {
-    const long long row = n / L.NX;
-    i = int(n - row * L.NX);
+    const long long row = n / L.PX;
+    i = int(n - row * L.PX);
     j = int(row % L.NY);
     k = int(row / L.NY);
 }
@@ -227,57 +237,117 @@ namespace dev {
 
 // ---------------------------------------------------------------- tiled operator
 //
-// One CTA per 32 x 8 x 8 node tile (only tiles with an active node are launched). The CTA stages
-// the tile's x values with a one-node halo (34 x 10 x 10 nodes) and the voxel words around it
-// (33 x 9 x 9) in shared memory with one burst of coalesced loads, all in flight together, then
-// computes its 2048 nodes from shared memory: uniform nodes with the 153-FMA assembled stencil,
-// the other active nodes (compacted in a fixed order) with the per-voxel gather, so the two code
-// paths never share a warp. Inactive nodes of the tile are written 0; inactive tiles are never
-// touched (their outputs are 0 already).
+// One CTA per 32 x 8 x 4 node tile (only tiles with an active node are launched). One thread stages
+// everything the tile needs with tensor-memory-access (TMA) copies, all in flight together on one
+// shared-memory barrier: the x values with a one-node halo, the voxel words around the tile and,
+// for the smoother and residual epilogues, the tile's r, d and 1/diag. The CTA then computes its
+// 1024 nodes from shared memory: uniform nodes with the 153-FMA assembled stencil, the other active
+// nodes (compacted in a fixed order) with the per-voxel gather, so the two code paths never share
+// a warp; the epilogue runs in shared memory and one thread writes the results back with TMA
+// stores. Inactive nodes of the tile are written 0; inactive tiles are never touched (their
+// outputs are 0 already).
+//
+// TMA boxes start on 16-byte boundaries: node rows are pitched (PX, a multiple of 4) and the halo
+// box starts 4 nodes (12 values) left of the tile instead of 1, the voxel box 4 words left of it;
+// boxes reaching outside the grid read zeros.
 
 constexpr int TX = 32, TY = 8, TZ = 4, TILE_THREADS = TX * TY, TILE_NODES = TX * TY * TZ;
-constexpr int HX = TX + 2, HY = TY + 2, HZ = TZ + 2, PROW = 3 * HX;  // x with halo; values per row
-constexpr int VX = TX + 1, VY = TY + 1, VZ = TZ + 1;                 // voxel words with halo
+constexpr int HY = TY + 2, HZ = TZ + 2;          // x halo rows and planes
+constexpr int XLEFT = 4;                         // halo box starts XLEFT nodes left of the tile
+constexpr int PROW = 112;                        // halo box row: nodes i0-4 .. i0+33, 112 values
+constexpr int VX = TX + 1, VY = TY + 1, VZ = TZ + 1;  // voxel words needed per axis
+constexpr int WROW = 40;                         // voxel box row: words i0-4 .. i0+35
+constexpr int TROW = 3 * TX;                     // tile box row (r, d, 1/diag, y): 96 values
+static_assert(3 * (TX + 1 + XLEFT) <= PROW, "halo row");
+static_assert(VX + XLEFT - 1 <= WROW, "voxel row");
 
 enum { TOP_APPLY = 0, TOP_CHEB = 1, TOP_RESID = 2, TOP_DOT = 3 };
 
+// tensor maps of one tiled launch: x (halo box), the voxel words, r, d, 1/diag and y (tile boxes)
+struct TileMaps {
+    CUtensorMap x, w, r, d, inv, y;
+};
+
 template <class T>
 struct TileIO {
-    const T* x;        // input vector
-    T* y;              // output vector
-    const float* r;    // CHEB / RESID: right-hand side (32-bit level vectors)
-    float* d;          // CHEB: Chebyshev direction, updated in place
     float c1, c2;      // CHEB: d = c1 d + c2 D^-1 (r - K x)
     int raw;           // APPLY: keep held DOFs
 };
 
 __host__ __device__ constexpr uint32_t packTile(int tx, int ty, int tz) { return uint32_t(tx) | (uint32_t(ty) << 11) | (uint32_t(tz) << 22); }
 
-// x halo, voxel words, per-node K x results (row-major like the global tile rows), node masks,
-// the gather list and the warp counts
-// every part starts on a 16-byte boundary
-__host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
-template <class T> __host__ __device__ constexpr size_t tileOffV() { return align16(sizeof(T) * HZ * HY * PROW); }
-template <class T> __host__ __device__ constexpr size_t tileOffK() { return tileOffV<T>() + align16(sizeof(uint32_t) * VZ * VY * VX); }
-template <class T> __host__ __device__ constexpr size_t tileOffM() { return tileOffK<T>() + align16(sizeof(T) * 3 * TILE_NODES); }
-template <class T> __host__ __device__ constexpr size_t tileOffB() { return tileOffM<T>() + align16(TILE_NODES); }
-template <class T> __host__ __device__ constexpr size_t tileSmemBytes() { return tileOffB<T>() + sizeof(int) * (TILE_NODES + 32); }
+// shared-memory layout of a tile CTA, every TMA destination on a 128-byte boundary:
+// x halo, voxel words, K x per tile node (then the y tile), r, d, 1/diag (smoother / residual),
+// node masks, the gather list, the warp counts and the barrier
+__host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
+__host__ __device__ constexpr bool tileHasR(int mode) { return mode == TOP_CHEB || mode == TOP_RESID; }
+__host__ __device__ constexpr bool tileHasD(int mode) { return mode == TOP_CHEB; }
+template <class T> __host__ __device__ constexpr size_t tileBytesX() { return sizeof(T) * PROW * HY * HZ; }
+__host__ __device__ constexpr size_t tileBytesW() { return sizeof(uint32_t) * WROW * VY * VZ; }
+template <class T> __host__ __device__ constexpr size_t tileBytesT() { return sizeof(T) * TROW * TY * TZ; }
+template <class T> __host__ __device__ constexpr size_t tileOffW() { return align128(tileBytesX<T>()); }
+template <class T> __host__ __device__ constexpr size_t tileOffK() { return tileOffW<T>() + align128(tileBytesW()); }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileOffR() { return tileOffK<T>() + align128(tileBytesT<T>()); }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileOffD() { return tileOffR<T, MODE>() + (tileHasR(MODE) ? align128(tileBytesT<float>()) : 0); }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileOffI() { return tileOffD<T, MODE>() + (tileHasD(MODE) ? align128(tileBytesT<float>()) : 0); }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileOffM() { return tileOffI<T, MODE>() + (tileHasD(MODE) ? align128(tileBytesT<float>()) : 0); }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileOffB() { return tileOffM<T, MODE>() + align128(TILE_NODES); }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileOffBar() { return tileOffB<T, MODE>() + align128(2 * TILE_NODES + 4 * 8); }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileSmemBytes() { return tileOffBar<T, MODE>() + 16; }
+// bytes the staging barrier expects
+template <class T, int MODE> __host__ __device__ constexpr unsigned tileStageBytes() {
+    return unsigned(tileBytesX<T>() + tileBytesW() + (tileHasR(MODE) ? tileBytesT<float>() : 0) + (tileHasD(MODE) ? 2 * tileBytesT<float>() : 0));
+}
 
-// asynchronous global -> shared copy of one 4- or 8-byte element, zero-filled when !valid
-template <int BYTES>
-__device__ __forceinline__ void cpAsync(void* dst, const void* src, bool valid) {
-    const unsigned d = unsigned(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES), "r"(valid ? BYTES : 0) : "memory");
+// ---- TMA and shared-memory barrier primitives (PTX, sm_90 and later; no cluster multicast)
+__device__ __forceinline__ unsigned smemAddr(const void* p) { return unsigned(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbarInit(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
-__device__ __forceinline__ void cpAsyncWaitAll() {
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+__device__ __forceinline__ void mbarExpectTx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
 }
+__device__ __forceinline__ bool mbarTryWait(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smemAddr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for the barrier's phase 0: false after `limit` polls (each poll may suspend the
+// thread for a hardware-defined time)
+__device__ __forceinline__ bool mbarWait(uint64_t* bar, unsigned limit) {
+    for (unsigned it = 0; it < limit; it++)
+        if (mbarTryWait(bar, 0)) return true;
+    return false;
+}
+// 3-D tiled load of a box at element coordinates (c0, c1, c2) into shared memory, completing on bar
+__device__ __forceinline__ void tmaLoad3d(void* dst, const void* map, int c0, int c1, int c2, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(smemAddr(dst)),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smemAddr(bar))
+        : "memory");
+}
+// 3-D tiled store of a shared-memory box to (c0, c1, c2), c0..c2 >= 0; elements outside the tensor are skipped
+__device__ __forceinline__ void tmaStore3d(const void* map, const void* src, int c0, int c1, int c2) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];\n" ::"l"(map), "r"(smemAddr(src)), "r"(c0),
+                 "r"(c1), "r"(c2)
+                 : "memory");
+}
+__device__ __forceinline__ void tmaStoreCommitWait() {
+    asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+}
+// makes this thread's shared-memory writes visible to later TMA (async proxy) reads
+__device__ __forceinline__ void fenceAsyncShared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
 // shared-memory offsets of x value (node tx + ox, ty + oy, tz + oz of the tile, component 0) and of
-// the voxel word at tile voxel (vx, vy, vz) (both with the halo offset of one)
-__device__ __forceinline__ int xOff(int cx, int cy, int cz) { return ((cz + 1) * HY + (cy + 1)) * PROW + 3 * (cx + 1); }
-__device__ __forceinline__ int vOff(int vx, int vy, int vz) { return (vz * VY + vy) * VX + vx; }
+// the voxel word at tile voxel (vx, vy, vz) (voxel i0 - 1 + vx, ...)
+__device__ __forceinline__ int xOff(int cx, int cy, int cz) { return ((cz + 1) * HY + (cy + 1)) * PROW + 3 * (cx + XLEFT); }
+__device__ __forceinline__ int vOff(int vx, int vy, int vz) { return (vz * VY + vy) * WROW + vx + XLEFT - 1; }
 
 template <class T, bool OWN16, bool DIFF>
 struct TileOp {

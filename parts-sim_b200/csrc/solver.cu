@@ -23,7 +23,9 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <map>
 #include <memory>
+#include <tuple>
 #include <mutex>
 #include <thread>
 #include <cmath>
@@ -46,6 +48,7 @@ struct SolveState {
     double bnorm, rel, tol, rz, alpha, beta, rmax, scale, peak, est, pq, foldFactor;
     double vscale;  // the scale the current FP32 right-hand side r32 was made with (r32 = r * vscale)
     int it, maxIter, done, status, fold, folds, first, mixed;
+    int err;  // a device-side failure (ST_ERR_*): the solve is ended and reported as a CUDA error
 };
 enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_BREAKDOWN = 3 };
 
@@ -83,7 +86,7 @@ __global__ void __launch_bounds__(NODE_THREADS) k_op(LevelView L, Coefs<T> C, co
         int i, j, k;
         nodeCoords(L, n, i, j, k);
         T acc[3];
-        applyAt<T, OWN16, DIFF>(L, C, x, i, j, k, n, mask, acc);
+        applyAt<T, OWN16, DIFF>(L, C, x, i, j, k, n, mask, acc, L.PX, n);
 #pragma unroll
         for (int q = 0; q < 3; q++) {
             const long long id = 3 * n + q;
@@ -118,7 +121,7 @@ __global__ void __launch_bounds__(NODE_THREADS) k_apply_alpha(LevelView L, Coefs
         int i, j, k;
         nodeCoords(L, n, i, j, k);
         T acc[3];
-        applyAt<T, OWN16, (sizeof(T) == 4)>(L, C, p, i, j, k, n, mask, acc);
+        applyAt<T, OWN16, (sizeof(T) == 4)>(L, C, p, i, j, k, n, mask, acc, L.PX, n);
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const T y = fixedDof(mask, c) ? T(0) : acc[c];
@@ -156,7 +159,7 @@ __global__ void __launch_bounds__(256) k_op8(LevelView L, Coefs<T> C, const T* _
     __syncthreads();
     const int lane = threadIdx.x & 31, v = lane & 7, group = lane >> 3;
     const int di = v & 1, dj = (v >> 1) & 1, dk = v >> 2, a = cornerOf(1 - di, 1 - dj, 1 - dk);
-    const long long NX = L.NX, NXY = (long long)L.NX * L.NY;
+    const long long NX = L.PX, NXY = (long long)L.PX * L.NY;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
     for (long long nb = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4; nb < L.nNodes; nb += warps * 4) {
         const long long n = nb + group;
@@ -169,7 +172,7 @@ __global__ void __launch_bounds__(256) k_op8(LevelView L, Coefs<T> C, const T* _
             const int ei = i - 1 + di, ej = j - 1 + dj, ek = k - 1 + dk;
             uint32_t w = 0;
             if (ei >= 0 && ej >= 0 && ek >= 0 && ei < L.nx && ej < L.ny && ek < L.nz)
-                w = __ldg(L.word + (ei + (long long)L.nx * (ej + (long long)L.ny * ek)));
+                w = __ldg(L.word + L.wi(ei, ej, ek));
             if (w) {
                 T own[3] = {T(0), T(0), T(0)};
                 if (DIFF) {
@@ -265,74 +268,20 @@ __global__ void __launch_bounds__(256) k_op8(LevelView L, Coefs<T> C, const T* _
 //   TOP_RESID  y = r - K x
 //   TOP_DOT    y = K x (held 0) and the CG step alpha = rz / (x . y); x . y <= 0 is a breakdown
 //              (voxel_fea.cpp:902-905)
+// A staging barrier that never completes (it cannot in a correct launch) is given up after a
+// bounded wait: the CTA records ST_ERR_STAGING in st->err and ends the solve.
+constexpr unsigned TILE_WAIT_POLLS = 1u << 22;
+constexpr int ST_ERR_STAGING = 1, ST_ERR_ALIGN = 2;
+
+// the staged tile's compute passes and epilogue (block-uniform: every thread calls it)
 template <class T, int MODE, bool OWN16, bool DIFF>
-__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? 2 : 3) k_tile(LevelView L, Coefs<T> C, const uint32_t* __restrict__ tiles, TileIO<T> io,
-                                                      SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
-    if (skipped(ctl)) return;
+__device__ __forceinline__ void tileBody(const LevelView& L, const Coefs<T>& C, const TileIO<T>& io, const TileMaps& maps, int i0, int j0,
+                                         int k0, const uint8_t (&mk)[TZ], bool anyUniform, const T* xs, const uint32_t* vs, T* ks,
+                                         const float* rs, float* ds, const float* is, const uint8_t* ms, uint16_t* blist, int* wsum,
+                                         double& dot) {
     using Op = TileOp<T, OWN16, DIFF>;
-    extern __shared__ __align__(16) unsigned char smem[];
-    T* xs = reinterpret_cast<T*>(smem);
-    uint32_t* vs = reinterpret_cast<uint32_t*>(smem + tileOffV<T>());
-    T* ks = reinterpret_cast<T*>(smem + tileOffK<T>());  // K x per tile node, [z][y][3 x + c]
-    uint8_t* ms = smem + tileOffM<T>();
-    int* blist = reinterpret_cast<int*>(smem + tileOffB<T>());
-    int* wsum = blist + TILE_NODES;
-    const uint32_t tw = tiles[blockIdx.x];
-    const int i0 = int(tw & 2047u) * TX, j0 = int((tw >> 11) & 2047u) * TY, k0 = int(tw >> 22) * TZ;
     const int tid = threadIdx.x, cx = tid & 31, cy = tid >> 5;
-    const int NX = L.NX, NY = L.NY, NZ = L.NZ;
-    const long long NXY = (long long)NX * NY;
-
-    // stage x (tile + halo) and the voxel words around it: asynchronous copies, all in flight; one
-    // warp per row of 34 nodes (102 contiguous values) / 33 voxel words
-    const int lane = tid & 31, warp = tid >> 5;
-    {
-        const int iLo = i0 - 1;
-        for (int row = warp; row < HZ * HY; row += TILE_THREADS / 32) {
-            const int z = row / HY, y = row - z * HY;
-            const int j = j0 - 1 + y, k = k0 - 1 + z;
-            const bool rowOk = j >= 0 && j < NY && k >= 0 && k < NZ;
-            const T* src = io.x + 3 * ((long long)iLo + (long long)NX * j + NXY * k);
-            T* dst = xs + row * PROW;
-#pragma unroll
-            for (int q = 0; q < (PROW + 31) / 32; q++) {
-                const int c3 = lane + 32 * q;
-                if (c3 >= PROW) break;
-                const int i = iLo + c3 / 3;
-                const bool ok = rowOk && i >= 0 && i < NX;
-                cpAsync<sizeof(T)>(dst + c3, ok ? src + c3 : io.x, ok);
-            }
-        }
-        for (int row = warp; row < VZ * VY; row += TILE_THREADS / 32) {
-            const int z = row / VY, y = row - z * VY;
-            const int j = j0 - 1 + y, k = k0 - 1 + z;
-            const bool rowOk = j >= 0 && j < L.ny && k >= 0 && k < L.nz;
-            const uint32_t* src = L.word + ((long long)(i0 - 1) + (long long)L.nx * (j + (long long)L.ny * k));
-#pragma unroll
-            for (int q = 0; q < (VX + 31) / 32; q++) {
-                const int c = lane + 32 * q;
-                if (c >= VX) break;
-                const int i = i0 - 1 + c;
-                const bool ok = rowOk && i >= 0 && i < L.nx;
-                cpAsync<4>(vs + row * VX + c, ok ? src + c : L.word, ok);
-            }
-        }
-    }
-    // the column's node masks meanwhile
-    const int i = i0 + cx, j = j0 + cy;
-    const bool col = i < NX && j < NY;
-    uint8_t mk[TZ];
-    bool anyUniform = false;
-#pragma unroll
-    for (int z = 0; z < TZ; z++) {
-        const int k = k0 + z;
-        mk[z] = (col && k < NZ) ? __ldg(L.nmask + i + (long long)NX * j + NXY * k) : uint8_t(0);
-        ms[(z * TY + cy) * TX + cx] = mk[z];
-        anyUniform = anyUniform || (mk[z] & NM_UNIFORM);
-    }
-    cpAsyncWaitAll();
-    __syncthreads();
-
+    const long long PXY = (long long)L.PX * L.NY;
     // pass 1: uniform nodes of the thread's column, all four from one sweep of the planes
     unsigned bmask = 0;
 #pragma unroll
@@ -345,7 +294,7 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? 2 : 3) k_tile(L
         for (int z = 0; z < TZ; z++) {
             if (!(mk[z] & NM_UNIFORM)) continue;
             const T s = T(__uint_as_float(vs[vOff(cx, cy, z)]));
-            T* kp = ks + (z * TY + cy) * (3 * TX) + 3 * cx;
+            T* kp = ks + (z * TY + cy) * TROW + 3 * cx;
             kp[0] = s * acc[z][0];
             kp[1] = s * acc[z][1];
             kp[2] = s * acc[z][2];
@@ -368,7 +317,7 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? 2 : 3) k_tile(L
         off += (w < cy) ? c : 0;
         total += c;
     }
-    for (unsigned b = bmask; b; b &= b - 1) blist[off++] = (tid << 4) | (__ffs(b) - 1);
+    for (unsigned b = bmask; b; b &= b - 1) blist[off++] = uint16_t((tid << 4) | (__ffs(b) - 1));
     __syncthreads();
     // pass 2: the listed nodes, all threads
     for (int q = tid; q < total; q += TILE_THREADS) {
@@ -380,51 +329,118 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? 2 : 3) k_tile(L
             own[0] = xn[0]; own[1] = xn[1]; own[2] = xn[2];
         }
         Op::general(L, C, xs, vs, bx, by, bz, acc, own);
-        T* kp = ks + (bz * TY + by) * (3 * TX) + 3 * bx;
+        T* kp = ks + (bz * TY + by) * TROW + 3 * bx;
         kp[0] = acc[0];
         kp[1] = acc[1];
         kp[2] = acc[2];
     }
     __syncthreads();
-    // pass 3: the epilogue, one warp per row of 32 nodes (96 contiguous values), independent loads
-    double dot = 0.0;
-    const int nxHere = min(TX, NX - i0);
+    // pass 3: the epilogue in shared memory, one warp per row of 32 nodes (96 contiguous values);
+    // the results replace K x (y) and d in place
 #pragma unroll
     for (int rr = 0; rr < TY * TZ / (TILE_THREADS / 32); rr++) {
-        const int row = warp + rr * (TILE_THREADS / 32), z = row / TY, y = row - z * TY;
-        if (j0 + y >= NY || k0 + z >= NZ) continue;
-        const long long rowBase = 3 * ((long long)i0 + (long long)NX * (j0 + y) + NXY * (k0 + z));
+        const int row = cy + rr * (TILE_THREADS / 32), z = row / TY, y = row - z * TY;
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-            const int c3 = lane + 32 * q, ex = c3 / 3, comp = c3 - 3 * ex;
-            if (ex >= nxHere) continue;
+            const int c3 = cx + 32 * q, ex = c3 / 3, comp = c3 - 3 * ex, e = row * TROW + c3;
             const uint8_t mask = ms[(z * TY + y) * TX + ex];
-            const long long id = rowBase + c3;
             const bool act = mask & NM_ACTIVE;
             const bool fx = fixedDof(mask, comp);
             const T xv = xs[xOff(ex, y, z) + comp];
-            T kx = act ? ks[row * (3 * TX) + c3] : T(0);
-            if (act && L.dadd) kx += (sizeof(T) == 8 ? T(L.dadd[id]) : T(L.dadd32[id])) * xv;
+            T kx = act ? ks[e] : T(0);
+            if (act && L.dadd) {
+                const long long id = 3 * ((long long)(i0 + ex) + (long long)L.PX * (j0 + y) + PXY * (k0 + z)) + comp;
+                kx += (sizeof(T) == 8 ? T(L.dadd[id]) : T(L.dadd32[id])) * xv;
+            }
             if (MODE == TOP_APPLY) {
-                io.y[id] = (!io.raw && fx) ? T(0) : kx;
+                ks[e] = (!io.raw && fx) ? T(0) : kx;
             } else if (MODE == TOP_RESID) {
-                io.y[id] = fx ? T(0) : T(io.r[id]) - kx;
+                ks[e] = fx ? T(0) : T(rs[e]) - kx;
             } else if (MODE == TOP_DOT) {
                 const T yv = fx ? T(0) : kx;
-                io.y[id] = yv;
+                ks[e] = yv;
                 dot += double(xv) * double(yv);
             } else {
                 if (fx) {
-                    io.d[id] = 0.f;
-                    io.y[id] = T(0);
+                    ds[e] = 0.f;
+                    ks[e] = T(0);
                 } else {
-                    const float dn = io.c1 * io.d[id] + io.c2 * L.invD[id] * (io.r[id] - float(kx));
-                    io.d[id] = dn;
-                    io.y[id] = xv + T(dn);
+                    const float dn = io.c1 * ds[e] + io.c2 * is[e] * (rs[e] - float(kx));
+                    ds[e] = dn;
+                    ks[e] = xv + T(dn);
                 }
             }
         }
     }
+    fenceAsyncShared();
+    __syncthreads();
+    if (tid == 0) {
+        tmaStore3d(&maps.y, ks, 3 * i0, j0, k0);
+        if (tileHasD(MODE)) tmaStore3d(&maps.d, ds, 3 * i0, j0, k0);
+        tmaStoreCommitWait();
+    }
+}
+
+template <class T, int MODE, bool OWN16, bool DIFF>
+__global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(LevelView L, Coefs<T> C, const uint32_t* __restrict__ tiles,
+                                                          const __grid_constant__ TileMaps maps, TileIO<T> io, SolveState* st, double* partials,
+                                                          unsigned* ticket, Ctl ctl) {
+    if (skipped(ctl)) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    if (smemAddr(smem) & 127u) {  // the layout's TMA alignment (never expected to fail)
+        if (threadIdx.x == 0) {
+            atomicExch(&st->err, ST_ERR_ALIGN);
+            st->done = 1;
+        }
+        return;
+    }
+    T* xs = reinterpret_cast<T*>(smem);
+    uint32_t* vs = reinterpret_cast<uint32_t*>(smem + tileOffW<T>());
+    T* ks = reinterpret_cast<T*>(smem + tileOffK<T>());  // K x per tile node, [z][y][3 x + c]; then y
+    float* rs = reinterpret_cast<float*>(smem + tileOffR<T, MODE>());
+    float* ds = reinterpret_cast<float*>(smem + tileOffD<T, MODE>());
+    float* is = reinterpret_cast<float*>(smem + tileOffI<T, MODE>());
+    uint8_t* ms = smem + tileOffM<T, MODE>();
+    uint16_t* blist = reinterpret_cast<uint16_t*>(smem + tileOffB<T, MODE>());
+    int* wsum = reinterpret_cast<int*>(blist + TILE_NODES);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + tileOffBar<T, MODE>());
+    const uint32_t tw = tiles[blockIdx.x];
+    const int i0 = int(tw & 2047u) * TX, j0 = int((tw >> 11) & 2047u) * TY, k0 = int(tw >> 22) * TZ;
+    const int tid = threadIdx.x, cx = tid & 31, cy = tid >> 5;
+    const long long PXY = (long long)L.PX * L.NY;
+
+    // stage: one thread issues every copy on one barrier
+    if (tid == 0) {
+        mbarInit(bar, 1);
+        mbarExpectTx(bar, tileStageBytes<T, MODE>());
+        tmaLoad3d(xs, &maps.x, 3 * (i0 - XLEFT), j0 - 1, k0 - 1, bar);
+        tmaLoad3d(vs, &maps.w, i0 - XLEFT, j0 - 1, k0 - 1, bar);
+        if (tileHasR(MODE)) tmaLoad3d(rs, &maps.r, 3 * i0, j0, k0, bar);
+        if (tileHasD(MODE)) {
+            tmaLoad3d(ds, &maps.d, 3 * i0, j0, k0, bar);
+            tmaLoad3d(is, &maps.inv, 3 * i0, j0, k0, bar);
+        }
+    }
+    // the column's node masks meanwhile (padding nodes i >= NX hold 7: inactive, all held)
+    const int i = i0 + cx, j = j0 + cy;
+    const bool col = i < L.PX && j < L.NY;
+    uint8_t mk[TZ];
+    bool anyUniform = false;
+#pragma unroll
+    for (int z = 0; z < TZ; z++) {
+        const int k = k0 + z;
+        mk[z] = (col && k < L.NZ) ? __ldg(L.nmask + i + (long long)L.PX * j + PXY * k) : uint8_t(0);
+        ms[(z * TY + cy) * TX + cx] = mk[z];
+        anyUniform = anyUniform || (mk[z] & NM_UNIFORM);
+    }
+    __syncthreads();  // the barrier is initialised, the masks are in place
+    const bool staged = __syncthreads_and(mbarWait(bar, TILE_WAIT_POLLS));
+    if (!staged && tid == 0) {
+        atomicExch(&st->err, ST_ERR_STAGING);
+        st->done = 1;
+    }
+    double dot = 0.0;
+    if (staged) tileBody<T, MODE, OWN16, DIFF>(L, C, io, maps, i0, j0, k0, mk, anyUniform, xs, vs, ks, rs, ds, is, ms, blist, wsum, dot);
     if (MODE == TOP_DOT) {
         double v[1] = {dot};
         double tot[1];
@@ -457,10 +473,11 @@ __global__ void k_cheb_first(long long nDof, const float* __restrict__ r, const 
 
 // rc = P^T rf gathered per coarse node: fine 2I (weight 1) and 2I +- 1 (weight 1/2) per axis;
 // held / inactive coarse DOFs 0
-__global__ void k_restrict(int FNX, int FNY, int FNZ, LevelView C, const float* __restrict__ rf, float* __restrict__ rc, float* __restrict__ dc,
+__global__ void k_restrict(LevelView F, LevelView C, const float* __restrict__ rf, float* __restrict__ rc, float* __restrict__ dc,
                            float* __restrict__ zc, float c0, Ctl ctl) {
     if (skipped(ctl)) return;
-    const long long FNXY = (long long)FNX * FNY;
+    const int FNX = F.NX, FNY = F.NY, FNZ = F.NZ;
+    const long long FPX = F.PX, FPXY = (long long)F.PX * F.NY;
     for (long long cn = blockIdx.x * (long long)blockDim.x + threadIdx.x; cn < C.nNodes; cn += (long long)gridDim.x * blockDim.x) {
         const uint8_t mask = C.nmask[cn];
         float s0 = 0, s1 = 0, s2 = 0;
@@ -479,7 +496,7 @@ __global__ void k_restrict(int FNX, int FNY, int FNZ, LevelView C, const float* 
                         const int i = 2 * I + di;
                         if (i < 0 || i >= FNX) continue;
                         const float w = (di ? 0.5f : 1.f) * wj;
-                        const float* p = rf + 3 * (i + j * (long long)FNX + k * FNXY);
+                        const float* p = rf + 3 * (i + j * FPX + k * FPXY);
                         s0 += w * p[0];
                         s1 += w * p[1];
                         s2 += w * p[2];
@@ -502,9 +519,9 @@ __global__ void k_restrict(int FNX, int FNY, int FNZ, LevelView C, const float* 
 }
 
 // zf += P zc at free fine DOFs (trilinear: coarse i/2 and, when odd, (i+1)/2, weight 1/2 each)
-__global__ void k_prolong(LevelView F, int CNX, int CNY, const float* __restrict__ zc, float* __restrict__ zf, Ctl ctl) {
+__global__ void k_prolong(LevelView F, int CPX, int CNY, const float* __restrict__ zc, float* __restrict__ zf, Ctl ctl) {
     if (skipped(ctl)) return;
-    const long long CNXY = (long long)CNX * CNY;
+    const long long CNX = CPX, CNXY = (long long)CPX * CNY;
     for (long long fn = blockIdx.x * (long long)blockDim.x + threadIdx.x; fn < F.nNodes; fn += (long long)gridDim.x * blockDim.x) {
         const uint8_t mask = F.nmask[fn];
         if ((mask & 7) == 7) continue;
@@ -517,7 +534,7 @@ __global__ void k_prolong(LevelView F, int CNX, int CNY, const float* __restrict
         for (int c = 0; c < nk; c++)
             for (int b = 0; b < nj; b++)
                 for (int a = 0; a < ni; a++) {
-                    const float* p = zc + 3 * ((i0 + a) + (j0 + b) * (long long)CNX + (k0 + c) * CNXY);
+                    const float* p = zc + 3 * ((i0 + a) + (j0 + b) * CNX + (k0 + c) * CNXY);
                     s0 += w * p[0];
                     s1 += w * p[1];
                     s2 += w * p[2];
@@ -879,14 +896,16 @@ __global__ void k_vc_store(long long nNodes, const uint8_t* __restrict__ nmask, 
 
 // v_i = LCG value i (seed 12345, s <- (1103515245 s + 12345) mod 2^31, voxel_fea.cpp:584-588),
 // computed for every index at once by jumping the affine recurrence ahead i + 1 steps
-__global__ void k_lz_start(long long nNodes, const uint8_t* __restrict__ nmask, double* __restrict__ v, double* partials, unsigned* ticket,
-                           SolveState* st) {
+__global__ void k_lz_start(LevelView L, double* __restrict__ v, double* partials, unsigned* ticket, SolveState* st) {
     double acc[1] = {0};
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
-        const uint8_t mask = nmask[n];
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < L.nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = L.nmask[n];
+        int i, j, k;
+        nodeCoords(L, n, i, j, k);
+        const long long nd = i + (long long)L.NX * (j + (long long)L.NY * k);  // the reference's (dense) node index
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            const unsigned long long steps = (unsigned long long)(3 * n + c) + 1;
+            const unsigned long long steps = (unsigned long long)(3 * nd + c) + 1;
             // (A, B): s -> A s + B for 2^bit steps; (RA, RB) accumulated
             unsigned long long A = 1103515245ull, B = 12345ull, RA = 1, RB = 0;
             const unsigned long long M = 0x7fffffffull;
@@ -955,6 +974,20 @@ __global__ void k_lz_next(long long n, const double* __restrict__ w, double* __r
     }
 }
 
+// ---- the C ABI's dense layout (node i + NX (j + NY k)) <-> the pitched device layout (i + PX (j + NY k))
+
+template <class T>
+__global__ void k_pitch(const T* __restrict__ src, T* __restrict__ dst, int comps, int NX, int NY, int NZ, int PX, int toPitched) {
+    const long long total = (long long)NX * NY * NZ * comps;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const long long nd = e / comps, row = nd / NX;
+        const int c = int(e - nd * comps), i = int(nd - row * NX);
+        const long long ep = (i + (long long)PX * row) * comps + c;
+        if (toPitched) dst[ep] = src[e];
+        else dst[e] = src[ep];
+    }
+}
+
 // ---- post-processing: nodal stresses (voxel_fea.cpp:968-1037) and reactions (:929-940)
 
 struct StressCoefs {
@@ -987,7 +1020,7 @@ __device__ void principals3(double sx, double sy, double sz, double txy, double 
 
 __global__ void __launch_bounds__(NODE_THREADS) k_stresses(LevelView L, StressCoefs SC, const double* __restrict__ u, int principals,
                                                            float* __restrict__ vm, float* __restrict__ p1, float* __restrict__ p3) {
-    const long long NX = L.NX, NXY = (long long)L.NX * L.NY;
+    const long long NX = L.PX, NXY = (long long)L.PX * L.NY;
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < L.nNodes; n += (long long)gridDim.x * blockDim.x) {
         const uint8_t mask = L.nmask[n];
         float ovm = 0, op1 = 0, op3 = 0;
@@ -1000,7 +1033,7 @@ __global__ void __launch_bounds__(NODE_THREADS) k_stresses(LevelView L, StressCo
                 const int di = v & 1, dj = (v >> 1) & 1, dk = v >> 2;
                 const int ei = i - 1 + di, ej = j - 1 + dj, ek = k - 1 + dk;
                 if (ei < 0 || ej < 0 || ek < 0 || ei >= L.nx || ej >= L.ny || ek >= L.nz) continue;
-                const uint32_t w = L.word[ei + (long long)L.nx * (ej + (long long)L.ny * ek)];
+                const uint32_t w = L.word[L.wi(ei, ej, ek)];
                 if (w == 0) continue;
                 const int a = cornerOf(1 - di, 1 - dj, 1 - dk);
                 double sig[6] = {0, 0, 0, 0, 0, 0};
@@ -1113,6 +1146,24 @@ struct DevMem {
     template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
+// a level's per-node (comps 1) or per-DOF (comps 3) host array in the pitched device layout,
+// padding entries `fill`
+template <class T>
+std::vector<T> pitched(const std::vector<T>& v, int comps, const HostLevel& h, int PX, T fill) {
+    std::vector<T> o(size_t(PX) * h.NY * h.NZ * comps, fill);
+    const size_t rowIn = size_t(h.NX) * comps, rowOut = size_t(PX) * comps;
+    for (int64_t row = 0; row < int64_t(h.NY) * h.NZ; row++)
+        std::copy(v.begin() + row * rowIn, v.begin() + (row + 1) * rowIn, o.begin() + row * rowOut);
+    return o;
+}
+std::vector<uint32_t> pitchedWords(const HostLevel& h, int px) {
+    std::vector<uint32_t> o(size_t(px) * h.ny * h.nz, 0u);
+    for (int64_t row = 0; row < int64_t(h.ny) * h.nz; row++)
+        std::copy(h.word.begin() + row * h.nx, h.word.begin() + (row + 1) * h.nx, o.begin() + row * px);
+    return o;
+}
+inline int pitch4(int n) { return (n + 3) & ~3; }
+
 template <class T>
 void upload(DevMem& m, const std::vector<T>& v, int64_t& total, cudaStream_t s = nullptr) {
     m.alloc(v.size() * sizeof(T), total, s);
@@ -1128,6 +1179,57 @@ int gridFor(int64_t n, int threads, int cap) {
 }
 
 }  // namespace
+
+// ---- tensor maps of the tiled kernels (cuTensorMapEncodeTiled through the runtime's driver entry
+// point, so the library needs no link to the driver library)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encodeTiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        else
+            cudaGetLastError();
+    });
+    if (!fn) throw Error(PS_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    return fn;
+}
+
+enum MapKind { MAP_HALO = 0, MAP_TILE = 1, MAP_WORDS = 2 };
+
+// x halo boxes (PROW x HY x HZ values), tile boxes (TROW x TY x TZ) over a level's pitched DOF
+// vector, or voxel-word boxes (WROW x VY x VZ); outside the tensor loads read 0 and stores are dropped
+CUtensorMap makeMap(const void* base, MapKind kind, bool f64, const dev::LevelView& v) {
+    CUtensorMap m;
+    cuuint64_t dims[3];
+    cuuint32_t box[3];
+    const cuuint32_t es[3] = {1, 1, 1};
+    CUtensorMapDataType dt;
+    size_t esz;
+    if (kind == MAP_WORDS) {
+        dt = CU_TENSOR_MAP_DATA_TYPE_UINT32;
+        esz = 4;
+        dims[0] = cuuint64_t(v.px); dims[1] = cuuint64_t(v.ny); dims[2] = cuuint64_t(v.nz);
+        box[0] = dev::WROW; box[1] = dev::VY; box[2] = dev::VZ;
+    } else {
+        dt = f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        esz = f64 ? 8 : 4;
+        dims[0] = cuuint64_t(3) * v.PX; dims[1] = cuuint64_t(v.NY); dims[2] = cuuint64_t(v.NZ);
+        if (kind == MAP_HALO) { box[0] = dev::PROW; box[1] = dev::HY; box[2] = dev::HZ; }
+        else { box[0] = dev::TROW; box[1] = dev::TY; box[2] = dev::TZ; }
+    }
+    const cuuint64_t strides[2] = {dims[0] * esz, dims[0] * dims[1] * esz};
+    const CUresult r = encodeTiled()(&m, dt, 3, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(PS_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+    return m;
+}
 
 // Read-only device data of one level, shared by every solve context of a handle.
 struct DevLevel {
@@ -1211,22 +1313,32 @@ void SharedModel::adopt(Hierarchy&& h) {
     static std::once_flag attrOnce;
     std::call_once(attrOnce, [] {
         // the tiled operator stages more than the default 48 KB of shared memory
-        const int s32 = int(dev::tileSmemBytes<float>()), s64 = int(dev::tileSmemBytes<double>());
-        check(cudaFuncSetAttribute(dev::k_tile<double, dev::TOP_APPLY, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64), "attr");
-        check(cudaFuncSetAttribute(dev::k_tile<double, dev::TOP_DOT, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64), "attr");
-        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_DOT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
-        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_CHEB, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
-        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_CHEB, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
-        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_RESID, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
-        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_RESID, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
-        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_CHEB, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
-        check(cudaFuncSetAttribute(dev::k_tile<float, dev::TOP_RESID, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32), "attr");
+        auto set = [](auto kernel, size_t bytes) {
+            check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)), "attr");
+        };
+        set(dev::k_tile<double, dev::TOP_APPLY, false, false>, dev::tileSmemBytes<double, dev::TOP_APPLY>());
+        set(dev::k_tile<double, dev::TOP_DOT, false, false>, dev::tileSmemBytes<double, dev::TOP_DOT>());
+        set(dev::k_tile<float, dev::TOP_DOT, false, true>, dev::tileSmemBytes<float, dev::TOP_DOT>());
+        set(dev::k_tile<float, dev::TOP_CHEB, false, false>, dev::tileSmemBytes<float, dev::TOP_CHEB>());
+        set(dev::k_tile<float, dev::TOP_CHEB, true, false>, dev::tileSmemBytes<float, dev::TOP_CHEB>());
+        set(dev::k_tile<float, dev::TOP_CHEB, true, true>, dev::tileSmemBytes<float, dev::TOP_CHEB>());
+        set(dev::k_tile<float, dev::TOP_RESID, false, false>, dev::tileSmemBytes<float, dev::TOP_RESID>());
+        set(dev::k_tile<float, dev::TOP_RESID, true, false>, dev::tileSmemBytes<float, dev::TOP_RESID>());
+        set(dev::k_tile<float, dev::TOP_RESID, true, true>, dev::tileSmemBytes<float, dev::TOP_RESID>());
     });
     L.resize(H.levels.size());
     for (int l = 0; l < int(H.levels.size()); l++) uploadLevel(l);
     m = int(H.coarseM);
     if (H.hasFactor()) {
-        upload(cDof, H.coarseDof, bytes, ms);
+        // the coarsest level's free DOFs as pitched indices
+        const HostLevel& hc = H.levels.back();
+        const int PX = L.back().view.PX;
+        std::vector<int32_t> dofs(H.coarseDof.size());
+        for (size_t q = 0; q < dofs.size(); q++) {
+            const int64_t e = H.coarseDof[q], nd = e / 3, row = nd / hc.NX;
+            dofs[q] = int32_t(3 * ((nd - row * hc.NX) + int64_t(PX) * row) + (e - 3 * nd));
+        }
+        upload(cDof, dofs, bytes, ms);
         upload(cInv, H.coarseInv, bytes, ms);
     }
     for (auto& D : L) maxTiles = std::max(maxTiles, D.nTiles);
@@ -1236,8 +1348,9 @@ void SharedModel::adopt(Hierarchy&& h) {
 void SharedModel::uploadLevel(int l) {
     const HostLevel& h = H.levels[size_t(l)];
     DevLevel& D = L[size_t(l)];
-    upload(D.word, h.word, bytes, ms);
-    upload(D.nmask, h.nmask, bytes, ms);
+    const int PX = pitch4(h.NX), px = pitch4(h.nx);
+    upload(D.word, pitchedWords(h, px), bytes, ms);
+    upload(D.nmask, pitched<uint8_t>(h.nmask, 1, h, PX, uint8_t(7)), bytes, ms);  // padding: inactive, all held
     D.hasOwn = h.nOwn > 0;
     if (D.hasOwn) {
         upload(D.own, h.own, bytes, ms);
@@ -1254,13 +1367,13 @@ void SharedModel::uploadLevel(int l) {
         D.view.hs = hs;
     }
     std::vector<float> invD(h.invDiag.begin(), h.invDiag.end());
-    upload(D.invD, invD, bytes, ms);
+    upload(D.invD, pitched<float>(invD, 3, h, PX, 0.f), bytes, ms);
     if (!h.diagAdd.empty()) {
-        upload(D.dadd, h.diagAdd, bytes, ms);
+        upload(D.dadd, pitched<double>(h.diagAdd, 3, h, PX, 0.0), bytes, ms);
         std::vector<float> d32(h.diagAdd.begin(), h.diagAdd.end());
-        upload(D.dadd32, d32, bytes, ms);
+        upload(D.dadd32, pitched<float>(d32, 3, h, PX, 0.f), bytes, ms);
     }
-    if (l == 0) upload(D.bc, h.bc, bytes, ms);
+    if (l == 0) upload(D.bc, pitched<uint8_t>(h.bc, 3, h, PX, uint8_t(0)), bytes, ms);
     {
         const int ntx = (h.NX + dev::TX - 1) / dev::TX, nty = (h.NY + dev::TY - 1) / dev::TY, ntz = (h.NZ + dev::TZ - 1) / dev::TZ;
         if (ntx > 2047 || nty > 2047 || ntz > 1023) throw Error(PS_EINVAL, "grid too large for the tile index");
@@ -1282,14 +1395,17 @@ void SharedModel::uploadLevel(int l) {
         // lanes per node on the smallest ones
         int64_t minNodes = 400000;
         if (const char* e = std::getenv("PSFEA_TILE_MIN_NODES")) minNodes = std::atoll(e);
-        D.useTiles = h.nNodes >= minNodes;
+        // (and grids no smaller than the staging boxes of 112 x 10 x 6 values and 40 x 9 x 5 words)
+        D.useTiles = h.nNodes >= minNodes && h.NY >= dev::HY && h.NZ >= dev::HZ && 3 * PX >= dev::PROW && px >= dev::WROW;
         int64_t max8 = 30000;
         if (const char* e = std::getenv("PSFEA_OP8_MAX_NODES")) max8 = std::atoll(e);
         D.use8 = !D.useTiles && l > 0 && h.nNodes <= max8;
     }
     dev::LevelView& v = D.view;
     v.nx = h.nx; v.ny = h.ny; v.nz = h.nz; v.NX = h.NX; v.NY = h.NY; v.NZ = h.NZ;
-    v.nNodes = h.nNodes;
+    v.PX = PX;
+    v.px = px;
+    v.nNodes = int64_t(PX) * h.NY * h.NZ;
     v.word = D.word.as<uint32_t>();
     v.nmask = D.nmask.as<uint8_t>();
     v.own = D.own.as<float>();
@@ -1366,6 +1482,36 @@ struct SolverImpl {
     }
 
     int nodeGrid(int64_t nNodes) const { return gridFor(nNodes, dev::NODE_THREADS, smCount * 16); }
+    // node and DOF counts of level l in the pitched device layout (every device vector's length)
+    int64_t pn(int l) const { return L[size_t(l)].view.nNodes; }
+    int64_t pd(int l) const { return 3 * pn(l); }
+    // tensor maps by (base, kind, level); a base address can only be reused for the same level's
+    // vector of the same kind, which has the same map
+    std::map<std::tuple<const void*, int, int>, CUtensorMap> mapCache;
+    const CUtensorMap& mapOf(const void* base, MapKind kind, bool f64, int l) {
+        const auto key = std::make_tuple(base, int(kind) * 2 + (f64 ? 1 : 0), l);
+        auto it = mapCache.find(key);
+        if (it == mapCache.end()) it = mapCache.emplace(key, makeMap(base, kind, f64, L[size_t(l)].view)).first;
+        return it->second;
+    }
+    // dense reference layout <-> pitched device layout of a level-l DOF vector (device to device)
+    void pitch(const double* src, double* dst, int l, bool toPitched) {
+        const dev::LevelView& v = L[size_t(l)].view;
+        launch(dev::k_pitch<double>, vecGrid(int64_t(v.NX) * v.NY * v.NZ * 3), dev::VEC_THREADS, 0, stream, src, dst, 3, v.NX, v.NY, v.NZ, v.PX,
+               toPitched ? 1 : 0);
+    }
+    // host dense vector -> pitched device vector, through `staging` (a device vector of at least the
+    // level's pitched size that holds nothing needed)
+    void uploadPitched(const double* host, double* dst, int l, double* staging) {
+        const size_t n = size_t(H.levels[size_t(l)].nDof);
+        check(cudaMemcpyAsync(staging, host, n * 8, cudaMemcpyHostToDevice, stream), "upload");
+        pitch(staging, dst, l, true);
+    }
+    void downloadPitched(const double* src, double* host, int l, double* staging) {
+        const size_t n = size_t(H.levels[size_t(l)].nDof);
+        pitch(src, staging, l, false);
+        check(cudaMemcpyAsync(host, staging, n * 8, cudaMemcpyDeviceToHost, stream), "download");
+    }
     int vecGrid(int64_t n) const { return gridFor(n, dev::VEC_THREADS, smCount * 8); }
     dev::SolveState* st() const { return state.as<dev::SolveState>(); }
     double* part() const { return partials.as<double>(); }
@@ -1440,13 +1586,13 @@ void SolverImpl::allocate() {
     cudaStream_t s = ownStream;
     W.resize(H.levels.size());
     for (size_t l = 0; l < W.size(); l++) {
-        const size_t n = size_t(H.levels[l].nDof);
+        const size_t n = size_t(pd(int(l)));
         W[l].r.alloc(n * 4, bytes, s);
         W[l].z.alloc(n * 4, bytes, s);
         W[l].t.alloc(n * 4, bytes, s);
         W[l].d.alloc(n * 4, bytes, s);
     }
-    const size_t n = size_t(H.levels[0].nDof);
+    const size_t n = size_t(pd(0));
     f.alloc(n * 8, bytes, s);
     x.alloc(n * 8, bytes, s);
     r.alloc(n * 8, bytes, s);
@@ -1475,9 +1621,14 @@ void SolverImpl::op64(int l, const double* xin, double* y, bool raw, dev::Ctl ct
                    nullptr, 0.f, 0.f, raw ? 1 : 0, ctl);
         return;
     }
-    dev::TileIO<double> io{xin, y, nullptr, nullptr, 0.f, 0.f, raw ? 1 : 0};
-    launch(dev::k_tile<double, dev::TOP_APPLY, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double>(), stream, D.view, D.c64,
-           D.tiles.as<uint32_t>(), io, st(), part(), tick(), ctl);
+    dev::TileIO<double> io{0.f, 0.f, raw ? 1 : 0};
+    dev::TileMaps mp;
+    mp.x = mapOf(xin, MAP_HALO, true, l);
+    mp.w = mapOf(D.word.p, MAP_WORDS, false, l);
+    mp.y = mapOf(y, MAP_TILE, true, l);
+    mp.r = mp.d = mp.inv = mp.y;  // not read by this epilogue
+    launch(dev::k_tile<double, dev::TOP_APPLY, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double, dev::TOP_APPLY>(), stream,
+           D.view, D.c64, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), ctl);
 }
 
 template <int MODE>
@@ -1501,12 +1652,20 @@ void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev
         else launch(dev::k_op<float, MODE, false>, g, dev::NODE_THREADS, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
         return;
     }
-    dev::TileIO<float> io{xin, y, rr, dd, c1, c2, 0};
-    const size_t sm = dev::tileSmemBytes<float>();
+    constexpr int TM = MODE == dev::OP_CHEB ? dev::TOP_CHEB : (MODE == dev::OP_RESID ? dev::TOP_RESID : dev::TOP_APPLY);
+    dev::TileIO<float> io{c1, c2, 0};
+    dev::TileMaps mp;
+    mp.x = mapOf(xin, MAP_HALO, false, l);
+    mp.w = mapOf(D.word.p, MAP_WORDS, false, l);
+    mp.y = mapOf(y, MAP_TILE, false, l);
+    mp.r = dev::tileHasR(TM) ? mapOf(rr, MAP_TILE, false, l) : mp.y;
+    mp.d = dev::tileHasD(TM) ? mapOf(dd, MAP_TILE, false, l) : mp.y;
+    mp.inv = dev::tileHasD(TM) ? mapOf(D.invD.p, MAP_TILE, false, l) : mp.y;
+    const size_t sm = dev::tileSmemBytes<float, TM>();
     const uint32_t* tl = D.tiles.as<uint32_t>();
-    if (diff) launch(dev::k_tile<float, MODE, true, true>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, io, st(), part(), tick(), ctl);
-    else if (o16) launch(dev::k_tile<float, MODE, true, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, io, st(), part(), tick(), ctl);
-    else launch(dev::k_tile<float, MODE, false, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, io, st(), part(), tick(), ctl);
+    if (diff) launch(dev::k_tile<float, TM, true, true>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
+    else if (o16) launch(dev::k_tile<float, TM, true, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
+    else launch(dev::k_tile<float, TM, false, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
 }
 
 // pre-smoothing from zero, residual, restriction, coarse correction, prolongation, post-smoothing
@@ -1526,7 +1685,7 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
         }
         // no factor: 40 damped Jacobi sweeps with the default weight (voxel_fea.cpp:676-678)
         if (!firstDone)
-            launch(dev::k_cheb_first, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, r, D.invD.as<float>(), d, z, D.omega, ctl);
+            launch(dev::k_cheb_first, vecGrid(pd(l)), dev::VEC_THREADS, 0, stream, pd(l), r, D.invD.as<float>(), d, z, D.omega, ctl);
         float* a = z;
         float* b = t;
         for (int s = 1; s < 40; s++) {
@@ -1539,7 +1698,7 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
     LevelWork& Wc = W[size_t(l + 1)];
     const HostLevel& hc = H.levels[size_t(l + 1)];
     if (!firstDone)
-        launch(dev::k_cheb_first, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, r, D.invD.as<float>(), d, z, D.cf0, ctl);
+        launch(dev::k_cheb_first, vecGrid(pd(l)), dev::VEC_THREADS, 0, stream, pd(l), r, D.invD.as<float>(), d, z, D.cf0, ctl);
     float* a = z;  // the current iterate
     float* b = t;
     for (size_t k = 0; k < D.chebC1.size(); k++) {  // pre-smoothing from zero
@@ -1550,10 +1709,10 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
     // restriction, with the coarse level's first smoothing step fused in (unless it is the dense solve)
     const bool fuse = !(l + 1 == last && H.hasFactor());
     const float c0c = (l + 1 == last) ? C.omega : C.cf0;
-    launch(dev::k_restrict, gridFor(hc.nNodes, 256, smCount * 16), 256, 0, stream, h.NX, h.NY, h.NZ, C.view, b, Wc.r.as<float>(),
+    launch(dev::k_restrict, gridFor(pn(l + 1), 256, smCount * 16), 256, 0, stream, D.view, C.view, b, Wc.r.as<float>(),
            fuse ? Wc.d.as<float>() : nullptr, fuse ? Wc.z.as<float>() : nullptr, c0c, ctl);
     float* zc = vcycle(l + 1, ctl, own16, fuse);
-    launch(dev::k_prolong, gridFor(h.nNodes, 256, smCount * 16), 256, 0, stream, D.view, hc.NX, hc.NY, zc, a, ctl);
+    launch(dev::k_prolong, gridFor(pn(l), 256, smCount * 16), 256, 0, stream, D.view, C.view.PX, hc.NY, zc, a, ctl);
     op32<dev::OP_CHEB>(l, a, b, 0.f, D.cf0, ctl, own16);  // post-smoothing: d = c0 D^-1 (r - K a); b = a + d
     std::swap(a, b);
     for (size_t k = 0; k < D.chebC1.size(); k++) {
@@ -1570,7 +1729,7 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
 void SolverImpl::enqueueLanczos(int l) {
     DevLevel& D = L[size_t(l)];
     const HostLevel& h = H.levels[size_t(l)];
-    const int64_t n = h.nDof;
+    const int64_t n = pd(l);
     int64_t scratch = 0;
     DevMem v, vp, w, xx, invD, ab;
     v.alloc(size_t(n) * 8, scratch, stream);
@@ -1578,9 +1737,9 @@ void SolverImpl::enqueueLanczos(int l) {
     w.alloc(size_t(n) * 8, scratch, stream);
     xx.alloc(size_t(n) * 8, scratch, stream);
     ab.alloc(20 * sizeof(double), scratch, stream);
-    upload(invD, h.invDiag, scratch, stream);
+    upload(invD, pitched<double>(h.invDiag, 3, h, D.view.PX, 0.0), scratch, stream);
     const int vg = vecGrid(n);
-    launch(dev::k_lz_start, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, h.nNodes, D.view.nmask, v.as<double>(), part(), tick(), st());
+    launch(dev::k_lz_start, nodeGrid(pn(l)), dev::NODE_THREADS, 0, stream, D.view, v.as<double>(), part(), tick(), st());
     launch(dev::k_scale, vg, dev::VEC_THREADS, 0, stream, n, v.as<double>(), st());
     const dev::Ctl none{nullptr, nullptr};
     double* abp = ab.as<double>();
@@ -1669,15 +1828,20 @@ void SolverImpl::recordPlainIteration(dev::Ctl ctl) {
     DevLevel& D = L[0];
     LevelWork& W0 = W[0];
     if (!D.useTiles) {
-        launch(dev::k_apply_alpha<double, false>, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c64, p.as<double>(), q.as<double>(),
+        launch(dev::k_apply_alpha<double, false>, nodeGrid(pn(0)), dev::NODE_THREADS, 0, stream, D.view, D.c64, p.as<double>(), q.as<double>(),
                st(), part(), tick(), ctl);
     } else {
-        dev::TileIO<double> io{p.as<double>(), q.as<double>(), nullptr, nullptr, 0.f, 0.f, 0};
-        launch(dev::k_tile<double, dev::TOP_DOT, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double>(), stream, D.view, D.c64,
-               D.tiles.as<uint32_t>(), io, st(), part(), tick(), ctl);
+        dev::TileIO<double> io{0.f, 0.f, 0};
+        dev::TileMaps mp;
+        mp.x = mapOf(p.p, MAP_HALO, true, 0);
+        mp.w = mapOf(D.word.p, MAP_WORDS, false, 0);
+        mp.y = mapOf(q.p, MAP_TILE, true, 0);
+        mp.r = mp.d = mp.inv = mp.y;
+        launch(dev::k_tile<double, dev::TOP_DOT, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double, dev::TOP_DOT>(), stream,
+               D.view, D.c64, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), ctl);
     }
     const bool one = exactOneLevel();
-    launch(dev::k_cg_update, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x.as<double>(), r.as<double>(), p.as<double>(),
+    launch(dev::k_cg_update, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, x.as<double>(), r.as<double>(), p.as<double>(),
            q.as<double>(), one ? nullptr : W0.r.as<float>(), D.invD.as<float>(), W0.d.as<float>(), W0.z.as<float>(), D.cf0, st(), part(), tick(),
            ctl);
     float* z32 = nullptr;
@@ -1689,9 +1853,9 @@ void SolverImpl::recordPlainIteration(dev::Ctl ctl) {
     } else {
         z32 = vcycle(0, ctl, false, true);  // r32 and the first smoothing step came with the update
     }
-    launch(dev::k_cg_dots, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), z32, z64.as<double>(),
+    launch(dev::k_cg_dots, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, r.as<double>(), z32, z64.as<double>(),
            q.as<double>(), st(), part(), tick(), ctl);
-    launch(dev::k_cg_p, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, z32, z64.as<double>(), p.as<double>(), st(), ctl);
+    launch(dev::k_cg_p, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, z32, z64.as<double>(), p.as<double>(), st(), ctl);
 }
 
 // one FP32 CG iteration with the FP64 fold (runs only when due)
@@ -1701,23 +1865,28 @@ void SolverImpl::recordMixedIteration(dev::Ctl ctl) {
     LevelWork& W0 = W[0];
     const int* foldFlag = &st()->fold;
     if (!D.useTiles) {
-        launch(dev::k_apply_alpha<float, true>, nodeGrid(h.nNodes), dev::NODE_THREADS, 0, stream, D.view, D.c32, p32.as<float>(), q32.as<float>(),
+        launch(dev::k_apply_alpha<float, true>, nodeGrid(pn(0)), dev::NODE_THREADS, 0, stream, D.view, D.c32, p32.as<float>(), q32.as<float>(),
                st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
     } else {
-        dev::TileIO<float> io{p32.as<float>(), q32.as<float>(), nullptr, nullptr, 0.f, 0.f, 0};
-        launch(dev::k_tile<float, dev::TOP_DOT, false, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float>(), stream, D.view, D.c32,
-               D.tiles.as<uint32_t>(), io, st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
+        dev::TileIO<float> io{0.f, 0.f, 0};
+        dev::TileMaps mp;
+        mp.x = mapOf(p32.p, MAP_HALO, false, 0);
+        mp.w = mapOf(D.word.p, MAP_WORDS, false, 0);
+        mp.y = mapOf(q32.p, MAP_TILE, false, 0);
+        mp.r = mp.d = mp.inv = mp.y;
+        launch(dev::k_tile<float, dev::TOP_DOT, false, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float, dev::TOP_DOT>(), stream, D.view,
+               D.c32, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
     }
-    launch(dev::k_mx_update, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x32.as<float>(), W0.r.as<float>(),
+    launch(dev::k_mx_update, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, x32.as<float>(), W0.r.as<float>(),
            p32.as<float>(), q32.as<float>(), st(), part(), tick(), ctl);
     const dev::Ctl foldCtl{ctl.skipIf, foldFlag};
-    launch(dev::k_mx_fold1, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, x.as<double>(), x32.as<float>(), st(), foldCtl);
+    launch(dev::k_mx_fold1, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), x.as<double>(), x32.as<float>(), st(), foldCtl);
     op64(0, x.as<double>(), q.as<double>(), false, foldCtl);
-    launch(dev::k_mx_fold2, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(),
+    launch(dev::k_mx_fold2, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, f.as<double>(), q.as<double>(),
            W0.r.as<float>(), st(), part(), tick(), foldCtl);
     float* z32 = vcycle(0, ctl, M->mixedOwn16);
-    launch(dev::k_mx_dots, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, W0.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
-    launch(dev::k_mx_p, vecGrid(h.nDof), dev::VEC_THREADS, 0, stream, h.nDof, z32, p32.as<float>(), st(), ctl);
+    launch(dev::k_mx_dots, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), W0.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
+    launch(dev::k_mx_p, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), z32, p32.as<float>(), st(), ctl);
 }
 
 void SolverImpl::startSolve(const double* fDev, const double* x0Dev, const ps_solve_opts& o, double* uDev, double* uHost) {
@@ -1751,7 +1920,7 @@ void SolverImpl::startIterations() {
     LevelWork& W0 = W[0];
     const bool mixed = o.precision == PS_PREC_MIXED && !exactOneLevel();
     pend.mixed = mixed;
-    const int64_t n = h.nDof;
+    const int64_t n = pd(0);
     // state
     dev::SolveState s{};
     s.tol = o.tol;
@@ -1761,17 +1930,17 @@ void SolverImpl::startIterations() {
     s.foldFactor = M->foldFactor;
     *hostState = s;
     check(cudaMemcpyAsync(state.p, hostState, sizeof s, cudaMemcpyHostToDevice, stream), "state");
-    if (fDev != f.p) check(cudaMemcpyAsync(f.p, fDev, size_t(n) * 8, cudaMemcpyDeviceToDevice, stream), "f copy");
-    launch(dev::k_mask_copy, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, x0Dev, x.as<double>());
+    if (fDev != f.p) pitch(fDev, f.as<double>(), 0, true);  // a caller's device vector (dense layout)
+    launch(dev::k_mask_copy, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, x0Dev, x.as<double>());
     const dev::Ctl none{nullptr, nullptr};
     const dev::Ctl ctl{&st()->done, nullptr};
     op64(0, x.as<double>(), q.as<double>(), false, none);
-    launch(dev::k_cg_init, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), r.as<double>(),
+    launch(dev::k_cg_init, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, f.as<double>(), q.as<double>(), r.as<double>(),
            nullptr, st(), part(), tick());
     // first preconditioned direction
     if (mixed) {
         check(cudaMemsetAsync(x32.p, 0, size_t(n) * 4, stream), "memset");
-        launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), W0.r.as<float>(),
+        launch(dev::k_vc_load, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, r.as<double>(), W0.r.as<float>(),
                D.invD.as<float>(), W0.d.as<float>(), W0.z.as<float>(), D.cf0, st(), ctl);
         float* z32 = vcycle(0, ctl, M->mixedOwn16, true);
         launch(dev::k_mx_dots, vecGrid(n), dev::VEC_THREADS, 0, stream, n, W0.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
@@ -1785,13 +1954,13 @@ void SolverImpl::startIterations() {
             launch(dev::k_coarse<double, double>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(),
                    r.as<double>(), z64.as<double>(), ctl);
         } else {
-            launch(dev::k_vc_load, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), W0.r.as<float>(),
+            launch(dev::k_vc_load, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, r.as<double>(), W0.r.as<float>(),
                    D.invD.as<float>(), W0.d.as<float>(), W0.z.as<float>(), D.cf0, st(), ctl);
             z32 = vcycle(0, ctl, false, true);
         }
-        launch(dev::k_cg_dots, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, r.as<double>(), z32, z64.as<double>(),
+        launch(dev::k_cg_dots, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, r.as<double>(), z32, z64.as<double>(),
                q.as<double>(), st(), part(), tick(), ctl);
-        launch(dev::k_cg_p, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, z32, z64.as<double>(), p.as<double>(), st(),
+        launch(dev::k_cg_p, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, z32, z64.as<double>(), p.as<double>(), st(),
                ctl);
     }
     launch(dev::k_clear_first, 1, 1, 0, stream, st());
@@ -1836,7 +2005,7 @@ bool SolverImpl::advance(bool block, ps_solve_result& res) {
     }
     const HostLevel& h = H.levels[0];
     DevLevel& D = L[0];
-    const int64_t n = h.nDof;
+    const int64_t n = pd(0);
     const ps_solve_opts& o = pend.o;
     const bool mixed = pend.mixed;
     const dev::Ctl none{nullptr, nullptr};
@@ -1874,23 +2043,29 @@ bool SolverImpl::advance(bool block, ps_solve_result& res) {
         if (hs.done == 2) check(cudaMemsetAsync(x.p, 0, size_t(n) * 8, stream), "memset");
         if (!mixed) {
             op64(0, x.as<double>(), q.as<double>(), false, none);
-            launch(dev::k_final, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), st(), part(),
+            launch(dev::k_final, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, f.as<double>(), q.as<double>(), st(), part(),
                    tick());
         } else if (pend.outcome == PS_CANCELLED || pend.outcome == PS_TIMEOUT) {
             // fold what the FP32 iterate holds and report the true residual
             launch(dev::k_mx_fold1, vecGrid(n), dev::VEC_THREADS, 0, stream, n, x.as<double>(), x32.as<float>(), st(), none);
             op64(0, x.as<double>(), q.as<double>(), false, none);
-            launch(dev::k_final, vecGrid(h.nNodes), dev::VEC_THREADS, 0, stream, h.nNodes, D.view.nmask, f.as<double>(), q.as<double>(), st(), part(),
+            launch(dev::k_final, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, f.as<double>(), q.as<double>(), st(), part(),
                    tick());
         }
-        if (pend.uDev && pend.uDev != x.p) check(cudaMemcpyAsync(pend.uDev, x.p, size_t(n) * 8, cudaMemcpyDeviceToDevice, stream), "u copy");
-        if (pend.uHost) check(cudaMemcpyAsync(pend.uHost, x.p, size_t(n) * 8, cudaMemcpyDeviceToHost, stream), "u download");
+        // u to the caller in the dense layout (q is free here: the staging vector of the download)
+        if (pend.uDev) pitch(x.as<double>(), pend.uDev, 0, false);
+        if (pend.uHost) downloadPitched(x.as<double>(), pend.uHost, 0, q.as<double>());
         enqueueStateRead();
         pend.finishing = true;
         return false;
     }
     check(cudaGetLastError(), "solve");
     const dev::SolveState& hs = *hostState;
+    if (hs.err) {
+        pend.active = false;
+        throw Error(PS_ECUDA, hs.err == dev::ST_ERR_STAGING ? "a tiled operator kernel gave up waiting for its staged data"
+                                                            : "a tiled operator kernel found its shared memory misaligned");
+    }
     ps_status outcome = pend.outcome;
     res.iterations = hs.it;
     res.residual = hs.rel;
@@ -1948,12 +2123,15 @@ int64_t estimateDeviceBytes(const Hierarchy& H) {
     int64_t b = 0, allocs = 0;
     for (size_t l = 0; l < H.levels.size(); l++) {
         const HostLevel& h = H.levels[l];
-        b += 4 * h.nVox + h.nNodes + 6 * 576 * h.nOwn + 4 * h.nDof + (h.diagAdd.empty() ? 0 : 12 * h.nDof) + 4 * (h.nNodes / 1024 + 1);
-        if (l == 0) b += h.nDof;
-        b += 16 * h.nDof;  // V-cycle vectors r, z, t, d
+        // pitched sizes: rows of PX = NX rounded up to 4 nodes, px = nx rounded up to 4 words
+        const int64_t nodes = int64_t(pitch4(h.NX)) * h.NY * h.NZ, dofs = 3 * nodes;
+        b += 4 * int64_t(pitch4(h.nx)) * h.ny * h.nz + nodes + 6 * 576 * h.nOwn + 4 * dofs + (h.diagAdd.empty() ? 0 : 12 * dofs) +
+             4 * (h.nNodes / 1024 + 1);
+        if (l == 0) b += dofs;
+        b += 16 * dofs;  // V-cycle vectors r, z, t, d
         allocs += 12;
     }
-    const int64_t n = H.levels[0].nDof;
+    const int64_t n = 3 * int64_t(pitch4(H.levels[0].NX)) * H.levels[0].NY * H.levels[0].NZ;
     b += 40 * n + 12 * n + (H.levels.size() == 1 ? 8 * n : 0);
     b += 4 * H.coarseM + 8 * H.coarseM * H.coarseM;
     b += 4096 * 32 + 64 * 1024;
@@ -1993,10 +2171,10 @@ ps_status Solver::solve(const double* f, const ps_solve_opts& o, double* u, ps_s
     const int64_t n = nDof();
     validateF(f, o.x0, n);
     const auto t0 = std::chrono::steady_clock::now();
-    check(cudaMemcpyAsync(I.f.p, f, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "f upload");
+    I.uploadPitched(f, I.f.as<double>(), 0, I.q.as<double>());
     const double* x0 = nullptr;
     if (o.x0) {
-        check(cudaMemcpyAsync(I.p.p, o.x0, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "x0 upload");
+        I.uploadPitched(o.x0, I.p.as<double>(), 0, I.q.as<double>());
         x0 = I.p.as<double>();
     }
     I.startSolve(I.f.as<double>(), x0, o, nullptr, u);
@@ -2010,7 +2188,7 @@ ps_status Solver::solveDevice(const double* fDev, const ps_solve_opts& o, double
     SolverImpl& I = *impl_;
     const double* x0 = o.x0;
     if (x0) {
-        check(cudaMemcpyAsync(I.p.p, x0, size_t(nDof()) * 8, cudaMemcpyDeviceToDevice, I.stream), "x0 copy");
+        I.pitch(x0, I.p.as<double>(), 0, true);
         x0 = I.p.as<double>();
     }
     return I.runSolve(fDev, x0, o, uDev, res);
@@ -2018,11 +2196,10 @@ ps_status Solver::solveDevice(const double* fDev, const ps_solve_opts& o, double
 
 void Solver::begin(const double* fHost, const ps_solve_opts& o, double* uHost) {
     SolverImpl& I = *impl_;
-    const int64_t n = nDof();
-    check(cudaMemcpyAsync(I.f.p, fHost, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "f upload");
+    I.uploadPitched(fHost, I.f.as<double>(), 0, I.q.as<double>());
     const double* x0 = nullptr;
     if (o.x0) {
-        check(cudaMemcpyAsync(I.p.p, o.x0, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "x0 upload");
+        I.uploadPitched(o.x0, I.p.as<double>(), 0, I.q.as<double>());
         x0 = I.p.as<double>();
     }
     I.startSolve(I.f.as<double>(), x0, o, nullptr, uHost);
@@ -2054,10 +2231,10 @@ ps_status Solver::solveBatch(int32_t nrhs, const double* f, const ps_solve_opts&
     auto startOn = [&](int k, int q) {
         SolverImpl& I = *ctx[size_t(k)];
         ps_solve_opts o = base;
-        check(cudaMemcpyAsync(I.f.p, f + int64_t(q) * n, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "f upload");
+        I.uploadPitched(f + int64_t(q) * n, I.f.as<double>(), 0, I.q.as<double>());
         const double* x0 = nullptr;
         if (base.x0) {
-            check(cudaMemcpyAsync(I.p.p, base.x0 + int64_t(q) * n, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "x0 upload");
+            I.uploadPitched(base.x0 + int64_t(q) * n, I.p.as<double>(), 0, I.q.as<double>());
             x0 = I.p.as<double>();
         }
         o.x0 = nullptr;
@@ -2092,10 +2269,10 @@ void Solver::precondition(const double* rHost, double* zHost) {
     const HostLevel& h = I.H.levels[0];
     DevLevel& D = I.L[0];
     LevelWork& W0 = I.W[0];
-    const int64_t n = h.nDof;
+    const int64_t n = I.pd(0), nn = I.pn(0);
     I.setDegree(2);  // the reference's preconditioner
     I.prepareSmoothers();
-    check(cudaMemcpyAsync(I.r.p, rHost, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "r upload");
+    I.uploadPitched(rHost, I.r.as<double>(), 0, I.q.as<double>());
     const dev::Ctl none{nullptr, nullptr};
     if (I.exactOneLevel()) {
         // the whole model is the coarsest level: its direct FP64 solve (voxel_fea.cpp:838-842)
@@ -2104,14 +2281,14 @@ void Solver::precondition(const double* rHost, double* zHost) {
         check(cudaMemsetAsync(I.z64.p, 0, size_t(n) * 8, I.stream), "memset");
         I.launch(dev::k_coarse<double, double>, grid, threads, size_t(I.m) * sizeof(double), I.stream, I.m, I.cDof.as<int>(), I.cInv.as<double>(),
                  I.r.as<double>(), I.z64.as<double>(), none);
-        check(cudaMemcpyAsync(zHost, I.z64.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "z download");
+        I.downloadPitched(I.z64.as<double>(), zHost, 0, I.q.as<double>());
     } else {
-        I.launch(dev::k_rmax, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, I.r.as<double>(), I.st(), I.part(), I.tick());
-        I.launch(dev::k_vc_load, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, I.r.as<double>(), W0.r.as<float>(),
+        I.launch(dev::k_rmax, I.vecGrid(nn), dev::VEC_THREADS, 0, I.stream, nn, D.view.nmask, I.r.as<double>(), I.st(), I.part(), I.tick());
+        I.launch(dev::k_vc_load, I.vecGrid(nn), dev::VEC_THREADS, 0, I.stream, nn, D.view.nmask, I.r.as<double>(), W0.r.as<float>(),
                  D.invD.as<float>(), W0.d.as<float>(), W0.z.as<float>(), D.cf0, I.st(), none);
         float* z32 = I.vcycle(0, none, false, true);
-        I.launch(dev::k_vc_store, I.vecGrid(h.nNodes), dev::VEC_THREADS, 0, I.stream, h.nNodes, D.view.nmask, z32, I.q.as<double>(), I.st());
-        check(cudaMemcpyAsync(zHost, I.q.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "z download");
+        I.launch(dev::k_vc_store, I.vecGrid(nn), dev::VEC_THREADS, 0, I.stream, nn, D.view.nmask, z32, I.q.as<double>(), I.st());
+        I.downloadPitched(I.q.as<double>(), zHost, 0, I.p.as<double>());
     }
     check(cudaStreamSynchronize(I.stream), "precondition");
 }
@@ -2160,32 +2337,37 @@ int64_t Solver::launches() const {
 void Solver::apply(int level, const double* xHost, double* yHost, bool raw) {
     SolverImpl& I = *impl_;
     if (level < 0 || level >= int(I.L.size())) throw Error(PS_EINVAL, "level out of range");
-    const int64_t n = I.H.levels[size_t(level)].nDof;
-    check(cudaMemcpyAsync(I.p.p, xHost, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "x upload");
+    const int64_t n = I.pd(level);
+    // p and q as level `level` vectors: cleared first, so their padding entries hold 0
+    check(cudaMemsetAsync(I.p.p, 0, size_t(n) * 8, I.stream), "memset");
+    I.uploadPitched(xHost, I.p.as<double>(), level, I.q.as<double>());
     check(cudaMemsetAsync(I.q.p, 0, size_t(n) * 8, I.stream), "memset");  // inactive tiles are not written
     I.op64(level, I.p.as<double>(), I.q.as<double>(), raw, dev::Ctl{nullptr, nullptr});
-    check(cudaMemcpyAsync(yHost, I.q.p, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream), "y download");
+    I.downloadPitched(I.q.as<double>(), yHost, level, I.p.as<double>());
     check(cudaStreamSynchronize(I.stream), "apply");
 }
 
 void Solver::stresses(const double* u, double E, double h, bool principals, float* vm, float* p1, float* p3) {
     SolverImpl& I = *impl_;
     const HostLevel& L0 = I.H.levels[0];
-    const int64_t nn = L0.nNodes;
+    const int64_t nn = I.pn(0);
+    const dev::LevelView& v = I.L[0].view;
     dev::StressCoefs sc;
     for (int a = 0; a < 8; a++)
         for (int i = 0; i < 144; i++) sc.S[a][i] = I.H.el.cornerStress[a][i] * E / h;
     int64_t scratch = 0;
     DevMem out;
-    out.alloc(size_t(nn) * 4 * 3, scratch);
-    check(cudaMemcpyAsync(I.p.p, u, size_t(L0.nDof) * 8, cudaMemcpyHostToDevice, I.stream), "u upload");
+    out.alloc(size_t(nn) * 4 * 6, scratch);  // three pitched fields and three dense ones
+    I.uploadPitched(u, I.p.as<double>(), 0, I.q.as<double>());
     float* o = out.as<float>();
-    I.launch(dev::k_stresses, I.nodeGrid(nn), dev::NODE_THREADS, 0, I.stream, I.L[0].view, sc, I.p.as<double>(), principals ? 1 : 0, o, o + nn,
+    I.launch(dev::k_stresses, I.nodeGrid(nn), dev::NODE_THREADS, 0, I.stream, v, sc, I.p.as<double>(), principals ? 1 : 0, o, o + nn,
              o + 2 * nn);
-    check(cudaMemcpyAsync(vm, o, size_t(nn) * 4, cudaMemcpyDeviceToHost, I.stream), "vm");
-    if (principals) {
-        check(cudaMemcpyAsync(p1, o + nn, size_t(nn) * 4, cudaMemcpyDeviceToHost, I.stream), "p1");
-        check(cudaMemcpyAsync(p3, o + 2 * nn, size_t(nn) * 4, cudaMemcpyDeviceToHost, I.stream), "p3");
+    const int64_t nd = L0.nNodes;
+    float* outs[3] = {vm, p1, p3};
+    for (int f = 0; f < (principals ? 3 : 1); f++) {
+        float* dense = o + 3 * nn + f * nn;
+        I.launch(dev::k_pitch<float>, I.vecGrid(nd), dev::VEC_THREADS, 0, I.stream, o + f * nn, dense, 1, v.NX, v.NY, v.NZ, v.PX, 0);
+        check(cudaMemcpyAsync(outs[f], dense, size_t(nd) * 4, cudaMemcpyDeviceToHost, I.stream), "stress download");
     }
     check(cudaStreamSynchronize(I.stream), "stresses");
 }
@@ -2193,12 +2375,17 @@ void Solver::stresses(const double* u, double E, double h, bool principals, floa
 void Solver::reactions(const double* u, const double* f, double R[3]) {
     SolverImpl& I = *impl_;
     const HostLevel& L0 = I.H.levels[0];
-    const int64_t n = L0.nDof;
-    check(cudaMemcpyAsync(I.p.p, u, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "u upload");
-    if (f) check(cudaMemcpyAsync(I.r.p, f, size_t(n) * 8, cudaMemcpyHostToDevice, I.stream), "f upload");
+    const int64_t n = I.pd(0);
+    (void)L0;
+    check(cudaMemsetAsync(I.p.p, 0, size_t(n) * 8, I.stream), "memset");
+    I.uploadPitched(u, I.p.as<double>(), 0, I.q.as<double>());
+    if (f) {
+        check(cudaMemsetAsync(I.r.p, 0, size_t(n) * 8, I.stream), "memset");
+        I.uploadPitched(f, I.r.as<double>(), 0, I.q.as<double>());
+    }
     check(cudaMemsetAsync(I.q.p, 0, size_t(n) * 8, I.stream), "memset");
     I.op64(0, I.p.as<double>(), I.q.as<double>(), true, dev::Ctl{nullptr, nullptr});
-    I.launch(dev::k_reactions, I.vecGrid(L0.nNodes), dev::VEC_THREADS, 0, I.stream, L0.nNodes, I.L[0].view.nmask, I.L[0].bc.as<uint8_t>(),
+    I.launch(dev::k_reactions, I.vecGrid(I.pn(0)), dev::VEC_THREADS, 0, I.stream, I.pn(0), I.L[0].view.nmask, I.L[0].bc.as<uint8_t>(),
              I.q.as<double>(), f ? I.r.as<double>() : nullptr, I.st(), I.part(), I.tick());
     I.readState();
     R[0] = I.hostState->alpha;
@@ -2227,18 +2414,22 @@ namespace dev {
 __global__ void __launch_bounds__(NODE_THREADS) k_apply_dot_static(LevelView L, Coefs<double> C, const double* __restrict__ p,
                                                                    double* __restrict__ q, double* __restrict__ dot,
                                                                    unsigned char* scratch) {
+    // p and q are the caller's vectors in the reference's dense layout (node nd = i + NX (j + NY k));
+    // masks, words and the diagonal shift are the level's pitched arrays
     double v[1] = {0.0};
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < L.nNodes; n += (long long)gridDim.x * blockDim.x) {
+    const long long nDense = (long long)L.NX * L.NY * L.NZ;
+    for (long long nd = blockIdx.x * (long long)blockDim.x + threadIdx.x; nd < nDense; nd += (long long)gridDim.x * blockDim.x) {
+        const long long row = nd / L.NX;
+        const int i = int(nd - row * L.NX), j = int(row % L.NY), k = int(row / L.NY);
+        const long long n = i + (long long)L.PX * row;
         const uint8_t mask = __ldg(L.nmask + n);
-        int i, j, k;
-        nodeCoords(L, n, i, j, k);
         double acc[3];
-        applyAt<double, false>(L, C, p, i, j, k, n, mask, acc);
+        applyAt<double, false>(L, C, p, i, j, k, nd, mask, acc, L.NX, n);
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const double y = fixedDof(mask, c) ? 0.0 : acc[c];
-            q[3 * n + c] = y;
-            v[0] += p[3 * n + c] * y;
+            q[3 * nd + c] = y;
+            v[0] += p[3 * nd + c] * y;
         }
     }
     unsigned* ticket = reinterpret_cast<unsigned*>(scratch);
