@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--impl", default="psfea", choices=["psfea", "reference"])
     ap.add_argument("--cpu-sample-s", type=float, default=15.0, help="CPU baseline budget (seconds of CPU work)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-only", choices=["cheb32", "apply64"], default=None,
+                    help="build the model and launch only this level-0 operator kernel --reps times (a small, fixed "
+                         "launch sequence for profilers); prints its mean CUDA-event time")
+    ap.add_argument("--reps", type=int, default=5)
     return ap.parse_args()
 
 
@@ -187,10 +191,24 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def kernel_only(args):
+    import torch
+    import psfea
+    from psfea import workloads as W
+    m = W.l_bracket()
+    S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    ms = S.time_kernel(0 if args.kernel_only == "cheb32" else 1, args.reps)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel": args.kernel_only, "reps": args.reps, "ms": ms}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.kernel_only:
+        kernel_only(args)
         return
     rank, world, local, pg = dist_setup(args.gpus)
     import torch
@@ -286,7 +304,7 @@ def main():
         "mixed_over_plain": value / plain,
         "e2e": {"value": e2e_value, "unit": "MDOF/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                     "kernel": "k_op<float,OP_CHEB> level 0 (FP32 Chebyshev step)", "ms": ms_cheb,
+                     "kernel": "k_tile<float,TOP_CHEB> level 0 (FP32 Chebyshev step)", "ms": ms_cheb,
                      "algorithmic_bytes": alg_bytes, "peak_kind": peak_kind, "fp64_apply_ms": ms_apply64},
         "cpu_baseline": cb,
         "gpu_launches": int(kmx),

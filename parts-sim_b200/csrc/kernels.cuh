@@ -238,14 +238,16 @@ namespace dev {
 // ---------------------------------------------------------------- tiled operator
 //
 // One CTA per 32 x 8 x 4 node tile (only tiles with an active node are launched). One thread stages
-// everything the tile needs with tensor-memory-access (TMA) copies, all in flight together on one
-// shared-memory barrier: the x values with a one-node halo, the voxel words around the tile and,
-// for the smoother and residual epilogues, the tile's r, d and 1/diag. The CTA then computes its
-// 1024 nodes from shared memory: uniform nodes with the 153-FMA assembled stencil, the other active
-// nodes (compacted in a fixed order) with the per-voxel gather, so the two code paths never share
-// a warp; the epilogue runs in shared memory and one thread writes the results back with TMA
-// stores. Inactive nodes of the tile are written 0; inactive tiles are never touched (their
-// outputs are 0 already).
+// what the tile needs with tensor-memory-access (TMA) copies on two shared-memory barriers: the x
+// values with a one-node halo and the voxel words around the tile first, the tile's r and d (the
+// smoother and residual epilogues) second. Each thread then computes its column of four nodes with
+// the 153-FMA assembled stencil from shared memory (uniform nodes) and runs their epilogues in
+// shared memory. Boundary nodes (active, not uniform): 32-bit tiles compact them in a fixed order
+// and give one thread each the per-voxel gather, packed into as few warps as possible; 64-bit tiles
+// leave them to the boundary-node kernel that follows, which overwrites their output slots (the
+// FP64 gather is heavy enough to want a launch of its own at full occupancy). One thread writes
+// the tile back with TMA stores. Inactive nodes are written 0; inactive tiles are never touched
+// (their outputs are 0 already).
 //
 // TMA boxes start on 16-byte boundaries: node rows are pitched (PX, a multiple of 4) and the halo
 // box starts 4 nodes (12 values) left of the tile instead of 1, the voxel box 4 words left of it;
@@ -256,29 +258,31 @@ constexpr int HY = TY + 2, HZ = TZ + 2;          // x halo rows and planes
 constexpr int XLEFT = 4;                         // halo box starts XLEFT nodes left of the tile
 constexpr int PROW = 112;                        // halo box row: nodes i0-4 .. i0+33, 112 values
 constexpr int VX = TX + 1, VY = TY + 1, VZ = TZ + 1;  // voxel words needed per axis
-constexpr int WROW = 40;                         // voxel box row: words i0-4 .. i0+35
+constexpr int WROW = 36;                         // voxel box row: words i0-4 .. i0+31 (144 bytes)
 constexpr int TROW = 3 * TX;                     // tile box row (r, d, 1/diag, y): 96 values
 static_assert(3 * (TX + 1 + XLEFT) <= PROW, "halo row");
 static_assert(VX + XLEFT - 1 <= WROW, "voxel row");
 
 enum { TOP_APPLY = 0, TOP_CHEB = 1, TOP_RESID = 2, TOP_DOT = 3 };
 
-// tensor maps of one tiled launch: x (halo box), the voxel words, r, d, 1/diag and y (tile boxes)
+// tensor maps of one tiled launch: x (halo box), the voxel words, r, d and y (tile boxes)
 struct TileMaps {
-    CUtensorMap x, w, r, d, inv, y;
+    CUtensorMap x, w, r, d, y;
 };
 
 template <class T>
 struct TileIO {
     float c1, c2;      // CHEB: d = c1 d + c2 D^-1 (r - K x)
     int raw;           // APPLY: keep held DOFs
+    int partial;       // DOT: leave the step to the boundary-node kernel (st->pqPart holds the tiles' share)
 };
 
 __host__ __device__ constexpr uint32_t packTile(int tx, int ty, int tz) { return uint32_t(tx) | (uint32_t(ty) << 11) | (uint32_t(tz) << 22); }
 
-// shared-memory layout of a tile CTA, every TMA destination on a 128-byte boundary:
-// x halo, voxel words, K x per tile node (then the y tile), r, d, 1/diag (smoother / residual),
-// node masks, the gather list, the warp counts and the barrier
+// shared-memory layout of a tile CTA, every TMA destination on a 128-byte boundary: x halo, voxel
+// words, the output tile (r for the smoother and residual epilogues, overwritten by y in place;
+// a separate y tile otherwise), d (smoother, updated in place) and two staging barriers (x and
+// words; the epilogue operands)
 __host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
 __host__ __device__ constexpr bool tileHasR(int mode) { return mode == TOP_CHEB || mode == TOP_RESID; }
 __host__ __device__ constexpr bool tileHasD(int mode) { return mode == TOP_CHEB; }
@@ -286,17 +290,23 @@ template <class T> __host__ __device__ constexpr size_t tileBytesX() { return si
 __host__ __device__ constexpr size_t tileBytesW() { return sizeof(uint32_t) * WROW * VY * VZ; }
 template <class T> __host__ __device__ constexpr size_t tileBytesT() { return sizeof(T) * TROW * TY * TZ; }
 template <class T> __host__ __device__ constexpr size_t tileOffW() { return align128(tileBytesX<T>()); }
-template <class T> __host__ __device__ constexpr size_t tileOffK() { return tileOffW<T>() + align128(tileBytesW()); }
-template <class T, int MODE> __host__ __device__ constexpr size_t tileOffR() { return tileOffK<T>() + align128(tileBytesT<T>()); }
-template <class T, int MODE> __host__ __device__ constexpr size_t tileOffD() { return tileOffR<T, MODE>() + (tileHasR(MODE) ? align128(tileBytesT<float>()) : 0); }
-template <class T, int MODE> __host__ __device__ constexpr size_t tileOffI() { return tileOffD<T, MODE>() + (tileHasD(MODE) ? align128(tileBytesT<float>()) : 0); }
-template <class T, int MODE> __host__ __device__ constexpr size_t tileOffM() { return tileOffI<T, MODE>() + (tileHasD(MODE) ? align128(tileBytesT<float>()) : 0); }
-template <class T, int MODE> __host__ __device__ constexpr size_t tileOffB() { return tileOffM<T, MODE>() + align128(TILE_NODES); }
-template <class T, int MODE> __host__ __device__ constexpr size_t tileOffBar() { return tileOffB<T, MODE>() + align128(2 * TILE_NODES + 4 * 8); }
+template <class T> __host__ __device__ constexpr size_t tileOffY() { return tileOffW<T>() + align128(tileBytesW()); }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileOffD() {
+    return tileOffY<T>() + align128(tileHasR(MODE) ? tileBytesT<float>() : tileBytesT<T>());
+}
+// 32-bit tiles compute their boundary nodes themselves (a compacted list in shared memory);
+// 64-bit tiles leave them to the boundary-node kernel
+template <class T> __host__ __device__ constexpr bool tileInnerBoundary() { return sizeof(T) == 4; }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileOffM() { return tileOffD<T, MODE>() + (tileHasD(MODE) ? align128(tileBytesT<float>()) : 0); }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileOffB() { return tileOffM<T, MODE>() + (tileInnerBoundary<T>() ? align128(TILE_NODES) : 0); }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileOffBar() {
+    return tileOffB<T, MODE>() + (tileInnerBoundary<T>() ? align128(2 * TILE_NODES + 4 * 8) : 0);
+}
 template <class T, int MODE> __host__ __device__ constexpr size_t tileSmemBytes() { return tileOffBar<T, MODE>() + 16; }
-// bytes the staging barrier expects
-template <class T, int MODE> __host__ __device__ constexpr unsigned tileStageBytes() {
-    return unsigned(tileBytesX<T>() + tileBytesW() + (tileHasR(MODE) ? tileBytesT<float>() : 0) + (tileHasD(MODE) ? 2 * tileBytesT<float>() : 0));
+// bytes each staging barrier expects
+template <class T> __host__ __device__ constexpr unsigned tileStage0Bytes() { return unsigned(tileBytesX<T>() + tileBytesW()); }
+template <int MODE> __host__ __device__ constexpr unsigned tileStage1Bytes() {
+    return unsigned((tileHasR(MODE) ? tileBytesT<float>() : 0) + (tileHasD(MODE) ? tileBytesT<float>() : 0));
 }
 
 // ---- TMA and shared-memory barrier primitives (PTX, sm_90 and later; no cluster multicast)
@@ -351,62 +361,73 @@ __device__ __forceinline__ int vOff(int vx, int vy, int vz) { return (vz * VY + 
 
 template <class T, bool OWN16, bool DIFF>
 struct TileOp {
-    // K x at tile node (cx, cy, cz) by the per-voxel gather; own = the node's value when DIFF
+    // adds voxel V's rows at tile node (cx, cy, cz) to acc (V = di + 2 dj + 4 dk: the voxel at
+    // offset (di - 1, dj - 1, dk - 1) from the node); own = the node's value when DIFF. V is a
+    // compile-time constant, so every Kb coefficient is a constant-bank FMA operand.
+    template <int V>
+    static __device__ __forceinline__ void voxel(const LevelView& L, const Coefs<T>& C, const T* xs, const uint32_t* vs, int cx, int cy, int cz,
+                                                 T acc[3], const T own[3]) {
+        constexpr int di = V & 1, dj = (V >> 1) & 1, dk = V >> 2;
+        constexpr int a = cornerOf(1 - di, 1 - dj, 1 - dk);
+        const uint32_t w = vs[vOff(cx + di, cy + dj, cz + dk)];
+        if (w == 0) return;
+        T xe[24];
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const int bx = (b == 1 || b == 2 || b == 5 || b == 6), by = (b == 2 || b == 3 || b == 6 || b == 7), bz = b >> 2;
+            const T* xp = xs + xOff(cx + di + bx - 1, cy + dj + by - 1, cz + dk + bz - 1);
+            xe[3 * b] = xp[0] - own[0];
+            xe[3 * b + 1] = xp[1] - own[1];
+            xe[3 * b + 2] = xp[2] - own[2];
+        }
+        if (!(w & OWN_BIT)) {
+            T t0 = 0, t1 = 0, t2 = 0;
+#pragma unroll
+            for (int q = 0; q < 24; q++) {
+                t0 += C.Kb[(3 * a + 0) * 24 + q] * xe[q];
+                t1 += C.Kb[(3 * a + 1) * 24 + q] * xe[q];
+                t2 += C.Kb[(3 * a + 2) * 24 + q] * xe[q];
+            }
+            const T s = T(__uint_as_float(w));
+            acc[0] += s * t0;
+            acc[1] += s * t1;
+            acc[2] += s * t2;
+        } else if (OWN16) {
+            const __half2* K2 = reinterpret_cast<const __half2*>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a);
+            T t[3] = {0, 0, 0};
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+#pragma unroll
+                for (int q = 0; q < 12; q++) {
+                    const float2 kv = __half22float2(__ldg(K2 + d * 12 + q));
+                    t[d] += T(kv.x) * xe[2 * q] + T(kv.y) * xe[2 * q + 1];
+                }
+            acc[0] += T(L.hs) * t[0];
+            acc[1] += T(L.hs) * t[1];
+            acc[2] += T(L.hs) * t[2];
+        } else {
+            const float4* K4 = reinterpret_cast<const float4*>(L.own + (long long)(w & ~OWN_BIT) * 576 + 72 * a);
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+#pragma unroll
+                for (int q = 0; q < 6; q++) {
+                    const float4 kv = __ldg(K4 + d * 6 + q);
+                    acc[d] += T(kv.x) * xe[4 * q] + T(kv.y) * xe[4 * q + 1] + T(kv.z) * xe[4 * q + 2] + T(kv.w) * xe[4 * q + 3];
+                }
+        }
+    }
+    // K x at tile node (cx, cy, cz) by the per-voxel gather over its 8 voxels
     static __device__ __forceinline__ void general(const LevelView& L, const Coefs<T>& C, const T* xs, const uint32_t* vs, int cx, int cy,
                                                    int cz, T acc[3], const T own[3]) {
         acc[0] = acc[1] = acc[2] = T(0);
-#pragma unroll
-        for (int v = 0; v < 8; v++) {
-            const int di = v & 1, dj = (v >> 1) & 1, dk = v >> 2;
-            // voxel (i - 1 + di, ...) is tile voxel (cx + di, cy + dj, cz + dk) with the halo offset
-            const uint32_t w = vs[vOff(cx + di, cy + dj, cz + dk)];
-            if (w == 0) continue;
-            const int a = cornerOf(1 - di, 1 - dj, 1 - dk);
-            T xe[24];
-#pragma unroll
-            for (int b = 0; b < 8; b++) {
-                const int bx = (b == 1 || b == 2 || b == 5 || b == 6), by = (b == 2 || b == 3 || b == 6 || b == 7), bz = b >> 2;
-                const T* xp = xs + xOff(cx + di + bx - 1, cy + dj + by - 1, cz + dk + bz - 1);
-                xe[3 * b] = xp[0] - own[0];
-                xe[3 * b + 1] = xp[1] - own[1];
-                xe[3 * b + 2] = xp[2] - own[2];
-            }
-            if (!(w & OWN_BIT)) {
-                T t0 = 0, t1 = 0, t2 = 0;
-#pragma unroll
-                for (int q = 0; q < 24; q++) {
-                    t0 += C.Kb[(3 * a + 0) * 24 + q] * xe[q];
-                    t1 += C.Kb[(3 * a + 1) * 24 + q] * xe[q];
-                    t2 += C.Kb[(3 * a + 2) * 24 + q] * xe[q];
-                }
-                const T s = T(__uint_as_float(w));
-                acc[0] += s * t0;
-                acc[1] += s * t1;
-                acc[2] += s * t2;
-            } else if (OWN16) {
-                const __half2* K2 = reinterpret_cast<const __half2*>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a);
-                T t[3] = {0, 0, 0};
-#pragma unroll
-                for (int d = 0; d < 3; d++)
-#pragma unroll
-                    for (int q = 0; q < 12; q++) {
-                        const float2 kv = __half22float2(__ldg(K2 + d * 12 + q));
-                        t[d] += T(kv.x) * xe[2 * q] + T(kv.y) * xe[2 * q + 1];
-                    }
-                acc[0] += T(L.hs) * t[0];
-                acc[1] += T(L.hs) * t[1];
-                acc[2] += T(L.hs) * t[2];
-            } else {
-                const float4* K4 = reinterpret_cast<const float4*>(L.own + (long long)(w & ~OWN_BIT) * 576 + 72 * a);
-#pragma unroll
-                for (int d = 0; d < 3; d++)
-#pragma unroll
-                    for (int q = 0; q < 6; q++) {
-                        const float4 kv = __ldg(K4 + d * 6 + q);
-                        acc[d] += T(kv.x) * xe[4 * q] + T(kv.y) * xe[4 * q + 1] + T(kv.z) * xe[4 * q + 2] + T(kv.w) * xe[4 * q + 3];
-                    }
-            }
-        }
+        voxel<0>(L, C, xs, vs, cx, cy, cz, acc, own);
+        voxel<1>(L, C, xs, vs, cx, cy, cz, acc, own);
+        voxel<2>(L, C, xs, vs, cx, cy, cz, acc, own);
+        voxel<3>(L, C, xs, vs, cx, cy, cz, acc, own);
+        voxel<4>(L, C, xs, vs, cx, cy, cz, acc, own);
+        voxel<5>(L, C, xs, vs, cx, cy, cz, acc, own);
+        voxel<6>(L, C, xs, vs, cx, cy, cz, acc, own);
+        voxel<7>(L, C, xs, vs, cx, cy, cz, acc, own);
     }
 
     // unscaled stencil sums of the thread's whole column (cz = 0..TZ-1) at once: every plane of the

@@ -46,6 +46,7 @@ namespace dev {
 
 struct SolveState {
     double bnorm, rel, tol, rz, alpha, beta, rmax, scale, peak, est, pq, foldFactor;
+    double pqPart;  // the tiled product's share of p.q, completed by the boundary-node kernel
     double vscale;  // the scale the current FP32 right-hand side r32 was made with (r32 = r * vscale)
     int it, maxIter, done, status, fold, folds, first, mixed;
     int err;  // a device-side failure (ST_ERR_*): the solve is ended and reported as a CUDA error
@@ -273,119 +274,57 @@ __global__ void __launch_bounds__(256) k_op8(LevelView L, Coefs<T> C, const T* _
 constexpr unsigned TILE_WAIT_POLLS = 1u << 22;
 constexpr int ST_ERR_STAGING = 1, ST_ERR_ALIGN = 2;
 
-// the staged tile's compute passes and epilogue (block-uniform: every thread calls it)
-template <class T, int MODE, bool OWN16, bool DIFF>
-__device__ __forceinline__ void tileBody(const LevelView& L, const Coefs<T>& C, const TileIO<T>& io, const TileMaps& maps, int i0, int j0,
-                                         int k0, const uint8_t (&mk)[TZ], bool anyUniform, const T* xs, const uint32_t* vs, T* ks,
-                                         const float* rs, float* ds, const float* is, const uint8_t* ms, uint16_t* blist, int* wsum,
-                                         double& dot) {
-    using Op = TileOp<T, OWN16, DIFF>;
-    const int tid = threadIdx.x, cx = tid & 31, cy = tid >> 5;
-    const long long PXY = (long long)L.PX * L.NY;
-    // pass 1: uniform nodes of the thread's column, all four from one sweep of the planes
-    unsigned bmask = 0;
+// the epilogue of tile node (cx, cy, cz) with its K x: results into the output tile (and d)
+template <class T, int MODE>
+__device__ __forceinline__ void tileFinish(const LevelView& L, const TileIO<T>& io, int i0, int j0, int k0, int cx, int cy, int cz, uint8_t mask,
+                                           const T kxIn[3], const float inv[3], const T* xs, T* ys, float* rs, float* ds, double& dot) {
+    const int base = (cz * TY + cy) * TROW + 3 * cx, xb = xOff(cx, cy, cz);
+    const bool act = mask & NM_ACTIVE;
 #pragma unroll
-    for (int z = 0; z < TZ; z++)
-        if ((mk[z] & NM_ACTIVE) && !(mk[z] & NM_UNIFORM)) bmask |= 1u << z;
-    if (anyUniform) {
-        T acc[TZ][3];
-        Op::column(C, xs, cx, cy, acc);
-#pragma unroll
-        for (int z = 0; z < TZ; z++) {
-            if (!(mk[z] & NM_UNIFORM)) continue;
-            const T s = T(__uint_as_float(vs[vOff(cx, cy, z)]));
-            T* kp = ks + (z * TY + cy) * TROW + 3 * cx;
-            kp[0] = s * acc[z][0];
-            kp[1] = s * acc[z][1];
-            kp[2] = s * acc[z][2];
+    for (int comp = 0; comp < 3; comp++) {
+        const int e = base + comp;
+        const bool fx = fixedDof(mask, comp);
+        const T xv = xs[xb + comp];
+        T kx = act ? kxIn[comp] : T(0);
+        if (act && L.dadd) {
+            const long long id = 3 * ((long long)(i0 + cx) + (long long)L.PX * ((j0 + cy) + (long long)L.NY * (k0 + cz))) + comp;
+            kx += (sizeof(T) == 8 ? T(L.dadd[id]) : T(L.dadd32[id])) * xv;
         }
-    }
-    // deterministic compaction: thread order, then z
-    const int cnt = __popc(bmask);
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (cx >= o) incl += v;
-    }
-    if (cx == 31) wsum[cy] = incl;
-    __syncthreads();
-    int off = incl - cnt, total = 0;
-#pragma unroll
-    for (int w = 0; w < TILE_THREADS / 32; w++) {
-        const int c = wsum[w];
-        off += (w < cy) ? c : 0;
-        total += c;
-    }
-    for (unsigned b = bmask; b; b &= b - 1) blist[off++] = uint16_t((tid << 4) | (__ffs(b) - 1));
-    __syncthreads();
-    // pass 2: the listed nodes, all threads
-    for (int q = tid; q < total; q += TILE_THREADS) {
-        const int e = blist[q], bt = e >> 4, bz = e & 15, bx = bt & 31, by = bt >> 5;
-        T own[3], acc[3];
-        own[0] = own[1] = own[2] = T(0);
-        if (DIFF) {
-            const T* xn = xs + xOff(bx, by, bz);
-            own[0] = xn[0]; own[1] = xn[1]; own[2] = xn[2];
-        }
-        Op::general(L, C, xs, vs, bx, by, bz, acc, own);
-        T* kp = ks + (bz * TY + by) * TROW + 3 * bx;
-        kp[0] = acc[0];
-        kp[1] = acc[1];
-        kp[2] = acc[2];
-    }
-    __syncthreads();
-    // pass 3: the epilogue in shared memory, one warp per row of 32 nodes (96 contiguous values);
-    // the results replace K x (y) and d in place
-#pragma unroll
-    for (int rr = 0; rr < TY * TZ / (TILE_THREADS / 32); rr++) {
-        const int row = cy + rr * (TILE_THREADS / 32), z = row / TY, y = row - z * TY;
-#pragma unroll
-        for (int q = 0; q < 3; q++) {
-            const int c3 = cx + 32 * q, ex = c3 / 3, comp = c3 - 3 * ex, e = row * TROW + c3;
-            const uint8_t mask = ms[(z * TY + y) * TX + ex];
-            const bool act = mask & NM_ACTIVE;
-            const bool fx = fixedDof(mask, comp);
-            const T xv = xs[xOff(ex, y, z) + comp];
-            T kx = act ? ks[e] : T(0);
-            if (act && L.dadd) {
-                const long long id = 3 * ((long long)(i0 + ex) + (long long)L.PX * (j0 + y) + PXY * (k0 + z)) + comp;
-                kx += (sizeof(T) == 8 ? T(L.dadd[id]) : T(L.dadd32[id])) * xv;
-            }
-            if (MODE == TOP_APPLY) {
-                ks[e] = (!io.raw && fx) ? T(0) : kx;
-            } else if (MODE == TOP_RESID) {
-                ks[e] = fx ? T(0) : T(rs[e]) - kx;
-            } else if (MODE == TOP_DOT) {
-                const T yv = fx ? T(0) : kx;
-                ks[e] = yv;
-                dot += double(xv) * double(yv);
+        if constexpr (MODE == TOP_APPLY) {
+            ys[e] = (!io.raw && fx) ? T(0) : kx;
+        } else if constexpr (MODE == TOP_DOT) {
+            const T yv = fx ? T(0) : kx;
+            ys[e] = yv;
+            dot += double(xv) * double(yv);
+        } else if constexpr (MODE == TOP_RESID) {
+            rs[e] = fx ? 0.f : rs[e] - float(kx);
+        } else {
+            if (fx) {
+                ds[e] = 0.f;
+                rs[e] = 0.f;
             } else {
-                if (fx) {
-                    ds[e] = 0.f;
-                    ks[e] = T(0);
-                } else {
-                    const float dn = io.c1 * ds[e] + io.c2 * is[e] * (rs[e] - float(kx));
-                    ds[e] = dn;
-                    ks[e] = xv + T(dn);
-                }
+                const float dn = io.c1 * ds[e] + io.c2 * inv[comp] * (rs[e] - float(kx));
+                ds[e] = dn;
+                rs[e] = float(xv) + dn;
             }
         }
-    }
-    fenceAsyncShared();
-    __syncthreads();
-    if (tid == 0) {
-        tmaStore3d(&maps.y, ks, 3 * i0, j0, k0);
-        if (tileHasD(MODE)) tmaStore3d(&maps.d, ds, 3 * i0, j0, k0);
-        tmaStoreCommitWait();
     }
 }
 
+// resident CTAs per SM the register budget is cut for (32-bit / 64-bit values)
+#ifndef PSFEA_TILE_CTAS32
+#define PSFEA_TILE_CTAS32 3
+#endif
+#ifndef PSFEA_TILE_CTAS64
+#define PSFEA_TILE_CTAS64 2
+#endif
+
 template <class T, int MODE, bool OWN16, bool DIFF>
-__global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(LevelView L, Coefs<T> C, const uint32_t* __restrict__ tiles,
-                                                          const __grid_constant__ TileMaps maps, TileIO<T> io, SolveState* st, double* partials,
-                                                          unsigned* ticket, Ctl ctl) {
+__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS64 : PSFEA_TILE_CTAS32)
+    k_tile(LevelView L, Coefs<T> C, const uint32_t* __restrict__ tiles, const __grid_constant__ TileMaps maps, TileIO<T> io, SolveState* st,
+           double* partials, unsigned* ticket, Ctl ctl) {
     if (skipped(ctl)) return;
+    using Op = TileOp<T, OWN16, DIFF>;
     extern __shared__ __align__(128) unsigned char smem[];
     if (smemAddr(smem) & 127u) {  // the layout's TMA alignment (never expected to fail)
         if (threadIdx.x == 0) {
@@ -396,32 +335,33 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(LevelView L, Coefs<T> 
     }
     T* xs = reinterpret_cast<T*>(smem);
     uint32_t* vs = reinterpret_cast<uint32_t*>(smem + tileOffW<T>());
-    T* ks = reinterpret_cast<T*>(smem + tileOffK<T>());  // K x per tile node, [z][y][3 x + c]; then y
-    float* rs = reinterpret_cast<float*>(smem + tileOffR<T, MODE>());
+    T* ys = reinterpret_cast<T*>(smem + tileOffY<T>());        // y tile (APPLY / DOT)
+    float* rs = reinterpret_cast<float*>(smem + tileOffY<T>()); // r tile, then y in place (CHEB / RESID)
     float* ds = reinterpret_cast<float*>(smem + tileOffD<T, MODE>());
-    float* is = reinterpret_cast<float*>(smem + tileOffI<T, MODE>());
     uint8_t* ms = smem + tileOffM<T, MODE>();
     uint16_t* blist = reinterpret_cast<uint16_t*>(smem + tileOffB<T, MODE>());
     int* wsum = reinterpret_cast<int*>(blist + TILE_NODES);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + tileOffBar<T, MODE>());
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + tileOffBar<T, MODE>());  // [0] x and words, [1] r and d
     const uint32_t tw = tiles[blockIdx.x];
     const int i0 = int(tw & 2047u) * TX, j0 = int((tw >> 11) & 2047u) * TY, k0 = int(tw >> 22) * TZ;
     const int tid = threadIdx.x, cx = tid & 31, cy = tid >> 5;
     const long long PXY = (long long)L.PX * L.NY;
 
-    // stage: one thread issues every copy on one barrier
+    // stage: one thread issues every copy, on two barriers
     if (tid == 0) {
         mbarInit(bar, 1);
-        mbarExpectTx(bar, tileStageBytes<T, MODE>());
+        mbarInit(bar + 1, 1);
+        mbarExpectTx(bar, tileStage0Bytes<T>());
         tmaLoad3d(xs, &maps.x, 3 * (i0 - XLEFT), j0 - 1, k0 - 1, bar);
         tmaLoad3d(vs, &maps.w, i0 - XLEFT, j0 - 1, k0 - 1, bar);
-        if (tileHasR(MODE)) tmaLoad3d(rs, &maps.r, 3 * i0, j0, k0, bar);
-        if (tileHasD(MODE)) {
-            tmaLoad3d(ds, &maps.d, 3 * i0, j0, k0, bar);
-            tmaLoad3d(is, &maps.inv, 3 * i0, j0, k0, bar);
+        if (tileHasR(MODE)) {
+            mbarExpectTx(bar + 1, tileStage1Bytes<MODE>());
+            tmaLoad3d(rs, &maps.r, 3 * i0, j0, k0, bar + 1);
+            if (tileHasD(MODE)) tmaLoad3d(ds, &maps.d, 3 * i0, j0, k0, bar + 1);
         }
     }
-    // the column's node masks meanwhile (padding nodes i >= NX hold 7: inactive, all held)
+    // the column's node masks (padding nodes i >= NX hold 7: inactive, all held) and, for the
+    // smoother, its 1/diag, meanwhile
     const int i = i0 + cx, j = j0 + cy;
     const bool col = i < L.PX && j < L.NY;
     uint8_t mk[TZ];
@@ -430,22 +370,166 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(LevelView L, Coefs<T> 
     for (int z = 0; z < TZ; z++) {
         const int k = k0 + z;
         mk[z] = (col && k < L.NZ) ? __ldg(L.nmask + i + (long long)L.PX * j + PXY * k) : uint8_t(0);
-        ms[(z * TY + cy) * TX + cx] = mk[z];
+        if (tileInnerBoundary<T>()) ms[(z * TY + cy) * TX + cx] = mk[z];
         anyUniform = anyUniform || (mk[z] & NM_UNIFORM);
     }
-    __syncthreads();  // the barrier is initialised, the masks are in place
-    const bool staged = __syncthreads_and(mbarWait(bar, TILE_WAIT_POLLS));
+    __syncthreads();  // barriers initialised; masks in place
+    bool staged = __syncthreads_and(mbarWait(bar, TILE_WAIT_POLLS));
+    double dot = 0.0;
+    if (staged) {
+        // pass 1: the thread's column, all four nodes from one sweep of the planes (uniform nodes)
+        T acc[TZ][3];
+        if (anyUniform) Op::column(C, xs, cx, cy, acc);
+        // the smoother's 1/diag of the column (read while the second barrier is awaited)
+        float inv[TZ][3];
+#pragma unroll
+        for (int z = 0; z < TZ; z++) {
+            const long long n = i + (long long)L.PX * j + PXY * (k0 + z);
+            const bool in = tileHasD(MODE) && (mk[z] & NM_ACTIVE);  // active nodes lie inside the grid
+#pragma unroll
+            for (int c = 0; c < 3; c++) inv[z][c] = in ? __ldg(L.invD + 3 * n + c) : 0.f;
+        }
+        if (tileHasR(MODE)) staged = __syncthreads_and(mbarWait(bar + 1, TILE_WAIT_POLLS));
+        if (staged) {
+            // epilogue of the column's nodes except the active non-uniform (boundary) ones
+            unsigned bmask = 0;
+#pragma unroll
+            for (int z = 0; z < TZ; z++) {
+                if ((mk[z] & NM_ACTIVE) && !(mk[z] & NM_UNIFORM)) {
+                    bmask |= 1u << z;
+                    continue;
+                }
+                T kx[3] = {T(0), T(0), T(0)};
+                if (mk[z] & NM_UNIFORM) {
+                    const T s = T(__uint_as_float(vs[vOff(cx, cy, z)]));
+                    kx[0] = s * acc[z][0];
+                    kx[1] = s * acc[z][1];
+                    kx[2] = s * acc[z][2];
+                }
+                tileFinish<T, MODE>(L, io, i0, j0, k0, cx, cy, z, mk[z], kx, inv[z], xs, ys, rs, ds, dot);
+            }
+            if constexpr (tileInnerBoundary<T>()) {
+                // deterministic compaction of the boundary nodes: thread order, then z
+                const int cnt = __popc(bmask);
+                int incl = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (cx >= o) incl += v;
+                }
+                if (cx == 31) wsum[cy] = incl;
+                __syncthreads();
+                int off = incl - cnt, total = 0;
+#pragma unroll
+                for (int w = 0; w < TILE_THREADS / 32; w++) {
+                    const int c = wsum[w];
+                    off += (w < cy) ? c : 0;
+                    total += c;
+                }
+                for (unsigned b = bmask; b; b &= b - 1) blist[off++] = uint16_t((tid << 4) | (__ffs(b) - 1));
+                __syncthreads();
+                // the listed nodes, one thread each, packed into as few warps as possible
+                for (int q = tid; q < total; q += TILE_THREADS) {
+                    const int e = blist[q], bt = e >> 4, bz = e & 15, bx = bt & 31, by = bt >> 5;
+                    T own[3] = {T(0), T(0), T(0)};
+                    if (DIFF) {
+                        const T* xn = xs + xOff(bx, by, bz);
+                        own[0] = xn[0]; own[1] = xn[1]; own[2] = xn[2];
+                    }
+                    T a[3];
+                    Op::general(L, C, xs, vs, bx, by, bz, a, own);
+                    float iv[3] = {0.f, 0.f, 0.f};
+                    if (tileHasD(MODE)) {
+                        const long long n = (i0 + bx) + (long long)L.PX * (j0 + by) + PXY * (k0 + bz);
+                        iv[0] = __ldg(L.invD + 3 * n);
+                        iv[1] = __ldg(L.invD + 3 * n + 1);
+                        iv[2] = __ldg(L.invD + 3 * n + 2);
+                    }
+                    tileFinish<T, MODE>(L, io, i0, j0, k0, bx, by, bz, ms[(bz * TY + by) * TX + bx], a, iv, xs, ys, rs, ds, dot);
+                }
+            }
+            // results out
+            fenceAsyncShared();
+            __syncthreads();
+            if (tid == 0) {
+                if (tileHasR(MODE)) tmaStore3d(&maps.y, rs, 3 * i0, j0, k0);
+                else tmaStore3d(&maps.y, ys, 3 * i0, j0, k0);
+                if (tileHasD(MODE)) tmaStore3d(&maps.d, ds, 3 * i0, j0, k0);
+                tmaStoreCommitWait();
+            }
+        }
+    }
     if (!staged && tid == 0) {
         atomicExch(&st->err, ST_ERR_STAGING);
         st->done = 1;
     }
-    double dot = 0.0;
-    if (staged) tileBody<T, MODE, OWN16, DIFF>(L, C, io, maps, i0, j0, k0, mk, anyUniform, xs, vs, ks, rs, ds, is, ms, blist, wsum, dot);
     if (MODE == TOP_DOT) {
-        double v[1] = {dot};
+        double vv[1] = {dot};
+        double tot[1];
+        if (gridReduce<1>(vv, 0u, partials, ticket, tot) && threadIdx.x == 0) {
+            const double pq = tot[0];
+            if (io.partial) {  // the boundary-node kernel adds its share and finishes the step
+                st->pqPart = pq;
+                return;
+            }
+            st->pq = pq;
+            if (!(pq > 0)) {
+                st->status = ST_BREAKDOWN;
+                if (st->mixed) st->fold = 1;  // fold what there is, then stop
+                else st->done = 1;
+            } else {
+                st->alpha = st->rz / pq;
+            }
+        }
+    }
+}
+
+// The boundary nodes of a tiled level (active, not uniform: next to an empty voxel, a voxel of
+// another scale or an own matrix) from their list, one thread each, with the per-voxel gather and
+// the tiled kernel's epilogues (TOP_*); runs after the tiled kernel on the same vectors and
+// overwrites the boundary nodes' output slots. TOP_DOT adds its p.q share to the tiled one
+// (fixed order: tiles, then boundary nodes) and takes the CG step.
+template <class T, int MODE, bool OWN16, bool DIFF>
+__global__ void __launch_bounds__(NODE_THREADS) k_bnd(LevelView L, Coefs<T> C, const int* __restrict__ list, int count, const T* __restrict__ x,
+                                                      T* __restrict__ y, const float* __restrict__ r, float* __restrict__ d, float c1, float c2,
+                                                      int raw, SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
+    if (skipped(ctl)) return;
+    double v[1] = {0.0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count; t += (long long)gridDim.x * blockDim.x) {
+        const long long n = list[t];
+        const uint8_t mask = __ldg(L.nmask + n);
+        int i, j, k;
+        nodeCoords(L, n, i, j, k);
+        T acc[3];
+        applyAt<T, OWN16, DIFF>(L, C, x, i, j, k, n, mask, acc, L.PX, n);
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const long long id = 3 * n + q;
+            const bool fx = fixedDof(mask, q);
+            if (MODE == TOP_APPLY) {
+                y[id] = (!raw && fx) ? T(0) : acc[q];
+            } else if (MODE == TOP_DOT) {
+                const T yv = fx ? T(0) : acc[q];
+                y[id] = yv;
+                v[0] += double(x[id]) * double(yv);
+            } else if (MODE == TOP_RESID) {
+                y[id] = fx ? T(0) : T(r[id]) - acc[q];
+            } else {
+                if (fx) {
+                    d[id] = 0.f;
+                    y[id] = T(0);
+                } else {
+                    const float dn = c1 * d[id] + c2 * L.invD[id] * (r[id] - float(acc[q]));
+                    d[id] = dn;
+                    y[id] = x[id] + T(dn);
+                }
+            }
+        }
+    }
+    if (MODE == TOP_DOT) {
         double tot[1];
         if (gridReduce<1>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) {
-            const double pq = tot[0];
+            const double pq = st->pqPart + tot[0];
             st->pq = pq;
             if (!(pq > 0)) {
                 st->status = ST_BREAKDOWN;
@@ -1239,13 +1323,15 @@ struct DevLevel {
     DevMem word, nmask, own, own16, invD, dadd, dadd32, bc;
     DevMem tiles;      // packed (tx, ty, tz) of the 32 x 8 x 4 node tiles with an active node
     int nTiles = 0;
+    DevMem blist;      // tiled levels: the boundary nodes (pitched indices, increasing)
+    int nBnd = 0;
     bool useTiles = false;  // tiled kernel (large levels) or one thread per node (small ones)
     bool use8 = false;      // eight lanes per node (the smallest levels)
     float cf0 = 0, cf1 = 0, cf2 = 0, omega = 0.5f;
     std::vector<float> chebC1, chebC2;  // steps 1 .. degree-1 of the Chebyshev smoother: d = c1 d + c2 D^-1 (r - K z)
     bool hasOwn = false;
     void release() {
-        for (DevMem* b : {&word, &nmask, &own, &own16, &invD, &dadd, &dadd32, &bc, &tiles}) b->release();
+        for (DevMem* b : {&word, &nmask, &own, &own16, &invD, &dadd, &dadd32, &bc, &tiles, &blist}) b->release();
     }
 };
 
@@ -1400,6 +1486,15 @@ void SharedModel::uploadLevel(int l) {
         int64_t max8 = 30000;
         if (const char* e = std::getenv("PSFEA_OP8_MAX_NODES")) max8 = std::atoll(e);
         D.use8 = !D.useTiles && l > 0 && h.nNodes <= max8;
+        if (D.useTiles) {  // for the 64-bit tiled kernels
+            std::vector<int32_t> bl(h.boundary.size());
+            for (size_t q = 0; q < bl.size(); q++) {
+                const int64_t nd = h.boundary[q], row = nd / h.NX;
+                bl[q] = int32_t((nd - row * h.NX) + int64_t(PX) * row);
+            }
+            D.nBnd = int(bl.size());
+            upload(D.blist, bl, bytes, ms);
+        }
     }
     dev::LevelView& v = D.view;
     v.nx = h.nx; v.ny = h.ny; v.nz = h.nz; v.NX = h.NX; v.NY = h.NY; v.NZ = h.NZ;
@@ -1621,14 +1716,17 @@ void SolverImpl::op64(int l, const double* xin, double* y, bool raw, dev::Ctl ct
                    nullptr, 0.f, 0.f, raw ? 1 : 0, ctl);
         return;
     }
-    dev::TileIO<double> io{0.f, 0.f, raw ? 1 : 0};
+    dev::TileIO<double> io{0.f, 0.f, raw ? 1 : 0, 0};
     dev::TileMaps mp;
     mp.x = mapOf(xin, MAP_HALO, true, l);
     mp.w = mapOf(D.word.p, MAP_WORDS, false, l);
     mp.y = mapOf(y, MAP_TILE, true, l);
-    mp.r = mp.d = mp.inv = mp.y;  // not read by this epilogue
+    mp.r = mp.d = mp.y;  // not read by this epilogue
     launch(dev::k_tile<double, dev::TOP_APPLY, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double, dev::TOP_APPLY>(), stream,
            D.view, D.c64, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), ctl);
+    if (D.nBnd)
+        launch(dev::k_bnd<double, dev::TOP_APPLY, false, false>, nodeGrid(D.nBnd), dev::NODE_THREADS, 0, stream, D.view, D.c64,
+               D.blist.as<int>(), D.nBnd, xin, y, nullptr, nullptr, 0.f, 0.f, raw ? 1 : 0, st(), part(), tick(), ctl);
 }
 
 template <int MODE>
@@ -1653,14 +1751,13 @@ void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev
         return;
     }
     constexpr int TM = MODE == dev::OP_CHEB ? dev::TOP_CHEB : (MODE == dev::OP_RESID ? dev::TOP_RESID : dev::TOP_APPLY);
-    dev::TileIO<float> io{c1, c2, 0};
+    dev::TileIO<float> io{c1, c2, 0, 0};
     dev::TileMaps mp;
     mp.x = mapOf(xin, MAP_HALO, false, l);
     mp.w = mapOf(D.word.p, MAP_WORDS, false, l);
     mp.y = mapOf(y, MAP_TILE, false, l);
     mp.r = dev::tileHasR(TM) ? mapOf(rr, MAP_TILE, false, l) : mp.y;
     mp.d = dev::tileHasD(TM) ? mapOf(dd, MAP_TILE, false, l) : mp.y;
-    mp.inv = dev::tileHasD(TM) ? mapOf(D.invD.p, MAP_TILE, false, l) : mp.y;
     const size_t sm = dev::tileSmemBytes<float, TM>();
     const uint32_t* tl = D.tiles.as<uint32_t>();
     if (diff) launch(dev::k_tile<float, TM, true, true>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
@@ -1831,14 +1928,17 @@ void SolverImpl::recordPlainIteration(dev::Ctl ctl) {
         launch(dev::k_apply_alpha<double, false>, nodeGrid(pn(0)), dev::NODE_THREADS, 0, stream, D.view, D.c64, p.as<double>(), q.as<double>(),
                st(), part(), tick(), ctl);
     } else {
-        dev::TileIO<double> io{0.f, 0.f, 0};
+        dev::TileIO<double> io{0.f, 0.f, 0, D.nBnd ? 1 : 0};
         dev::TileMaps mp;
         mp.x = mapOf(p.p, MAP_HALO, true, 0);
         mp.w = mapOf(D.word.p, MAP_WORDS, false, 0);
         mp.y = mapOf(q.p, MAP_TILE, true, 0);
-        mp.r = mp.d = mp.inv = mp.y;
+        mp.r = mp.d = mp.y;
         launch(dev::k_tile<double, dev::TOP_DOT, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double, dev::TOP_DOT>(), stream,
                D.view, D.c64, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), ctl);
+        if (D.nBnd)
+            launch(dev::k_bnd<double, dev::TOP_DOT, false, false>, nodeGrid(D.nBnd), dev::NODE_THREADS, 0, stream, D.view, D.c64,
+                   D.blist.as<int>(), D.nBnd, p.as<double>(), q.as<double>(), nullptr, nullptr, 0.f, 0.f, 0, st(), part(), tick(), ctl);
     }
     const bool one = exactOneLevel();
     launch(dev::k_cg_update, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, x.as<double>(), r.as<double>(), p.as<double>(),
@@ -1868,12 +1968,12 @@ void SolverImpl::recordMixedIteration(dev::Ctl ctl) {
         launch(dev::k_apply_alpha<float, true>, nodeGrid(pn(0)), dev::NODE_THREADS, 0, stream, D.view, D.c32, p32.as<float>(), q32.as<float>(),
                st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
     } else {
-        dev::TileIO<float> io{0.f, 0.f, 0};
+        dev::TileIO<float> io{0.f, 0.f, 0, 0};
         dev::TileMaps mp;
         mp.x = mapOf(p32.p, MAP_HALO, false, 0);
         mp.w = mapOf(D.word.p, MAP_WORDS, false, 0);
         mp.y = mapOf(q32.p, MAP_TILE, false, 0);
-        mp.r = mp.d = mp.inv = mp.y;
+        mp.r = mp.d = mp.y;
         launch(dev::k_tile<float, dev::TOP_DOT, false, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float, dev::TOP_DOT>(), stream, D.view,
                D.c32, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
     }
