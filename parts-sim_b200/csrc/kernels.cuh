@@ -41,6 +41,11 @@ struct Coefs {
     T S[243];   // [m][3 d + c], m = (ox+1) + 3 (oy+1) + 9 (oz+1)
     T Kb[576];  // row-major 24x24
 };
+// the 32-bit coefficients also as duplicated pairs (s, s), the operand of a paired FMA that
+// advances two nodes at once
+struct Coefs32 : Coefs<float> {
+    float2 S2[243];
+};
 
 // corner index of the unit offset (x, y, z)
 __host__ __device__ constexpr int cornerOf(int x, int y, int z) { return (y ? (x ? 2 : 3) : (x ? 1 : 0)) + 4 * z; }
@@ -327,13 +332,14 @@ __device__ __forceinline__ bool mbarTryWait(uint64_t* bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
-// bounded wait for the barrier's phase 0: false after `limit` polls (each poll may suspend the
-// thread for a hardware-defined time)
-__device__ __forceinline__ bool mbarWait(uint64_t* bar, unsigned limit) {
+// bounded wait for the completion of the barrier phase with the given parity: false after `limit`
+// polls (each poll may suspend the thread for a hardware-defined time)
+__device__ __forceinline__ bool mbarWaitParity(uint64_t* bar, unsigned parity, unsigned limit) {
     for (unsigned it = 0; it < limit; it++)
-        if (mbarTryWait(bar, 0)) return true;
+        if (mbarTryWait(bar, parity)) return true;
     return false;
 }
+__device__ __forceinline__ bool mbarWait(uint64_t* bar, unsigned limit) { return mbarWaitParity(bar, 0, limit); }
 // 3-D tiled load of a box at element coordinates (c0, c1, c2) into shared memory, completing on bar
 __device__ __forceinline__ void tmaLoad3d(void* dst, const void* map, int c0, int c1, int c2, uint64_t* bar) {
     asm volatile(
@@ -472,6 +478,51 @@ struct TileOp {
                     if (oy && oz) { a[1] += C.S[m * 9 + 5] * x2; a[2] += C.S[m * 9 + 7] * x1; }
                 }
             }
+        }
+    }
+
+    // the same column sums with paired FMAs (__ffma2_rn, two nodes per instruction; each lane of
+    // the pair rounds exactly like fmaf): nodes (0, 1) and (2, 3) of the column advance together,
+    // fed by the pair of planes (p, p + 1) that the two nodes see at the same offset
+    static __device__ __forceinline__ void column2(const Coefs32& C, const float* xs, int cx, int cy, float acc[TZ][3]) {
+        static_assert(TZ == 4, "node pairs (0, 1) and (2, 3)");
+        float2 A[2][3];
+#pragma unroll
+        for (int h = 0; h < 2; h++) A[h][0] = A[h][1] = A[h][2] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int p = -1; p <= 3; p++) {
+            float2 v[9][3];
+#pragma unroll
+            for (int b = 0; b < 9; b++) {
+                const float* x0 = xs + xOff(cx + b % 3 - 1, cy + b / 3 - 1, p);
+                const float* x1 = xs + xOff(cx + b % 3 - 1, cy + b / 3 - 1, p + 1);
+                v[b][0] = make_float2(x0[0], x1[0]);
+                v[b][1] = make_float2(x0[1], x1[1]);
+                v[b][2] = make_float2(x0[2], x1[2]);
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int oz = p - 2 * h;  // pair h = nodes (2h, 2h + 1) sees planes (p, p + 1) at offset oz
+                if (oz < -1 || oz > 1) continue;
+#pragma unroll
+                for (int b = 0; b < 9; b++) {
+                    const int ox = b % 3 - 1, oy = b / 3 - 1, m = (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1);
+                    float2* a = A[h];
+                    a[0] = __ffma2_rn(C.S2[m * 9 + 0], v[b][0], a[0]);
+                    a[1] = __ffma2_rn(C.S2[m * 9 + 4], v[b][1], a[1]);
+                    a[2] = __ffma2_rn(C.S2[m * 9 + 8], v[b][2], a[2]);
+                    if (ox && oy) { a[0] = __ffma2_rn(C.S2[m * 9 + 1], v[b][1], a[0]); a[1] = __ffma2_rn(C.S2[m * 9 + 3], v[b][0], a[1]); }
+                    if (ox && oz) { a[0] = __ffma2_rn(C.S2[m * 9 + 2], v[b][2], a[0]); a[2] = __ffma2_rn(C.S2[m * 9 + 6], v[b][0], a[2]); }
+                    if (oy && oz) { a[1] = __ffma2_rn(C.S2[m * 9 + 5], v[b][2], a[1]); a[2] = __ffma2_rn(C.S2[m * 9 + 7], v[b][1], a[2]); }
+                }
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            acc[0][d] = A[0][d].x;
+            acc[1][d] = A[0][d].y;
+            acc[2][d] = A[1][d].x;
+            acc[3][d] = A[1][d].y;
         }
     }
 

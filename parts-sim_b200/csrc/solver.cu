@@ -319,9 +319,12 @@ __device__ __forceinline__ void tileFinish(const LevelView& L, const TileIO<T>& 
 #define PSFEA_TILE_CTAS64 2
 #endif
 
+template <class T> struct CoefsFor { using type = Coefs<T>; };
+template <> struct CoefsFor<float> { using type = Coefs32; };
+
 template <class T, int MODE, bool OWN16, bool DIFF>
 __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS64 : PSFEA_TILE_CTAS32)
-    k_tile(LevelView L, Coefs<T> C, const uint32_t* __restrict__ tiles, const __grid_constant__ TileMaps maps, TileIO<T> io, SolveState* st,
+    k_tile(LevelView L, typename CoefsFor<T>::type C, const uint32_t* __restrict__ tiles, const __grid_constant__ TileMaps maps, TileIO<T> io, SolveState* st,
            double* partials, unsigned* ticket, Ctl ctl) {
     if (skipped(ctl)) return;
     using Op = TileOp<T, OWN16, DIFF>;
@@ -379,7 +382,10 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS
     if (staged) {
         // pass 1: the thread's column, all four nodes from one sweep of the planes (uniform nodes)
         T acc[TZ][3];
-        if (anyUniform) Op::column(C, xs, cx, cy, acc);
+        if (anyUniform) {
+            if constexpr (sizeof(T) == 4) Op::column2(C, xs, cx, cy, acc);
+            else Op::column(C, xs, cx, cy, acc);
+        }
         // the smoother's 1/diag of the column (read while the second barrier is awaited)
         float inv[TZ][3];
 #pragma unroll
@@ -1319,7 +1325,7 @@ CUtensorMap makeMap(const void* base, MapKind kind, bool f64, const dev::LevelVi
 struct DevLevel {
     dev::LevelView view{};
     dev::Coefs<double> c64{};
-    dev::Coefs<float> c32{};
+    dev::Coefs32 c32{};
     DevMem word, nmask, own, own16, invD, dadd, dadd32, bc;
     DevMem tiles;      // packed (tx, ty, tz) of the 32 x 8 x 4 node tiles with an active node
     int nTiles = 0;
@@ -1411,6 +1417,7 @@ void SharedModel::adopt(Hierarchy&& h) {
         set(dev::k_tile<float, dev::TOP_RESID, false, false>, dev::tileSmemBytes<float, dev::TOP_RESID>());
         set(dev::k_tile<float, dev::TOP_RESID, true, false>, dev::tileSmemBytes<float, dev::TOP_RESID>());
         set(dev::k_tile<float, dev::TOP_RESID, true, true>, dev::tileSmemBytes<float, dev::TOP_RESID>());
+        set(dev::k_tile<float, dev::TOP_DOT, false, true>, dev::tileSmemBytes<float, dev::TOP_DOT>());
     });
     L.resize(H.levels.size());
     for (int l = 0; l < int(H.levels.size()); l++) uploadLevel(l);
@@ -1516,6 +1523,7 @@ void SharedModel::uploadLevel(int l) {
         for (int e = 0; e < 9; e++) {
             D.c64.S[m * 9 + e] = h.S[m][e];
             D.c32.S[m * 9 + e] = float(h.S[m][e]);
+            D.c32.S2[m * 9 + e] = make_float2(float(h.S[m][e]), float(h.S[m][e]));
         }
 }
 
