@@ -50,6 +50,8 @@ def parse():
                     help="build the model and launch only this level-0 operator kernel --reps times (a small, fixed "
                          "launch sequence for profilers); prints its mean CUDA-event time")
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--batch-rhs", type=int, default=32, help="load cases of the batched SIMP leg (0: skip the leg)")
+    ap.add_argument("--serve-requests", type=int, default=64, help="requests of the serving leg (0: skip the leg)")
     return ap.parse_args()
 
 
@@ -191,6 +193,68 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def batched_leg(nrhs):
+    """The multi-RHS workload: the SIMP grid (192x96x96, graded E = 1e-9 + rho^3) with `nrhs` unit
+    loads, solved through the host API one at a time with the plain FP64 MG-PCG and as one batch
+    (ps_fea_solve_batch: concurrent solve contexts over one shared hierarchy). Wall-clock time of
+    each call sequence, host buffers in and out; solved MDOF/s = nrhs * nDOF / time."""
+    import torch
+    import psfea
+    from psfea import workloads as W
+    m = W.simp(nrhs=nrhs)
+    S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    F = np.ascontiguousarray(m.f)
+    S.solve(F[0], tol=TOL, max_iter=MAX_ITER, precision="fp64")  # smoother setup, warm-up
+    S.solve_batch(F[:2], tol=TOL, max_iter=MAX_ITER, precision="mixed")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    seq = [S.solve(F[q], tol=TOL, max_iter=MAX_ITER, precision="fp64") for q in range(nrhs)]
+    t_seq = time.perf_counter() - t0
+    out = {"workload": f"simp {m.dims[0]}x{m.dims[1]}x{m.dims[2]}, {nrhs} unit loads on the top centre line, rtol 1e-8",
+           "n_dof": m.n_dof, "plain_fp64_sequential": {"value": nrhs * m.n_dof / t_seq / 1e6, "unit": "MDOF/s", "seconds": t_seq,
+                                                       "iterations_max": max(r.iterations for r in seq)}}
+    for prec in ("fp64", "mixed"):
+        t0 = time.perf_counter()
+        res = S.solve_batch(F, tol=TOL, max_iter=MAX_ITER, precision=prec)
+        t = time.perf_counter() - t0
+        ok = all(r.converged for r in res)
+        out[f"batched_{prec}"] = {"value": nrhs * m.n_dof / t / 1e6, "unit": "MDOF/s", "seconds": t, "converged": ok,
+                                  "iterations_max": max(r.iterations for r in res)}
+    out["batched_mixed_over_plain_sequential"] = out["batched_mixed"]["value"] / out["plain_fp64_sequential"]["value"]
+    S.close()
+    return out
+
+
+def serving_leg(n):
+    """The serving stream: the first `n` requests of the Poisson stream (200 requests/s; box grids
+    24-160 voxels per axis with spherical voids, random material, face and traction; rtol 1e-8,
+    mixed precision), submitted at their arrival times to the continuous-batching server; latency =
+    submit to result, per request."""
+    import psfea
+    from psfea import workloads as W
+    reqs = list(W.serving_stream(n=n))
+    srv = psfea.Server()
+    t0 = time.perf_counter()
+    ids = []
+    for ta, m in reqs:
+        now = time.perf_counter() - t0
+        if ta > now:
+            time.sleep(ta - now)
+        ids.append((srv.submit(m.dims, m.density, m.nu, m.bc, m.f, tol=TOL, max_iter=MAX_ITER, precision="mixed",
+                               coarsest_max_dof=m.coarsest_max_dof), m.n_dof))
+    res = [srv.wait(rid, keep_u=False) for rid, _ in ids]
+    span = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    lat = np.array([r["total_s"] for r in res]) * 1e3
+    dofs = sum(nd for _, nd in ids)
+    return {"workload": f"serving stream, first {n} requests at 200 req/s (box grids 24-160 voxels per axis), rtol 1e-8, mixed",
+            "requests": n, "converged": int(sum(r["converged"] for r in res)), "MDOF_per_s": dofs / span / 1e6, "makespan_s": span,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+            "solve_ms_p50": float(np.percentile([r["solve_s"] * 1e3 for r in res], 50)),
+            "peak_active": int(st["peak_active"]), "peak_device_bytes": int(st["peak_device_bytes"])}
+
+
 def kernel_only(args):
     import torch
     import psfea
@@ -282,6 +346,9 @@ def main():
             pg.barrier()
             pg.destroy_process_group()
         return
+    # the multi-RHS and serving workloads, on one GPU (rank 0 of a replica run skips them)
+    batched = batched_leg(args.batch_rhs) if args.batch_rhs > 0 and world == 1 else None
+    serving = serving_leg(args.serve_requests) if args.serve_requests > 0 and world == 1 else None
     cb = None
     if world == 1 and not args.no_cpu_baseline:
         try:
@@ -306,6 +373,8 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                      "kernel": "k_tile<float,TOP_CHEB> level 0 (FP32 Chebyshev step)", "ms": ms_cheb,
                      "algorithmic_bytes": alg_bytes, "peak_kind": peak_kind, "fp64_apply_ms": ms_apply64},
+        "batched": batched,
+        "serving": serving,
         "cpu_baseline": cb,
         "gpu_launches": int(kmx),
         "clocks": clk.summary(),

@@ -270,9 +270,9 @@ static_assert(VX + XLEFT - 1 <= WROW, "voxel row");
 
 enum { TOP_APPLY = 0, TOP_CHEB = 1, TOP_RESID = 2, TOP_DOT = 3 };
 
-// tensor maps of one tiled launch: x (halo box), the voxel words, r, d and y (tile boxes)
+// tensor maps of one tiled launch: x (halo box), the voxel words, r, d, 1/diag and y (tile boxes)
 struct TileMaps {
-    CUtensorMap x, w, r, d, y;
+    CUtensorMap x, w, r, d, inv, y;
 };
 
 template <class T>
@@ -286,8 +286,8 @@ __host__ __device__ constexpr uint32_t packTile(int tx, int ty, int tz) { return
 
 // shared-memory layout of a tile CTA, every TMA destination on a 128-byte boundary: x halo, voxel
 // words, the output tile (r for the smoother and residual epilogues, overwritten by y in place;
-// a separate y tile otherwise), d (smoother, updated in place) and two staging barriers (x and
-// words; the epilogue operands)
+// a separate y tile otherwise), d (smoother, updated in place), 1/diag (smoother), the node masks
+// and boundary list (32-bit) and two staging barriers (x and words; the epilogue operands)
 __host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
 __host__ __device__ constexpr bool tileHasR(int mode) { return mode == TOP_CHEB || mode == TOP_RESID; }
 __host__ __device__ constexpr bool tileHasD(int mode) { return mode == TOP_CHEB; }
@@ -302,7 +302,8 @@ template <class T, int MODE> __host__ __device__ constexpr size_t tileOffD() {
 // 32-bit tiles compute their boundary nodes themselves (a compacted list in shared memory);
 // 64-bit tiles leave them to the boundary-node kernel
 template <class T> __host__ __device__ constexpr bool tileInnerBoundary() { return sizeof(T) == 4; }
-template <class T, int MODE> __host__ __device__ constexpr size_t tileOffM() { return tileOffD<T, MODE>() + (tileHasD(MODE) ? align128(tileBytesT<float>()) : 0); }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileOffI() { return tileOffD<T, MODE>() + (tileHasD(MODE) ? align128(tileBytesT<float>()) : 0); }
+template <class T, int MODE> __host__ __device__ constexpr size_t tileOffM() { return tileOffI<T, MODE>() + (tileHasD(MODE) ? align128(tileBytesT<float>()) : 0); }
 template <class T, int MODE> __host__ __device__ constexpr size_t tileOffB() { return tileOffM<T, MODE>() + (tileInnerBoundary<T>() ? align128(TILE_NODES) : 0); }
 template <class T, int MODE> __host__ __device__ constexpr size_t tileOffBar() {
     return tileOffB<T, MODE>() + (tileInnerBoundary<T>() ? align128(2 * TILE_NODES + 4 * 8) : 0);
@@ -311,7 +312,7 @@ template <class T, int MODE> __host__ __device__ constexpr size_t tileSmemBytes(
 // bytes each staging barrier expects
 template <class T> __host__ __device__ constexpr unsigned tileStage0Bytes() { return unsigned(tileBytesX<T>() + tileBytesW()); }
 template <int MODE> __host__ __device__ constexpr unsigned tileStage1Bytes() {
-    return unsigned((tileHasR(MODE) ? tileBytesT<float>() : 0) + (tileHasD(MODE) ? tileBytesT<float>() : 0));
+    return unsigned((tileHasR(MODE) ? tileBytesT<float>() : 0) + (tileHasD(MODE) ? 2 * tileBytesT<float>() : 0));
 }
 
 // ---- TMA and shared-memory barrier primitives (PTX, sm_90 and later; no cluster multicast)

@@ -277,7 +277,7 @@ constexpr int ST_ERR_STAGING = 1, ST_ERR_ALIGN = 2;
 // the epilogue of tile node (cx, cy, cz) with its K x: results into the output tile (and d)
 template <class T, int MODE>
 __device__ __forceinline__ void tileFinish(const LevelView& L, const TileIO<T>& io, int i0, int j0, int k0, int cx, int cy, int cz, uint8_t mask,
-                                           const T kxIn[3], const float inv[3], const T* xs, T* ys, float* rs, float* ds, double& dot) {
+                                           const T kxIn[3], const float* is, const T* xs, T* ys, float* rs, float* ds, double& dot) {
     const int base = (cz * TY + cy) * TROW + 3 * cx, xb = xOff(cx, cy, cz);
     const bool act = mask & NM_ACTIVE;
 #pragma unroll
@@ -303,7 +303,7 @@ __device__ __forceinline__ void tileFinish(const LevelView& L, const TileIO<T>& 
                 ds[e] = 0.f;
                 rs[e] = 0.f;
             } else {
-                const float dn = io.c1 * ds[e] + io.c2 * inv[comp] * (rs[e] - float(kx));
+                const float dn = io.c1 * ds[e] + io.c2 * is[e] * (rs[e] - float(kx));
                 ds[e] = dn;
                 rs[e] = float(xv) + dn;
             }
@@ -341,6 +341,7 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS
     T* ys = reinterpret_cast<T*>(smem + tileOffY<T>());        // y tile (APPLY / DOT)
     float* rs = reinterpret_cast<float*>(smem + tileOffY<T>()); // r tile, then y in place (CHEB / RESID)
     float* ds = reinterpret_cast<float*>(smem + tileOffD<T, MODE>());
+    const float* is = reinterpret_cast<const float*>(smem + tileOffI<T, MODE>());
     uint8_t* ms = smem + tileOffM<T, MODE>();
     uint16_t* blist = reinterpret_cast<uint16_t*>(smem + tileOffB<T, MODE>());
     int* wsum = reinterpret_cast<int*>(blist + TILE_NODES);
@@ -360,7 +361,10 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS
         if (tileHasR(MODE)) {
             mbarExpectTx(bar + 1, tileStage1Bytes<MODE>());
             tmaLoad3d(rs, &maps.r, 3 * i0, j0, k0, bar + 1);
-            if (tileHasD(MODE)) tmaLoad3d(ds, &maps.d, 3 * i0, j0, k0, bar + 1);
+            if (tileHasD(MODE)) {
+                tmaLoad3d(ds, &maps.d, 3 * i0, j0, k0, bar + 1);
+                tmaLoad3d(const_cast<float*>(is), &maps.inv, 3 * i0, j0, k0, bar + 1);
+            }
         }
     }
     // the column's node masks (padding nodes i >= NX hold 7: inactive, all held) and, for the
@@ -386,15 +390,6 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS
             if constexpr (sizeof(T) == 4) Op::column2(C, xs, cx, cy, acc);
             else Op::column(C, xs, cx, cy, acc);
         }
-        // the smoother's 1/diag of the column (read while the second barrier is awaited)
-        float inv[TZ][3];
-#pragma unroll
-        for (int z = 0; z < TZ; z++) {
-            const long long n = i + (long long)L.PX * j + PXY * (k0 + z);
-            const bool in = tileHasD(MODE) && (mk[z] & NM_ACTIVE);  // active nodes lie inside the grid
-#pragma unroll
-            for (int c = 0; c < 3; c++) inv[z][c] = in ? __ldg(L.invD + 3 * n + c) : 0.f;
-        }
         if (tileHasR(MODE)) staged = __syncthreads_and(mbarWait(bar + 1, TILE_WAIT_POLLS));
         if (staged) {
             // epilogue of the column's nodes except the active non-uniform (boundary) ones
@@ -412,7 +407,7 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS
                     kx[1] = s * acc[z][1];
                     kx[2] = s * acc[z][2];
                 }
-                tileFinish<T, MODE>(L, io, i0, j0, k0, cx, cy, z, mk[z], kx, inv[z], xs, ys, rs, ds, dot);
+                tileFinish<T, MODE>(L, io, i0, j0, k0, cx, cy, z, mk[z], kx, is, xs, ys, rs, ds, dot);
             }
             if constexpr (tileInnerBoundary<T>()) {
                 // deterministic compaction of the boundary nodes: thread order, then z
@@ -444,14 +439,7 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS
                     }
                     T a[3];
                     Op::general(L, C, xs, vs, bx, by, bz, a, own);
-                    float iv[3] = {0.f, 0.f, 0.f};
-                    if (tileHasD(MODE)) {
-                        const long long n = (i0 + bx) + (long long)L.PX * (j0 + by) + PXY * (k0 + bz);
-                        iv[0] = __ldg(L.invD + 3 * n);
-                        iv[1] = __ldg(L.invD + 3 * n + 1);
-                        iv[2] = __ldg(L.invD + 3 * n + 2);
-                    }
-                    tileFinish<T, MODE>(L, io, i0, j0, k0, bx, by, bz, ms[(bz * TY + by) * TX + bx], a, iv, xs, ys, rs, ds, dot);
+                    tileFinish<T, MODE>(L, io, i0, j0, k0, bx, by, bz, ms[(bz * TY + by) * TX + bx], a, is, xs, ys, rs, ds, dot);
                 }
             }
             // results out
@@ -1729,7 +1717,7 @@ void SolverImpl::op64(int l, const double* xin, double* y, bool raw, dev::Ctl ct
     mp.x = mapOf(xin, MAP_HALO, true, l);
     mp.w = mapOf(D.word.p, MAP_WORDS, false, l);
     mp.y = mapOf(y, MAP_TILE, true, l);
-    mp.r = mp.d = mp.y;  // not read by this epilogue
+    mp.r = mp.d = mp.inv = mp.y;  // not read by this epilogue
     launch(dev::k_tile<double, dev::TOP_APPLY, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double, dev::TOP_APPLY>(), stream,
            D.view, D.c64, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), ctl);
     if (D.nBnd)
@@ -1766,6 +1754,7 @@ void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev
     mp.y = mapOf(y, MAP_TILE, false, l);
     mp.r = dev::tileHasR(TM) ? mapOf(rr, MAP_TILE, false, l) : mp.y;
     mp.d = dev::tileHasD(TM) ? mapOf(dd, MAP_TILE, false, l) : mp.y;
+    mp.inv = dev::tileHasD(TM) ? mapOf(D.invD.p, MAP_TILE, false, l) : mp.y;
     const size_t sm = dev::tileSmemBytes<float, TM>();
     const uint32_t* tl = D.tiles.as<uint32_t>();
     if (diff) launch(dev::k_tile<float, TM, true, true>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
@@ -1941,7 +1930,7 @@ void SolverImpl::recordPlainIteration(dev::Ctl ctl) {
         mp.x = mapOf(p.p, MAP_HALO, true, 0);
         mp.w = mapOf(D.word.p, MAP_WORDS, false, 0);
         mp.y = mapOf(q.p, MAP_TILE, true, 0);
-        mp.r = mp.d = mp.y;
+        mp.r = mp.d = mp.inv = mp.y;
         launch(dev::k_tile<double, dev::TOP_DOT, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double, dev::TOP_DOT>(), stream,
                D.view, D.c64, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), ctl);
         if (D.nBnd)
@@ -1981,7 +1970,7 @@ void SolverImpl::recordMixedIteration(dev::Ctl ctl) {
         mp.x = mapOf(p32.p, MAP_HALO, false, 0);
         mp.w = mapOf(D.word.p, MAP_WORDS, false, 0);
         mp.y = mapOf(q32.p, MAP_TILE, false, 0);
-        mp.r = mp.d = mp.y;
+        mp.r = mp.d = mp.inv = mp.y;
         launch(dev::k_tile<float, dev::TOP_DOT, false, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float, dev::TOP_DOT>(), stream, D.view,
                D.c32, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
     }
