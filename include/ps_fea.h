@@ -52,10 +52,16 @@ typedef enum ps_precision {
      * V-cycle with r scaled to order one, exactly the reference's VoxelFEA::solve
      * (voxel_fea.cpp:835-927). */
     PS_PREC_FP64 = 0,
-    /* FP32 CG and FP32 V-cycle with FP16 coarse-level element matrices, kept to FP64 accuracy by
-     * reliable updates: whenever the FP32 residual has dropped tenfold the FP32 iterate is folded
-     * into the FP64 solution and the FP64 defect f - K u replaces the FP32 residual. */
-    PS_PREC_MIXED = 1
+    /* The same FP64 flexible CG with a reduced-precision preconditioner: the FP32 V-cycle reads
+     * every own (Galerkin) element matrix as FP16 times a power-of-two level scale, halving the
+     * HBM traffic of the coarse levels' operators. The Krylov recurrence and its iteration count
+     * are those of PS_PREC_FP64. */
+    PS_PREC_MIXED = 1,
+    /* FP32 CG and FP32 V-cycle with FP16 element matrices, kept to FP64 accuracy by reliable
+     * updates: whenever the FP32 residual has dropped tenfold the FP32 iterate is folded into the
+     * FP64 solution and the FP64 defect f - K u replaces the FP32 residual. On ill-conditioned
+     * models the FP32 recurrence needs markedly more iterations than the FP64 one. */
+    PS_PREC_FP32 = 2
 } ps_precision;
 
 typedef struct ps_fea ps_fea_t;
@@ -76,7 +82,7 @@ typedef struct ps_solve_result {
     int32_t iterations;   /* CG iterations (voxel_fea.hpp:121) */
     int32_t converged;    /* residual <= 10 * tol */
     int32_t status;       /* ps_status of the outcome */
-    int32_t folds;        /* PS_PREC_MIXED: number of FP64 reliable updates */
+    int32_t folds;        /* PS_PREC_FP32: number of FP64 reliable updates */
     double residual;      /* true relative residual ||f - K u|| / ||f_free||, in FP64 */
     double seconds;       /* wall time of the call */
     int64_t kernels;      /* device kernels this call launched */

@@ -81,7 +81,7 @@ ps_status ps_fea_solve(ps_fea_t* h, const double* f, const ps_solve_opts* opts, 
     return guarded([&] {
         if (!h || !f || !u_out) return fail(PS_EINVAL, "Force or displacement vector has the wrong size.");
         const ps_solve_opts o = resolve(opts);
-        if (!(o.tol >= 0) || o.max_iter < 0 || (o.precision != PS_PREC_FP64 && o.precision != PS_PREC_MIXED) || o.smoother_degree < 0 ||
+        if (!(o.tol >= 0) || o.max_iter < 0 || (o.precision < PS_PREC_FP64 || o.precision > PS_PREC_FP32) || o.smoother_degree < 0 ||
             o.smoother_degree > 8)
             return fail(PS_EINVAL, "invalid solve options");
         ps_solve_result r{};
@@ -95,7 +95,7 @@ ps_status ps_fea_solve_dev(ps_fea_t* h, const double* f_dev, const ps_solve_opts
     return guarded([&] {
         if (!h || !f_dev || !u_dev) return fail(PS_EINVAL, "Force or displacement vector has the wrong size.");
         const ps_solve_opts o = resolve(opts);
-        if (!(o.tol >= 0) || o.max_iter < 0 || (o.precision != PS_PREC_FP64 && o.precision != PS_PREC_MIXED) || o.smoother_degree < 0 ||
+        if (!(o.tol >= 0) || o.max_iter < 0 || (o.precision < PS_PREC_FP64 || o.precision > PS_PREC_FP32) || o.smoother_degree < 0 ||
             o.smoother_degree > 8)
             return fail(PS_EINVAL, "invalid solve options");
         ps_solve_result r{};
@@ -109,11 +109,11 @@ ps_status ps_fea_solve_batch(ps_fea_t* h, int32_t nrhs, const double* f, const p
     return guarded([&] {
         if (!h || !f || !u_out || nrhs < 0) return fail(PS_EINVAL, "Force or displacement vector has the wrong size.");
         const ps_solve_opts base = resolve(opts);
-        if (!(base.tol >= 0) || base.max_iter < 0 || (base.precision != PS_PREC_FP64 && base.precision != PS_PREC_MIXED) ||
+        if (!(base.tol >= 0) || base.max_iter < 0 || (base.precision < PS_PREC_FP64 || base.precision > PS_PREC_FP32) ||
             base.smoother_degree < 0 || base.smoother_degree > 8)
             return fail(PS_EINVAL, "invalid solve options");
         if (nrhs == 0) return PS_OK;
-        int concurrency = 8;
+        int concurrency = 2;  // concurrent solve contexts; two measured best on a B200 (each solve already fills the GPU)
         if (const char* e = std::getenv("PSFEA_BATCH_CONCURRENCY")) concurrency = std::max(1, std::atoi(e));
         return h->solver.solveBatch(nrhs, f, base, u_out, results, concurrency);
     });

@@ -1537,9 +1537,10 @@ struct SolverImpl {
     cudaEvent_t ev = nullptr;           // recorded after each asynchronous state read
     int64_t launches = 0;     // kernels launched by this context (graph replays add their kernel count)
     // graphs of one iteration, per precision, and the coefficient version they were recorded with
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    int64_t graphKernels[2] = {0, 0};
-    int64_t graphVersion[2] = {-1, -1};
+    // (by ps_precision: FP64 Krylov with the FP32 or the FP16-matrix V-cycle, FP32 Krylov)
+    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+    int64_t graphKernels[3] = {0, 0, 0};
+    int64_t graphVersion[3] = {-1, -1, -1};
 
     // smoother estimation in flight: its scratch (stream-ordered, freed as soon as the kernels
     // have run) and the Lanczos scalars of every level, copied to pinned host memory
@@ -1549,6 +1550,7 @@ struct SolverImpl {
     // the solve in progress (a resumable state machine, so one host thread can drive many)
     struct Pending {
         bool active = false, finishing = false, mixed = false, lanczos = false;
+        int graph = 0;  // the iteration graph in use
         const double* fDev = nullptr;
         const double* x0Dev = nullptr;
         ps_solve_opts o{};
@@ -1629,7 +1631,7 @@ struct SolverImpl {
     float* vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone = false);
     bool exactOneLevel() const { return M->exactOneLevel(); }
 
-    void recordPlainIteration(dev::Ctl ctl);
+    void recordPlainIteration(dev::Ctl ctl, bool own16);
     void recordMixedIteration(dev::Ctl ctl);
     // enqueue a solve (f, x0, u in device memory; uHost, if set, receives u as well)
     void startSolve(const double* fDev, const double* x0Dev, const ps_solve_opts& o, double* uDev, double* uHost);
@@ -1917,7 +1919,7 @@ void SolverImpl::prepareSmoothers() {
 }
 
 // one FP64 CG iteration (voxel_fea.cpp:901-919)
-void SolverImpl::recordPlainIteration(dev::Ctl ctl) {
+void SolverImpl::recordPlainIteration(dev::Ctl ctl, bool own16) {
     const HostLevel& h = H.levels[0];
     DevLevel& D = L[0];
     LevelWork& W0 = W[0];
@@ -1948,7 +1950,7 @@ void SolverImpl::recordPlainIteration(dev::Ctl ctl) {
         launch(dev::k_coarse<double, double>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(), r.as<double>(),
                z64.as<double>(), ctl);
     } else {
-        z32 = vcycle(0, ctl, false, true);  // r32 and the first smoothing step came with the update
+        z32 = vcycle(0, ctl, own16, true);  // r32 and the first smoothing step came with the update
     }
     launch(dev::k_cg_dots, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, r.as<double>(), z32, z64.as<double>(),
            q.as<double>(), st(), part(), tick(), ctl);
@@ -2015,7 +2017,9 @@ void SolverImpl::startIterations() {
     const HostLevel& h = H.levels[0];
     DevLevel& D = L[0];
     LevelWork& W0 = W[0];
-    const bool mixed = o.precision == PS_PREC_MIXED && !exactOneLevel();
+    // FP32 Krylov (PS_PREC_FP32); the FP64 Krylov forms differ only in the V-cycle's matrices
+    const bool mixed = o.precision == PS_PREC_FP32 && !exactOneLevel();
+    const bool own16 = o.precision == PS_PREC_MIXED && M->mixedOwn16;
     pend.mixed = mixed;
     const int64_t n = pd(0);
     // state
@@ -2053,7 +2057,7 @@ void SolverImpl::startIterations() {
         } else {
             launch(dev::k_vc_load, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, r.as<double>(), W0.r.as<float>(),
                    D.invD.as<float>(), W0.d.as<float>(), W0.z.as<float>(), D.cf0, st(), ctl);
-            z32 = vcycle(0, ctl, false, true);
+            z32 = vcycle(0, ctl, own16, true);
         }
         launch(dev::k_cg_dots, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, r.as<double>(), z32, z64.as<double>(),
                q.as<double>(), st(), part(), tick(), ctl);
@@ -2063,7 +2067,8 @@ void SolverImpl::startIterations() {
     launch(dev::k_clear_first, 1, 1, 0, stream, st());
     check(cudaGetLastError(), "solve setup");
     // the iteration graph (recorded once per precision and smoother version)
-    const int gi = mixed ? 1 : 0;
+    const int gi = mixed ? 2 : (own16 ? 1 : 0);
+    pend.graph = gi;
     if (graph[gi] && graphVersion[gi] != M->version) {
         cudaGraphExecDestroy(graph[gi]);
         graph[gi] = nullptr;
@@ -2072,7 +2077,7 @@ void SolverImpl::startIterations() {
         cudaGraph_t gr;
         check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
         if (mixed) recordMixedIteration(ctl);
-        else recordPlainIteration(ctl);
+        else recordPlainIteration(ctl, own16);
         check(cudaStreamEndCapture(stream, &gr), "capture end");
         size_t nodes = 0;
         check(cudaGraphGetNodes(gr, nullptr, &nodes), "graph nodes");
@@ -2130,7 +2135,7 @@ bool SolverImpl::advance(bool block, ps_solve_result& res) {
             pend.lastRel = rel;
             pend.lastIt = hs.it;
             const int batch = std::max(1, std::min(pend.batch, o.max_iter - hs.it + 1));
-            const int gi = mixed ? 1 : 0;
+            const int gi = pend.graph;
             for (int b = 0; b < batch; b++) check(cudaGraphLaunch(graph[gi], stream), "graph launch");
             launches += int64_t(batch) * graphKernels[gi];
             enqueueStateRead();

@@ -15,7 +15,7 @@ def requests(n, seed=17):
     return [W.box_with_voids(W.Rng(seed * 7919 + q), lo=12, hi=36) for q in range(n)]
 
 
-@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+@pytest.mark.parametrize("precision", ["mixed", "fp64", "fp32"])
 def test_results_identical_alone_and_in_the_mix(precision):
     models = requests(8)
     srv = psfea.Server(max_active=8, build_threads=4)
