@@ -52,6 +52,10 @@ def parse():
                     help="build the model and launch only this level-0 operator kernel --reps times (a small, fixed "
                          "launch sequence for profilers); prints its mean CUDA-event time")
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--solve-only", choices=["l_bracket", "simp"], default=None,
+                    help="build the model, run one warm-up solve and one solve of --precision (a fixed launch "
+                         "sequence for profilers); prints its time and iterations")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp32"])
     ap.add_argument("--batch-rhs", type=int, default=32, help="load cases of the batched SIMP leg (0: skip the leg)")
     ap.add_argument("--serve-requests", type=int, default=64, help="requests of the serving leg (0: skip the leg)")
     return ap.parse_args()
@@ -268,8 +272,26 @@ def kernel_only(args):
     print(json.dumps({"kernel": args.kernel_only, "reps": args.reps, "ms": ms}), flush=True)
 
 
+def solve_only(args):
+    import torch
+    import psfea
+    from psfea import workloads as W
+    m = W.l_bracket() if args.solve_only == "l_bracket" else W.simp(nrhs=1)
+    f = m.f if m.f.ndim == 1 else m.f[0]
+    S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    S.solve(f, tol=TOL, max_iter=MAX_ITER, precision=args.precision)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = S.solve(f, tol=TOL, max_iter=MAX_ITER, precision=args.precision)
+    print(json.dumps({"workload": args.solve_only, "precision": args.precision, "iterations": r.iterations, "residual": r.residual,
+                      "seconds": time.perf_counter() - t0, "kernels": r.kernels}), flush=True)
+
+
 def main():
     args = parse()
+    if args.solve_only:
+        solve_only(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return

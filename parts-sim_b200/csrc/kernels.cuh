@@ -38,8 +38,8 @@ struct LevelView {
 
 template <class T>
 struct Coefs {
-    T S[243];   // [m][3 d + c], m = (ox+1) + 3 (oy+1) + 9 (oz+1)
-    T Kb[576];  // row-major 24x24
+    alignas(16) T Kb[576];  // row-major 24x24 (16-byte aligned: read as pairs by the paired FMAs)
+    T S[243];               // [m][3 d + c], m = (ox+1) + 3 (oy+1) + 9 (oz+1)
 };
 // the 32-bit coefficients also as duplicated pairs (s, s), the operand of a paired FMA that
 // advances two nodes at once
@@ -49,6 +49,58 @@ struct Coefs32 : Coefs<float> {
 
 // corner index of the unit offset (x, y, z)
 __host__ __device__ constexpr int cornerOf(int x, int y, int z) { return (y ? (x ? 2 : 3) : (x ? 1 : 0)) + 4 * z; }
+
+// the three rows of corner a of a 24x24 matrix times the 24 corner values xe, added to t[3]:
+//   Kb (the level's uniform matrix, kernel parameter): 32-bit values pair consecutive columns in
+//   paired FMAs (__ffma2_rn; the pair's two partial sums are added at the end)
+//   own16 (FP16 Galerkin matrices): 16-byte loads of eight halves each, widened to the value type
+template <class T>
+__device__ __forceinline__ void kbRows(const T* Kb, int a, const T xe[24], T t[3]) {
+    if constexpr (sizeof(T) == 4) {
+        const float2* K2 = reinterpret_cast<const float2*>(Kb) + 36 * a;
+        float2 p0 = make_float2(0.f, 0.f), p1 = p0, p2 = p0;
+#pragma unroll
+        for (int q = 0; q < 12; q++) {
+            const float2 xq = make_float2(xe[2 * q], xe[2 * q + 1]);
+            p0 = __ffma2_rn(K2[q], xq, p0);
+            p1 = __ffma2_rn(K2[12 + q], xq, p1);
+            p2 = __ffma2_rn(K2[24 + q], xq, p2);
+        }
+        t[0] = p0.x + p0.y;
+        t[1] = p1.x + p1.y;
+        t[2] = p2.x + p2.y;
+    } else {
+        T t0 = 0, t1 = 0, t2 = 0;
+#pragma unroll
+        for (int q = 0; q < 24; q++) {
+            t0 += Kb[(3 * a + 0) * 24 + q] * xe[q];
+            t1 += Kb[(3 * a + 1) * 24 + q] * xe[q];
+            t2 += Kb[(3 * a + 2) * 24 + q] * xe[q];
+        }
+        t[0] = t0;
+        t[1] = t1;
+        t[2] = t2;
+    }
+}
+template <class T>
+__device__ __forceinline__ void own16Rows(const __half* M, const T xe[24], T t[3]) {
+    const uint4* K16 = reinterpret_cast<const uint4*>(M);  // 72 halves: rows d at [24 d, 24 d + 24)
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        T acc = 0;
+#pragma unroll
+        for (int g = 0; g < 3; g++) {
+            const uint4 u = __ldg(K16 + 3 * d + g);
+            const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const float2 kv = __half22float2(*reinterpret_cast<const __half2*>(&w[e]));
+                acc += T(kv.x) * xe[8 * g + 2 * e] + T(kv.y) * xe[8 * g + 2 * e + 1];
+            }
+        }
+        t[d] = acc;
+    }
+}
 
 // (K x) at node (i, j, k). Uniform nodes: s times the assembled stencil, structural zeros skipped
 // (entry (d, c) of neighbour o is zero by the cube's reflection symmetry unless d == c or both
@@ -115,27 +167,15 @@ __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, c
                 xe[3 * b + 2] = __ldg(xp + 2) - own2;
             }
             if (!(w & OWN_BIT)) {
-                T t0 = 0, t1 = 0, t2 = 0;
-#pragma unroll
-                for (int q = 0; q < 24; q++) {
-                    t0 += C.Kb[(3 * a + 0) * 24 + q] * xe[q];
-                    t1 += C.Kb[(3 * a + 1) * 24 + q] * xe[q];
-                    t2 += C.Kb[(3 * a + 2) * 24 + q] * xe[q];
-                }
+                T t[3];
+                kbRows<T>(C.Kb, a, xe, t);
                 const T s = T(__uint_as_float(w));
-                acc[0] += s * t0;
-                acc[1] += s * t1;
-                acc[2] += s * t2;
+                acc[0] += s * t[0];
+                acc[1] += s * t[1];
+                acc[2] += s * t[2];
             } else if (OWN16) {
-                const __half2* K2 = reinterpret_cast<const __half2*>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a);
-                T t[3] = {0, 0, 0};
-#pragma unroll
-                for (int d = 0; d < 3; d++)
-#pragma unroll
-                    for (int q = 0; q < 12; q++) {
-                        const float2 kv = __half22float2(__ldg(K2 + d * 12 + q));
-                        t[d] += T(kv.x) * xe[2 * q] + T(kv.y) * xe[2 * q + 1];
-                    }
+                T t[3];
+                own16Rows<T>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a, xe, t);
                 acc[0] += T(L.hs) * t[0];
                 acc[1] += T(L.hs) * t[1];
                 acc[2] += T(L.hs) * t[2];
@@ -388,27 +428,15 @@ struct TileOp {
             xe[3 * b + 2] = xp[2] - own[2];
         }
         if (!(w & OWN_BIT)) {
-            T t0 = 0, t1 = 0, t2 = 0;
-#pragma unroll
-            for (int q = 0; q < 24; q++) {
-                t0 += C.Kb[(3 * a + 0) * 24 + q] * xe[q];
-                t1 += C.Kb[(3 * a + 1) * 24 + q] * xe[q];
-                t2 += C.Kb[(3 * a + 2) * 24 + q] * xe[q];
-            }
+            T t[3];
+            kbRows<T>(C.Kb, a, xe, t);
             const T s = T(__uint_as_float(w));
-            acc[0] += s * t0;
-            acc[1] += s * t1;
-            acc[2] += s * t2;
+            acc[0] += s * t[0];
+            acc[1] += s * t[1];
+            acc[2] += s * t[2];
         } else if (OWN16) {
-            const __half2* K2 = reinterpret_cast<const __half2*>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a);
-            T t[3] = {0, 0, 0};
-#pragma unroll
-            for (int d = 0; d < 3; d++)
-#pragma unroll
-                for (int q = 0; q < 12; q++) {
-                    const float2 kv = __half22float2(__ldg(K2 + d * 12 + q));
-                    t[d] += T(kv.x) * xe[2 * q] + T(kv.y) * xe[2 * q + 1];
-                }
+            T t[3];
+            own16Rows<T>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a, xe, t);
             acc[0] += T(L.hs) * t[0];
             acc[1] += T(L.hs) * t[1];
             acc[2] += T(L.hs) * t[2];

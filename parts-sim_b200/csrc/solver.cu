@@ -204,17 +204,10 @@ __global__ void __launch_bounds__(256) k_op8(LevelView L, Coefs<T> C, const T* _
                     acc[1] = s * t1;
                     acc[2] = s * t2;
                 } else if (OWN16) {
-                    const __half2* K2 = reinterpret_cast<const __half2*>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a);
+                    T t[3];
+                    own16Rows<T>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a, xe, t);
 #pragma unroll
-                    for (int dd = 0; dd < 3; dd++) {
-                        T t = 0;
-#pragma unroll
-                        for (int q = 0; q < 12; q++) {
-                            const float2 kv = __half22float2(__ldg(K2 + dd * 12 + q));
-                            t += T(kv.x) * xe[2 * q] + T(kv.y) * xe[2 * q + 1];
-                        }
-                        acc[dd] = T(L.hs) * t;
-                    }
+                    for (int dd = 0; dd < 3; dd++) acc[dd] = T(L.hs) * t[dd];
                 } else {
                     const float4* K4 = reinterpret_cast<const float4*>(L.own + (long long)(w & ~OWN_BIT) * 576 + 72 * a);
 #pragma unroll
