@@ -35,6 +35,10 @@ MAX_ITER = 5000
 # mask byte, r, d, 1/diag read and d written: 4x12 B) and per solid voxel (its 4-byte word)
 BYTES_PER_NODE_CHEB32 = 12 + 12 + 1 + 4 * 12
 BYTES_PER_VOXEL = 4
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of that kernel on this
+# model, from an ncu capture of `bench.py --kernel-only cheb32` (the launch moves the algorithmic
+# bytes plus halo re-reads of partial tiles and the inactive node slots of active tiles)
+TRAFFIC_BYTES_CHEB32 = 209.6e6
 # iterations of the reference's FP64 MG-PCG on this model to 1e-8, measured with its own solver
 # (oracle/_ref, 8 threads): used to turn a bounded CPU sample into a full-solve time
 REFERENCE_ITERATIONS_L_BRACKET = 1181
@@ -398,7 +402,7 @@ def main():
                         "residual": res32[0]},
         "mixed_over_plain": value / plain,
         "e2e": {"value": e2e_value, "unit": "MDOF/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": TRAFFIC_BYTES_CHEB32,
                      "kernel": "k_tile<float,TOP_CHEB> level 0 (FP32 Chebyshev step)", "ms": ms_cheb,
                      "algorithmic_bytes": alg_bytes, "peak_kind": peak_kind, "fp64_apply_ms": ms_apply64},
         "batched": batched,
