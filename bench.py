@@ -44,6 +44,19 @@ TRAFFIC_BYTES_CHEB32 = 209.6e6
 REFERENCE_ITERATIONS_L_BRACKET = 1181
 
 
+WORKLOAD = "l_bracket 256x128x128 voxels (0.5 mm), 64 y-holes, y=0 held, 500 N tip patch, rtol 1e-8"
+
+
+def bench_config(m, world, levels=None, free_dof=None):
+    """the `config` object of both arms' lines"""
+    c = {"workload": WORKLOAD, "n_dof": m.n_dof, "parallelism": f"replicas x{world}",
+         "l2": "inputs > L2 (126 MB): x/r/d/1/diag at 51 MB each per level-0 vector"}
+    if levels is not None:
+        c["levels"] = levels
+        c["free_dof"] = free_dof
+    return c
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -56,12 +69,13 @@ def parse():
                     help="build the model and launch only this level-0 operator kernel --reps times (a small, fixed "
                          "launch sequence for profilers); prints its mean CUDA-event time")
     ap.add_argument("--reps", type=int, default=5)
-    ap.add_argument("--solve-only", choices=["l_bracket", "simp"], default=None,
+    ap.add_argument("--solve-only", choices=["l_bracket", "simp", "gyroid"], default=None,
                     help="build the model, run one warm-up solve and one solve of --precision (a fixed launch "
                          "sequence for profilers); prints its time and iterations")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp32"])
     ap.add_argument("--batch-rhs", type=int, default=32, help="load cases of the batched SIMP leg (0: skip the leg)")
     ap.add_argument("--serve-requests", type=int, default=64, help="requests of the serving leg (0: skip the leg)")
+    ap.add_argument("--large", type=int, default=1, help="1: the 85.8 M-DOF gyroid leg, 0: skip it")
     return ap.parse_args()
 
 
@@ -197,7 +211,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": v, "unit": "MDOF/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": m.n_dof / v / 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": "l_bracket 256x128x128 voxels, 64 holes, 500 N tip patch, rtol 1e-8", "n_dof": m.n_dof},
+            "config": bench_config(m, args.gpus),
             "cpu_baseline": {"value": v, "unit": "MDOF/s", "cores": cb["cores"], "kind": cb["kind"], "sample": cb["sample"]},
             "e2e": {"value": v, "unit": "MDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -231,6 +245,37 @@ def batched_leg(nrhs):
         out[f"batched_{prec}"] = {"value": nrhs * m.n_dof / t / 1e6, "unit": "MDOF/s", "seconds": t, "converged": ok,
                                   "iterations_max": max(r.iterations for r in res)}
     out["batched_mixed_over_plain_sequential"] = out["batched_mixed"]["value"] / out["plain_fp64_sequential"]["value"]
+    S.close()
+    return out
+
+
+def large_leg():
+    """The capacity workload: the gyroid sheet lattice 384x384x192 (85.8 M DOF, titanium, bottom
+    face held, 5 MPa on the top face), one solve per form after a warm-up, f and u resident in HBM;
+    CUDA-event time on the solver's stream."""
+    import torch
+    import psfea
+    from psfea import workloads as W
+    m = W.gyroid()
+    S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.Stream(device=dev)
+    S.set_stream(stream.cuda_stream)
+    f_dev = torch.from_numpy(m.f).to(dev)
+    u_dev = torch.zeros(m.n_dof, dtype=torch.float64, device=dev)
+    out = {"workload": "gyroid 384x384x192 (period 24, |g| < 0.3), bottom held, 5 MPa top, rtol 1e-8", "n_dof": m.n_dof,
+           "device_bytes": S.device_bytes}
+    for prec in ("fp64", "mixed"):
+        S.solve_dev(f_dev.data_ptr(), u_dev.data_ptr(), tol=TOL, max_iter=MAX_ITER, precision=prec)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        r = S.solve_dev(f_dev.data_ptr(), u_dev.data_ptr(), tol=TOL, max_iter=MAX_ITER, precision=prec)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[prec] = {"value": m.n_dof / (ms / 1e3) / 1e6, "unit": "MDOF/s", "ms": ms, "iterations": r.iterations, "converged": r.converged}
+    S.set_stream(0)
     S.close()
     return out
 
@@ -280,15 +325,19 @@ def solve_only(args):
     import torch
     import psfea
     from psfea import workloads as W
-    m = W.l_bracket() if args.solve_only == "l_bracket" else W.simp(nrhs=1)
+    m = {"l_bracket": W.l_bracket, "simp": lambda: W.simp(nrhs=1), "gyroid": W.gyroid}[args.solve_only]()
     f = m.f if m.f.ndim == 1 else m.f[0]
+    t0 = time.perf_counter()
     S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    build_s = time.perf_counter() - t0
     S.solve(f, tol=TOL, max_iter=MAX_ITER, precision=args.precision)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     r = S.solve(f, tol=TOL, max_iter=MAX_ITER, precision=args.precision)
-    print(json.dumps({"workload": args.solve_only, "precision": args.precision, "iterations": r.iterations, "residual": r.residual,
-                      "seconds": time.perf_counter() - t0, "kernels": r.kernels}), flush=True)
+    sec = time.perf_counter() - t0
+    print(json.dumps({"workload": args.solve_only, "n_dof": m.n_dof, "precision": args.precision, "iterations": r.iterations,
+                      "residual": r.residual, "converged": r.converged, "seconds": sec, "MDOF_per_s": m.n_dof / sec / 1e6,
+                      "build_seconds": build_s, "device_bytes": S.device_bytes, "kernels": r.kernels}), flush=True)
 
 
 def main():
@@ -379,6 +428,7 @@ def main():
     # the multi-RHS and serving workloads, on one GPU (rank 0 of a replica run skips them)
     batched = batched_leg(args.batch_rhs) if args.batch_rhs > 0 and world == 1 else None
     serving = serving_leg(args.serve_requests) if args.serve_requests > 0 and world == 1 else None
+    large = large_leg() if args.large and world == 1 else None
     cb = None
     if world == 1 and not args.no_cpu_baseline:
         try:
@@ -390,9 +440,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "MDOF/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": tmx_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 Krylov + f32 V-cycle on f16-scaled element matrices", "data": "synthetic",
-        "config": {"workload": "l_bracket 256x128x128 voxels (0.5 mm), 64 y-holes, y=0 held, 500 N tip patch, rtol 1e-8",
-                   "n_dof": n, "free_dof": int(S.level_info(0)["freeDof"]), "levels": S.n_levels,
-                   "parallelism": f"replicas x{world}", "l2": "inputs > L2 (126 MB): x/r/d/1/diag at 51 MB each per level-0 vector"},
+        "config": bench_config(m, world, S.n_levels, int(S.level_info(0)["freeDof"])),
         "latency_ms": {"p50": float(np.percentile(permx, 50)), "p99": float(np.percentile(permx, 99)),
                        "plain_fp64_p50": float(np.percentile(per64, 50))},
         "iterations": {"mixed": itmx, "plain_fp64": it64},
@@ -407,6 +455,7 @@ def main():
                      "algorithmic_bytes": alg_bytes, "peak_kind": peak_kind, "fp64_apply_ms": ms_apply64},
         "batched": batched,
         "serving": serving,
+        "large": large,
         "cpu_baseline": cb,
         "gpu_launches": int(kmx),
         "clocks": clk.summary(),

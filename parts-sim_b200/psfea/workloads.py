@@ -258,11 +258,13 @@ def gyroid(nx=384, ny=384, nz=192, period=24, thickness=0.3, pressure=5e6, h=1e-
     y = t(ny)[None, :, None]
     z = t(nz)[:, None, None]
     val = np.sin(x) * np.cos(y) + np.sin(y) * np.cos(z) + np.sin(z) * np.cos(x)
+    from . import prune_floating as _prune  # the library's breadth-first search (label propagation
+    #                                          would need as many sweeps as the sheet is long)
     density = (np.abs(val) < thickness).astype(np.float32).ravel()
     NX, NY, NZ = nx + 1, ny + 1, nz + 1
     bc = np.zeros((NZ, NY, NX, 3), np.uint8)
     bc[0] = 1
-    density, removed = prune_floating((nx, ny, nz), density, bc.ravel())
+    density, removed = _prune((nx, ny, nz), density, bc.reshape(-1, 3).max(axis=1))
     f, nface = _face_load((nx, ny, nz), density, 2, 1, (0.0, 0.0, -pressure * h * h))
     return Model("gyroid", (nx, ny, nz), density, bc.ravel(), f, nu, E, h, 1100, {"removed": removed, "loaded_faces": nface})
 
