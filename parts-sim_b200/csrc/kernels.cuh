@@ -346,7 +346,7 @@ template <class T, int MODE> __host__ __device__ constexpr size_t tileOffI() { r
 template <class T, int MODE> __host__ __device__ constexpr size_t tileOffM() { return tileOffI<T, MODE>() + (tileHasD(MODE) ? align128(tileBytesT<float>()) : 0); }
 template <class T, int MODE> __host__ __device__ constexpr size_t tileOffB() { return tileOffM<T, MODE>() + (tileInnerBoundary<T>() ? align128(TILE_NODES) : 0); }
 template <class T, int MODE> __host__ __device__ constexpr size_t tileOffBar() {
-    return tileOffB<T, MODE>() + (tileInnerBoundary<T>() ? align128(2 * TILE_NODES + 4 * 8) : 0);
+    return tileOffB<T, MODE>() + (tileInnerBoundary<T>() ? align128(2 * TILE_NODES + 4 * 16) : 0);  // list, warp counts, chunk counter
 }
 template <class T, int MODE> __host__ __device__ constexpr size_t tileSmemBytes() { return tileOffBar<T, MODE>() + 16; }
 // bytes each staging barrier expects

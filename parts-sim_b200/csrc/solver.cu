@@ -360,91 +360,105 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS
             }
         }
     }
-    // the column's node masks (padding nodes i >= NX hold 7: inactive, all held) and, for the
-    // smoother, its 1/diag, meanwhile
+    // the column's node masks (padding nodes i >= NX hold 7: inactive, all held) meanwhile
     const int i = i0 + cx, j = j0 + cy;
     const bool col = i < L.PX && j < L.NY;
     uint8_t mk[TZ];
     bool anyUniform = false;
+    unsigned bmask = 0;  // the column's boundary nodes (active, not uniform)
 #pragma unroll
     for (int z = 0; z < TZ; z++) {
         const int k = k0 + z;
         mk[z] = (col && k < L.NZ) ? __ldg(L.nmask + i + (long long)L.PX * j + PXY * k) : uint8_t(0);
         if (tileInnerBoundary<T>()) ms[(z * TY + cy) * TX + cx] = mk[z];
         anyUniform = anyUniform || (mk[z] & NM_UNIFORM);
+        if ((mk[z] & NM_ACTIVE) && !(mk[z] & NM_UNIFORM)) bmask |= 1u << z;
     }
-    __syncthreads();  // barriers initialised; masks in place
-    bool staged = __syncthreads_and(mbarWait(bar, TILE_WAIT_POLLS));
+    int total = 0;
+    if constexpr (tileInnerBoundary<T>()) {
+        // the boundary nodes compacted in a fixed order (thread order, then z) while the copies land
+        const int cnt = __popc(bmask);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (cx >= o) incl += v;
+        }
+        if (cx == 31) wsum[cy] = incl;
+        if (tid == 0) wsum[TILE_THREADS / 32] = 0;  // the counter of handed-out boundary chunks
+        __syncthreads();
+        int off = incl - cnt;
+#pragma unroll
+        for (int w = 0; w < TILE_THREADS / 32; w++) {
+            const int c = wsum[w];
+            off += (w < cy) ? c : 0;
+            total += c;
+        }
+        for (unsigned b = bmask; b; b &= b - 1) blist[off++] = uint16_t((tid << 4) | (__ffs(b) - 1));
+    }
+    __syncthreads();  // barriers initialised; masks and the boundary list in place
+    // each warp goes on as soon as its own wait ends; the outcome is combined before the stores
+    bool ok = mbarWait(bar, TILE_WAIT_POLLS);
     double dot = 0.0;
-    if (staged) {
-        // pass 1: the thread's column, all four nodes from one sweep of the planes (uniform nodes)
-        T acc[TZ][3];
-        if (anyUniform) {
-            if constexpr (sizeof(T) == 4) Op::column2(C, xs, cx, cy, acc);
-            else Op::column(C, xs, cx, cy, acc);
+    // pass 1: the thread's column, all four nodes from one sweep of the planes (uniform nodes)
+    T acc[TZ][3];
+    if (ok && anyUniform) {
+        if constexpr (sizeof(T) == 4) Op::column2(C, xs, cx, cy, acc);
+        else Op::column(C, xs, cx, cy, acc);
+    }
+    if (tileHasR(MODE)) ok = ok && mbarWait(bar + 1, TILE_WAIT_POLLS);
+    if (ok) {
+        // epilogue of the column's nodes except the boundary ones
+#pragma unroll
+        for (int z = 0; z < TZ; z++) {
+            if ((bmask >> z) & 1u) continue;
+            T kx[3] = {T(0), T(0), T(0)};
+            if (mk[z] & NM_UNIFORM) {
+                const T s = T(__uint_as_float(vs[vOff(cx, cy, z)]));
+                kx[0] = s * acc[z][0];
+                kx[1] = s * acc[z][1];
+                kx[2] = s * acc[z][2];
+            }
+            tileFinish<T, MODE>(L, io, i0, j0, k0, cx, cy, z, mk[z], kx, is, xs, ys, rs, ds, dot);
         }
-        if (tileHasR(MODE)) staged = __syncthreads_and(mbarWait(bar + 1, TILE_WAIT_POLLS));
-        if (staged) {
-            // epilogue of the column's nodes except the active non-uniform (boundary) ones
-            unsigned bmask = 0;
-#pragma unroll
-            for (int z = 0; z < TZ; z++) {
-                if ((mk[z] & NM_ACTIVE) && !(mk[z] & NM_UNIFORM)) {
-                    bmask |= 1u << z;
-                    continue;
-                }
-                T kx[3] = {T(0), T(0), T(0)};
-                if (mk[z] & NM_UNIFORM) {
-                    const T s = T(__uint_as_float(vs[vOff(cx, cy, z)]));
-                    kx[0] = s * acc[z][0];
-                    kx[1] = s * acc[z][1];
-                    kx[2] = s * acc[z][2];
-                }
-                tileFinish<T, MODE>(L, io, i0, j0, k0, cx, cy, z, mk[z], kx, is, xs, ys, rs, ds, dot);
+    }
+    if constexpr (tileInnerBoundary<T>()) {
+        // pass 2: the listed nodes, one thread each (per-voxel gather)
+        auto node = [&](int q) {
+            const int e = blist[q], bt = e >> 4, bz = e & 15, bx = bt & 31, by = bt >> 5;
+            T own[3] = {T(0), T(0), T(0)};
+            if (DIFF) {
+                const T* xn = xs + xOff(bx, by, bz);
+                own[0] = xn[0]; own[1] = xn[1]; own[2] = xn[2];
             }
-            if constexpr (tileInnerBoundary<T>()) {
-                // deterministic compaction of the boundary nodes: thread order, then z
-                const int cnt = __popc(bmask);
-                int incl = cnt;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (cx >= o) incl += v;
-                }
-                if (cx == 31) wsum[cy] = incl;
-                __syncthreads();
-                int off = incl - cnt, total = 0;
-#pragma unroll
-                for (int w = 0; w < TILE_THREADS / 32; w++) {
-                    const int c = wsum[w];
-                    off += (w < cy) ? c : 0;
-                    total += c;
-                }
-                for (unsigned b = bmask; b; b &= b - 1) blist[off++] = uint16_t((tid << 4) | (__ffs(b) - 1));
-                __syncthreads();
-                // the listed nodes, one thread each, packed into as few warps as possible
-                for (int q = tid; q < total; q += TILE_THREADS) {
-                    const int e = blist[q], bt = e >> 4, bz = e & 15, bx = bt & 31, by = bt >> 5;
-                    T own[3] = {T(0), T(0), T(0)};
-                    if (DIFF) {
-                        const T* xn = xs + xOff(bx, by, bz);
-                        own[0] = xn[0]; own[1] = xn[1]; own[2] = xn[2];
-                    }
-                    T a[3];
-                    Op::general(L, C, xs, vs, bx, by, bz, a, own);
-                    tileFinish<T, MODE>(L, io, i0, j0, k0, bx, by, bz, ms[(bz * TY + by) * TX + bx], a, is, xs, ys, rs, ds, dot);
-                }
-            }
-            // results out
-            fenceAsyncShared();
-            __syncthreads();
-            if (tid == 0) {
-                if (tileHasR(MODE)) tmaStore3d(&maps.y, rs, 3 * i0, j0, k0);
-                else tmaStore3d(&maps.y, ys, 3 * i0, j0, k0);
-                if (tileHasD(MODE)) tmaStore3d(&maps.d, ds, 3 * i0, j0, k0);
-                tmaStoreCommitWait();
+            T a[3];
+            Op::general(L, C, xs, vs, bx, by, bz, a, own);
+            tileFinish<T, MODE>(L, io, i0, j0, k0, bx, by, bz, ms[(bz * TY + by) * TX + bx], a, is, xs, ys, rs, ds, dot);
+        };
+        if (MODE == TOP_DOT) {
+            // fixed assignment: the thread's share of x.y is summed in a fixed order
+            if (ok)
+                for (int q = tid; q < total; q += TILE_THREADS) node(q);
+        } else {
+            // chunks of 32 listed nodes to whichever warp is free first (a node's result does not
+            // depend on the warp that computes it)
+            for (;;) {
+                int c = 0;
+                if (cx == 0) c = atomicAdd(&wsum[TILE_THREADS / 32], 32);
+                c = __shfl_sync(0xffffffffu, c, 0);
+                if (c >= total) break;
+                if (ok && c + cx < total) node(c + cx);
             }
         }
+    }
+    // results out
+    fenceAsyncShared();
+    const bool staged = __syncthreads_and(ok) != 0;
+    if (staged && tid == 0) {
+        if (tileHasR(MODE)) tmaStore3d(&maps.y, rs, 3 * i0, j0, k0);
+        else tmaStore3d(&maps.y, ys, 3 * i0, j0, k0);
+        if (tileHasD(MODE)) tmaStore3d(&maps.d, ds, 3 * i0, j0, k0);
+        tmaStoreCommitWait();
     }
     if (!staged && tid == 0) {
         atomicExch(&st->err, ST_ERR_STAGING);
