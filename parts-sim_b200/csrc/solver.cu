@@ -1405,7 +1405,6 @@ void SharedModel::adopt(Hierarchy&& h) {
         };
         set(dev::k_tile<double, dev::TOP_APPLY, false, false>, dev::tileSmemBytes<double, dev::TOP_APPLY>());
         set(dev::k_tile<double, dev::TOP_DOT, false, false>, dev::tileSmemBytes<double, dev::TOP_DOT>());
-        set(dev::k_tile<float, dev::TOP_DOT, false, true>, dev::tileSmemBytes<float, dev::TOP_DOT>());
         set(dev::k_tile<float, dev::TOP_CHEB, false, false>, dev::tileSmemBytes<float, dev::TOP_CHEB>());
         set(dev::k_tile<float, dev::TOP_CHEB, true, false>, dev::tileSmemBytes<float, dev::TOP_CHEB>());
         set(dev::k_tile<float, dev::TOP_CHEB, true, true>, dev::tileSmemBytes<float, dev::TOP_CHEB>());
