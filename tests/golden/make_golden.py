@@ -6,7 +6,8 @@ stores inputs and outputs as compressed .npz files. Run from the repository root
 
     make -C oracle && python tests/golden/make_golden.py
 
-The fixtures are committed; the tests read them, never the reference itself.
+The fixtures are committed; the tests read them, never the reference itself. Names given on the
+command line limit the run to those fixtures (``element``, ``prune`` or a model name).
 """
 import os
 import sys
@@ -88,10 +89,23 @@ def prune_fixture():
 if __name__ == "__main__":
     if not oracle.available("reference"):
         sys.exit("oracle/_ref/libpsref.so is missing: run `make -C oracle` where the reference sources are present")
-    element_fixture()
-    prune_fixture()
-    model_fixture("cantilever_32x8x8", W.cantilever(32, 8, 8, coarsest_max_dof=1100))
-    model_fixture("cantilever_64x16x16", W.cantilever())
-    model_fixture("lbracket_32x16x16", W.l_bracket(32, 16, 16, holes=3))
-    model_fixture("simp_16x8x8", W.simp(16, 8, 8, nrhs=1))
-    model_fixture("lbracket_24x12x12_loose", W.l_bracket(24, 12, 12, holes=2), tol=1e-6)
+    models = {
+        "cantilever_32x8x8": lambda: W.cantilever(32, 8, 8, coarsest_max_dof=1100),
+        "cantilever_64x16x16": W.cantilever,
+        "lbracket_32x16x16": lambda: W.l_bracket(32, 16, 16, holes=3),
+        "simp_16x8x8": lambda: W.simp(16, 8, 8, nrhs=1),
+        "lbracket_24x12x12_loose": lambda: (W.l_bracket(24, 12, 12, holes=2), 1e-6),
+        # the lattice and the serving-stream shapes, small
+        "gyroid_48x48x24": lambda: W.gyroid(48, 48, 24),
+        "box_request_20_28": lambda: W.box_with_voids(W.Rng(11), lo=20, hi=28),
+    }
+    want = sys.argv[1:] or ["element", "prune"] + list(models)
+    if "element" in want:
+        element_fixture()
+    if "prune" in want:
+        prune_fixture()
+    for name, make in models.items():
+        if name in want:
+            m = make()
+            m, tol = m if isinstance(m, tuple) else (m, 1e-8)
+            model_fixture(name, m, tol=tol)

@@ -10,7 +10,8 @@ import psfea
 from conftest import ROOT, golden
 from psfea import workloads as W
 
-MODELS = ["cantilever_32x8x8", "cantilever_64x16x16", "lbracket_32x16x16", "simp_16x8x8", "lbracket_24x12x12_loose"]
+MODELS = ["cantilever_32x8x8", "cantilever_64x16x16", "lbracket_32x16x16", "simp_16x8x8", "lbracket_24x12x12_loose", "gyroid_48x48x24",
+          "box_request_20_28"]
 
 
 def declared_symbols():
