@@ -69,6 +69,8 @@ def parse():
                     help="build the model and launch only this level-0 operator kernel --reps times (a small, fixed "
                          "launch sequence for profilers); prints its mean CUDA-event time")
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--kernel-workload", choices=["l_bracket", "simp", "gyroid"], default="l_bracket",
+                    help="the model of --kernel-only")
     ap.add_argument("--solve-only", choices=["l_bracket", "simp", "gyroid"], default=None,
                     help="build the model, run one warm-up solve and one solve of --precision (a fixed launch "
                          "sequence for profilers); prints its time and iterations")
@@ -314,11 +316,11 @@ def kernel_only(args):
     import torch
     import psfea
     from psfea import workloads as W
-    m = W.l_bracket()
+    m = {"l_bracket": W.l_bracket, "simp": lambda: W.simp(nrhs=1), "gyroid": W.gyroid}[args.kernel_workload]()
     S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
     ms = S.time_kernel(0 if args.kernel_only == "cheb32" else 1, args.reps)
     torch.cuda.synchronize()
-    print(json.dumps({"kernel": args.kernel_only, "reps": args.reps, "ms": ms}), flush=True)
+    print(json.dumps({"kernel": args.kernel_only, "workload": args.kernel_workload, "reps": args.reps, "ms": ms}), flush=True)
 
 
 def solve_only(args):

@@ -301,7 +301,10 @@ namespace dev {
 constexpr int TX = 32, TY = 8, TZ = 4, TILE_THREADS = TX * TY, TILE_NODES = TX * TY * TZ;
 constexpr int HY = TY + 2, HZ = TZ + 2;          // x halo rows and planes
 constexpr int XLEFT = 4;                         // halo box starts XLEFT nodes left of the tile
-constexpr int PROW = 112;                        // halo box row: nodes i0-4 .. i0+33, 112 values
+// halo box row: nodes i0-4 .. i0+33 (111 values) padded to 116, so that the plane stride of the
+// shared-memory halo (10 rows, 1160 words) is not a multiple of the 32 banks: the four planes of a
+// column then sit in different banks when the lanes of a warp take the nodes of a few columns
+constexpr int PROW = 116;
 constexpr int VX = TX + 1, VY = TY + 1, VZ = TZ + 1;  // voxel words needed per axis
 constexpr int WROW = 36;                         // voxel box row: words i0-4 .. i0+31 (144 bytes)
 constexpr int TROW = 3 * TX;                     // tile box row (r, d, 1/diag, y): 96 values

@@ -1482,7 +1482,7 @@ void SharedModel::uploadLevel(int l) {
         // lanes per node on the smallest ones
         int64_t minNodes = 400000;
         if (const char* e = std::getenv("PSFEA_TILE_MIN_NODES")) minNodes = std::atoll(e);
-        // (and grids no smaller than the staging boxes of 112 x 10 x 6 values and 40 x 9 x 5 words)
+        // (and grids no smaller than the staging boxes of 116 x 10 x 6 values and 36 x 9 x 5 words)
         D.useTiles = h.nNodes >= minNodes && h.NY >= dev::HY && h.NZ >= dev::HZ && 3 * PX >= dev::PROW && px >= dev::WROW;
         int64_t max8 = 30000;
         if (const char* e = std::getenv("PSFEA_OP8_MAX_NODES")) max8 = std::atoll(e);
