@@ -412,12 +412,13 @@ __device__ __forceinline__ int vOff(int vx, int vy, int vz) { return (vz * VY + 
 template <class T, bool OWN16, bool DIFF>
 struct TileOp {
     // adds voxel V's rows at a tile node to acc (V = di + 2 dj + 4 dk: the voxel at offset
-    // (di - 1, dj - 1, dk - 1) from the node); A and B: the node's 3 x 3 neighbourhood in planes
-    // oz = dk - 1 and oz = dk (values already relative to the node's own value when DIFF). V is a
-    // compile-time constant, so every Kb coefficient is a constant-bank operand.
+    // (di - 1, dj - 1, dk - 1) from the node); A and B: rows oy = dj - 1 and dj (x offsets -1..1) of
+    // the node's neighbourhood in planes oz = dk - 1 and dk (values already relative to the node's
+    // own value when DIFF). V is a compile-time constant, so every Kb coefficient is a constant-bank
+    // operand.
     template <int V>
     static __device__ __forceinline__ void voxel(const LevelView& L, const Coefs<T>& C, const uint32_t* vs, int cx, int cy, int cz,
-                                                 const T (&A)[9][3], const T (&B)[9][3], T acc[3]) {
+                                                 const T (&A)[2][3][3], const T (&B)[2][3][3], T acc[3]) {
         constexpr int di = V & 1, dj = (V >> 1) & 1, dk = V >> 2;
         constexpr int a = cornerOf(1 - di, 1 - dj, 1 - dk);
         const uint32_t w = vs[vOff(cx + di, cy + dj, cz + dk)];
@@ -426,10 +427,8 @@ struct TileOp {
 #pragma unroll
         for (int b = 0; b < 8; b++) {
             const int bx = (b == 1 || b == 2 || b == 5 || b == 6), by = (b == 2 || b == 3 || b == 6 || b == 7), bz = b >> 2;
-            const int e = (dj + by) * 3 + (di + bx);
-            xe[3 * b] = bz ? B[e][0] : A[e][0];
-            xe[3 * b + 1] = bz ? B[e][1] : A[e][1];
-            xe[3 * b + 2] = bz ? B[e][2] : A[e][2];
+#pragma unroll
+            for (int c = 0; c < 3; c++) xe[3 * b + c] = bz ? B[by][di + bx][c] : A[by][di + bx][c];
         }
         if (!(w & OWN_BIT)) {
             T t[3];
@@ -455,33 +454,41 @@ struct TileOp {
                 }
         }
     }
-    // one plane (oz) of the node's 3 x 3 neighbourhood from shared memory, less own (DIFF)
-    static __device__ __forceinline__ void plane(const T* xs, int cx, int cy, int cz, int oz, const T own[3], T (&P)[9][3]) {
+    // rows oy and oy + 1 (x offsets -1..1) of plane oz around tile node (cx, cy, cz), less own (DIFF)
+    static __device__ __forceinline__ void rowPair(const T* xs, int cx, int cy, int cz, int oy, int oz, const T own[3], T (&R)[2][3][3]) {
 #pragma unroll
-        for (int e = 0; e < 9; e++) {
-            const T* xp = xs + xOff(cx + e % 3 - 1, cy + e / 3 - 1, cz + oz);
-            P[e][0] = xp[0] - own[0];
-            P[e][1] = xp[1] - own[1];
-            P[e][2] = xp[2] - own[2];
-        }
+        for (int yy = 0; yy < 2; yy++)
+#pragma unroll
+            for (int e = 0; e < 3; e++) {
+                const T* xp = xs + xOff(cx + e - 1, cy + oy + yy, cz + oz);
+                R[yy][e][0] = xp[0] - own[0];
+                R[yy][e][1] = xp[1] - own[1];
+                R[yy][e][2] = xp[2] - own[2];
+            }
     }
-    // K x at tile node (cx, cy, cz) by the per-voxel gather over its 8 voxels; the 27 neighbour
-    // values are read from shared memory once, a plane at a time (81 loads instead of 8 x 24)
+    // K x at tile node (cx, cy, cz) by the per-voxel gather over its 8 voxels, two at a time: each
+    // pair of voxels sharing (dj, dk) reads the two row pairs it needs (36 values live, not the 81
+    // of the whole neighbourhood: fewer registers outweigh the extra shared-memory loads)
     static __device__ __forceinline__ void general(const LevelView& L, const Coefs<T>& C, const T* xs, const uint32_t* vs, int cx, int cy,
                                                    int cz, T acc[3], const T own[3]) {
         acc[0] = acc[1] = acc[2] = T(0);
-        T P0[9][3], P1[9][3];
-        plane(xs, cx, cy, cz, -1, own, P0);
-        plane(xs, cx, cy, cz, 0, own, P1);
-        voxel<0>(L, C, vs, cx, cy, cz, P0, P1, acc);
-        voxel<1>(L, C, vs, cx, cy, cz, P0, P1, acc);
-        voxel<2>(L, C, vs, cx, cy, cz, P0, P1, acc);
-        voxel<3>(L, C, vs, cx, cy, cz, P0, P1, acc);
-        plane(xs, cx, cy, cz, 1, own, P0);
-        voxel<4>(L, C, vs, cx, cy, cz, P1, P0, acc);
-        voxel<5>(L, C, vs, cx, cy, cz, P1, P0, acc);
-        voxel<6>(L, C, vs, cx, cy, cz, P1, P0, acc);
-        voxel<7>(L, C, vs, cx, cy, cz, P1, P0, acc);
+        T A[2][3][3], B[2][3][3];
+        rowPair(xs, cx, cy, cz, -1, -1, own, A);
+        rowPair(xs, cx, cy, cz, -1, 0, own, B);
+        voxel<0>(L, C, vs, cx, cy, cz, A, B, acc);
+        voxel<1>(L, C, vs, cx, cy, cz, A, B, acc);
+        rowPair(xs, cx, cy, cz, 0, -1, own, A);
+        rowPair(xs, cx, cy, cz, 0, 0, own, B);
+        voxel<2>(L, C, vs, cx, cy, cz, A, B, acc);
+        voxel<3>(L, C, vs, cx, cy, cz, A, B, acc);
+        rowPair(xs, cx, cy, cz, -1, 0, own, A);
+        rowPair(xs, cx, cy, cz, -1, 1, own, B);
+        voxel<4>(L, C, vs, cx, cy, cz, A, B, acc);
+        voxel<5>(L, C, vs, cx, cy, cz, A, B, acc);
+        rowPair(xs, cx, cy, cz, 0, 0, own, A);
+        rowPair(xs, cx, cy, cz, 0, 1, own, B);
+        voxel<6>(L, C, vs, cx, cy, cz, A, B, acc);
+        voxel<7>(L, C, vs, cx, cy, cz, A, B, acc);
     }
 
     // unscaled stencil sums of the thread's whole column (cz = 0..TZ-1) at once: every plane of the
