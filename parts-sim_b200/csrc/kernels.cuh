@@ -342,16 +342,15 @@ template <class T> __host__ __device__ constexpr size_t tileOffY() { return tile
 template <class T, int MODE> __host__ __device__ constexpr size_t tileOffD() {
     return tileOffY<T>() + align128(tileHasR(MODE) ? tileBytesT<float>() : tileBytesT<T>());
 }
-// 32-bit tiles compute their boundary nodes themselves (a compacted list in shared memory);
-// 64-bit tiles leave them to the boundary-node kernel
-template <class T> __host__ __device__ constexpr bool tileInnerBoundary() { return sizeof(T) == 4; }
+// INNER: the tile computes its boundary nodes itself (a compacted list in shared memory); else the
+// boundary-node kernel does
 template <class T, int MODE> __host__ __device__ constexpr size_t tileOffI() { return tileOffD<T, MODE>() + (tileHasD(MODE) ? align128(tileBytesT<float>()) : 0); }
 template <class T, int MODE> __host__ __device__ constexpr size_t tileOffM() { return tileOffI<T, MODE>() + (tileHasD(MODE) ? align128(tileBytesT<float>()) : 0); }
-template <class T, int MODE> __host__ __device__ constexpr size_t tileOffB() { return tileOffM<T, MODE>() + (tileInnerBoundary<T>() ? align128(TILE_NODES) : 0); }
-template <class T, int MODE> __host__ __device__ constexpr size_t tileOffBar() {
-    return tileOffB<T, MODE>() + (tileInnerBoundary<T>() ? align128(2 * TILE_NODES + 4 * 16) : 0);  // list, warp counts, chunk counter
+template <class T, int MODE, bool INNER> __host__ __device__ constexpr size_t tileOffB() { return tileOffM<T, MODE>() + (INNER ? align128(TILE_NODES) : 0); }
+template <class T, int MODE, bool INNER> __host__ __device__ constexpr size_t tileOffBar() {
+    return tileOffB<T, MODE, INNER>() + (INNER ? align128(2 * TILE_NODES + 4 * 16) : 0);  // list, warp counts, chunk counter
 }
-template <class T, int MODE> __host__ __device__ constexpr size_t tileSmemBytes() { return tileOffBar<T, MODE>() + 16; }
+template <class T, int MODE, bool INNER> __host__ __device__ constexpr size_t tileSmemBytes() { return tileOffBar<T, MODE, INNER>() + 16; }
 // bytes each staging barrier expects
 template <class T> __host__ __device__ constexpr unsigned tileStage0Bytes() { return unsigned(tileBytesX<T>() + tileBytesW()); }
 template <int MODE> __host__ __device__ constexpr unsigned tileStage1Bytes() {

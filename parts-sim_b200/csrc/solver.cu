@@ -315,7 +315,7 @@ __device__ __forceinline__ void tileFinish(const LevelView& L, const TileIO<T>& 
 template <class T> struct CoefsFor { using type = Coefs<T>; };
 template <> struct CoefsFor<float> { using type = Coefs32; };
 
-template <class T, int MODE, bool OWN16, bool DIFF>
+template <class T, int MODE, bool OWN16, bool DIFF, bool INNER = (sizeof(T) == 4)>
 __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS64 : PSFEA_TILE_CTAS32)
     k_tile(LevelView L, typename CoefsFor<T>::type C, const uint32_t* __restrict__ tiles, const __grid_constant__ TileMaps maps, TileIO<T> io, SolveState* st,
            double* partials, unsigned* ticket, Ctl ctl) {
@@ -336,9 +336,9 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS
     float* ds = reinterpret_cast<float*>(smem + tileOffD<T, MODE>());
     const float* is = reinterpret_cast<const float*>(smem + tileOffI<T, MODE>());
     uint8_t* ms = smem + tileOffM<T, MODE>();
-    uint16_t* blist = reinterpret_cast<uint16_t*>(smem + tileOffB<T, MODE>());
+    uint16_t* blist = reinterpret_cast<uint16_t*>(smem + tileOffB<T, MODE, INNER>());
     int* wsum = reinterpret_cast<int*>(blist + TILE_NODES);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + tileOffBar<T, MODE>());  // [0] x and words, [1] r and d
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + tileOffBar<T, MODE, INNER>());  // [0] x and words, [1] r and d
     const uint32_t tw = tiles[blockIdx.x];
     const int i0 = int(tw & 2047u) * TX, j0 = int((tw >> 11) & 2047u) * TY, k0 = int(tw >> 22) * TZ;
     const int tid = threadIdx.x, cx = tid & 31, cy = tid >> 5;
@@ -370,12 +370,12 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS
     for (int z = 0; z < TZ; z++) {
         const int k = k0 + z;
         mk[z] = (col && k < L.NZ) ? __ldg(L.nmask + i + (long long)L.PX * j + PXY * k) : uint8_t(0);
-        if (tileInnerBoundary<T>()) ms[(z * TY + cy) * TX + cx] = mk[z];
+        if (INNER) ms[(z * TY + cy) * TX + cx] = mk[z];
         anyUniform = anyUniform || (mk[z] & NM_UNIFORM);
         if ((mk[z] & NM_ACTIVE) && !(mk[z] & NM_UNIFORM)) bmask |= 1u << z;
     }
     int total = 0;
-    if constexpr (tileInnerBoundary<T>()) {
+    if constexpr (INNER) {
         // the boundary nodes compacted in a fixed order (thread order, then z) while the copies land
         const int cnt = __popc(bmask);
         int incl = cnt;
@@ -422,38 +422,44 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS
             tileFinish<T, MODE>(L, io, i0, j0, k0, cx, cy, z, mk[z], kx, is, xs, ys, rs, ds, dot);
         }
     }
-    if constexpr (tileInnerBoundary<T>()) {
-        // pass 2: the listed nodes, one thread each (per-voxel gather)
-        auto node = [&](int q) {
-            const int e = blist[q], bt = e >> 4, bz = e & 15, bx = bt & 31, by = bt >> 5;
-            T own[3] = {T(0), T(0), T(0)};
-            if (DIFF) {
-                const T* xn = xs + xOff(bx, by, bz);
-                own[0] = xn[0]; own[1] = xn[1]; own[2] = xn[2];
-            }
-            T a[3];
-            Op::general(L, C, xs, vs, bx, by, bz, a, own);
-            tileFinish<T, MODE>(L, io, i0, j0, k0, bx, by, bz, ms[(bz * TY + by) * TX + bx], a, is, xs, ys, rs, ds, dot);
-        };
-        if (MODE == TOP_DOT) {
-            // fixed assignment: the thread's share of x.y is summed in a fixed order
-            if (ok)
-                for (int q = tid; q < total; q += TILE_THREADS) node(q);
-        } else {
-            // chunks of 32 listed nodes to whichever warp is free first (a node's result does not
-            // depend on the warp that computes it)
-            for (;;) {
-                int c = 0;
-                if (cx == 0) c = atomicAdd(&wsum[TILE_THREADS / 32], 32);
-                c = __shfl_sync(0xffffffffu, c, 0);
-                if (c >= total) break;
-                if (ok && c + cx < total) node(c + cx);
+    if constexpr (INNER) {
+        // pass 2: the listed nodes in chunks of 32 to whichever warp is free first, one thread a node
+        // (per-voxel gather); a node's result does not depend on the warp that computes it, and its
+        // share of x.y is added below by the thread owning its column, in a fixed order
+        for (;;) {
+            int c = 0;
+            if (cx == 0) c = atomicAdd(&wsum[TILE_THREADS / 32], 32);
+            c = __shfl_sync(0xffffffffu, c, 0);
+            if (c >= total) break;
+            const int q = c + cx;
+            if (ok && q < total) {
+                const int e = blist[q], bt = e >> 4, bz = e & 15, bx = bt & 31, by = bt >> 5;
+                T own[3] = {T(0), T(0), T(0)};
+                if (DIFF) {
+                    const T* xn = xs + xOff(bx, by, bz);
+                    own[0] = xn[0]; own[1] = xn[1]; own[2] = xn[2];
+                }
+                T a[3];
+                Op::general(L, C, xs, vs, bx, by, bz, a, own);
+                double unused = 0.0;
+                tileFinish<T, MODE>(L, io, i0, j0, k0, bx, by, bz, ms[(bz * TY + by) * TX + bx], a, is, xs, ys, rs, ds, unused);
             }
         }
     }
     // results out
     fenceAsyncShared();
     const bool staged = __syncthreads_and(ok) != 0;
+    if (INNER && MODE == TOP_DOT && staged) {
+        // the column's boundary nodes' share of x.y, from the y tile
+#pragma unroll
+        for (int z = 0; z < TZ; z++) {
+            if (!((bmask >> z) & 1u)) continue;
+            const T* xn = xs + xOff(cx, cy, z);
+            const T* yn = ys + (z * TY + cy) * TROW + 3 * cx;
+#pragma unroll
+            for (int c = 0; c < 3; c++) dot += double(xn[c]) * double(yn[c]);
+        }
+    }
     if (staged && tid == 0) {
         if (tileHasR(MODE)) tmaStore3d(&maps.y, rs, 3 * i0, j0, k0);
         else tmaStore3d(&maps.y, ys, 3 * i0, j0, k0);
@@ -1326,6 +1332,7 @@ struct DevLevel {
     int nTiles = 0;
     DevMem blist;      // tiled levels: the boundary nodes (pitched indices, increasing)
     int nBnd = 0;
+    bool inner64 = false;  // 64-bit tiles compute their boundary nodes themselves (else k_bnd does)
     bool useTiles = false;  // tiled kernel (large levels) or one thread per node (small ones)
     bool use8 = false;      // eight lanes per node (the smallest levels)
     float cf0 = 0, cf1 = 0, cf2 = 0, omega = 0.5f;
@@ -1403,15 +1410,17 @@ void SharedModel::adopt(Hierarchy&& h) {
         auto set = [](auto kernel, size_t bytes) {
             check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)), "attr");
         };
-        set(dev::k_tile<double, dev::TOP_APPLY, false, false>, dev::tileSmemBytes<double, dev::TOP_APPLY>());
-        set(dev::k_tile<double, dev::TOP_DOT, false, false>, dev::tileSmemBytes<double, dev::TOP_DOT>());
-        set(dev::k_tile<float, dev::TOP_CHEB, false, false>, dev::tileSmemBytes<float, dev::TOP_CHEB>());
-        set(dev::k_tile<float, dev::TOP_CHEB, true, false>, dev::tileSmemBytes<float, dev::TOP_CHEB>());
-        set(dev::k_tile<float, dev::TOP_CHEB, true, true>, dev::tileSmemBytes<float, dev::TOP_CHEB>());
-        set(dev::k_tile<float, dev::TOP_RESID, false, false>, dev::tileSmemBytes<float, dev::TOP_RESID>());
-        set(dev::k_tile<float, dev::TOP_RESID, true, false>, dev::tileSmemBytes<float, dev::TOP_RESID>());
-        set(dev::k_tile<float, dev::TOP_RESID, true, true>, dev::tileSmemBytes<float, dev::TOP_RESID>());
-        set(dev::k_tile<float, dev::TOP_DOT, false, true>, dev::tileSmemBytes<float, dev::TOP_DOT>());
+        set(dev::k_tile<double, dev::TOP_APPLY, false, false>, dev::tileSmemBytes<double, dev::TOP_APPLY, false>());
+        set(dev::k_tile<double, dev::TOP_DOT, false, false>, dev::tileSmemBytes<double, dev::TOP_DOT, false>());
+        set(dev::k_tile<double, dev::TOP_APPLY, false, false, true>, dev::tileSmemBytes<double, dev::TOP_APPLY, true>());
+        set(dev::k_tile<double, dev::TOP_DOT, false, false, true>, dev::tileSmemBytes<double, dev::TOP_DOT, true>());
+        set(dev::k_tile<float, dev::TOP_CHEB, false, false>, dev::tileSmemBytes<float, dev::TOP_CHEB, true>());
+        set(dev::k_tile<float, dev::TOP_CHEB, true, false>, dev::tileSmemBytes<float, dev::TOP_CHEB, true>());
+        set(dev::k_tile<float, dev::TOP_CHEB, true, true>, dev::tileSmemBytes<float, dev::TOP_CHEB, true>());
+        set(dev::k_tile<float, dev::TOP_RESID, false, false>, dev::tileSmemBytes<float, dev::TOP_RESID, true>());
+        set(dev::k_tile<float, dev::TOP_RESID, true, false>, dev::tileSmemBytes<float, dev::TOP_RESID, true>());
+        set(dev::k_tile<float, dev::TOP_RESID, true, true>, dev::tileSmemBytes<float, dev::TOP_RESID, true>());
+        set(dev::k_tile<float, dev::TOP_DOT, false, true>, dev::tileSmemBytes<float, dev::TOP_DOT, true>());
     });
     L.resize(H.levels.size());
     for (int l = 0; l < int(H.levels.size()); l++) uploadLevel(l);
@@ -1495,6 +1504,15 @@ void SharedModel::uploadLevel(int l) {
             }
             D.nBnd = int(bl.size());
             upload(D.blist, bl, bytes, ms);
+            // in the tile once boundary nodes are a large share of the level (graded grids, thin
+            // walls); PSFEA_TILE_INNER64: 0 never, 1 always
+            int64_t active = 0;
+            for (uint8_t mk : h.nmask) active += (mk & NM_ACTIVE) ? 1 : 0;
+            D.inner64 = active > 0 && double(bl.size()) >= 0.3 * double(active);
+            if (const char* e = std::getenv("PSFEA_TILE_INNER64")) {
+                const int v = std::atoi(e);
+                if (v == 0 || v == 1) D.inner64 = v == 1;
+            }
         }
     }
     dev::LevelView& v = D.view;
@@ -1726,7 +1744,12 @@ void SolverImpl::op64(int l, const double* xin, double* y, bool raw, dev::Ctl ct
     mp.w = mapOf(D.word.p, MAP_WORDS, false, l);
     mp.y = mapOf(y, MAP_TILE, true, l);
     mp.r = mp.d = mp.inv = mp.y;  // not read by this epilogue
-    launch(dev::k_tile<double, dev::TOP_APPLY, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double, dev::TOP_APPLY>(), stream,
+    if (D.inner64) {
+        launch(dev::k_tile<double, dev::TOP_APPLY, false, false, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double, dev::TOP_APPLY, true>(),
+               stream, D.view, D.c64, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), ctl);
+        return;
+    }
+    launch(dev::k_tile<double, dev::TOP_APPLY, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double, dev::TOP_APPLY, false>(), stream,
            D.view, D.c64, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), ctl);
     if (D.nBnd)
         launch(dev::k_bnd<double, dev::TOP_APPLY, false, false>, nodeGrid(D.nBnd), dev::NODE_THREADS, 0, stream, D.view, D.c64,
@@ -1763,7 +1786,7 @@ void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev
     mp.r = dev::tileHasR(TM) ? mapOf(rr, MAP_TILE, false, l) : mp.y;
     mp.d = dev::tileHasD(TM) ? mapOf(dd, MAP_TILE, false, l) : mp.y;
     mp.inv = dev::tileHasD(TM) ? mapOf(D.invD.p, MAP_TILE, false, l) : mp.y;
-    const size_t sm = dev::tileSmemBytes<float, TM>();
+    const size_t sm = dev::tileSmemBytes<float, TM, true>();
     const uint32_t* tl = D.tiles.as<uint32_t>();
     if (diff) launch(dev::k_tile<float, TM, true, true>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
     else if (o16) launch(dev::k_tile<float, TM, true, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
@@ -1933,15 +1956,19 @@ void SolverImpl::recordPlainIteration(dev::Ctl ctl, bool own16) {
         launch(dev::k_apply_alpha<double, false>, nodeGrid(pn(0)), dev::NODE_THREADS, 0, stream, D.view, D.c64, p.as<double>(), q.as<double>(),
                st(), part(), tick(), ctl);
     } else {
-        dev::TileIO<double> io{0.f, 0.f, 0, D.nBnd ? 1 : 0};
+        dev::TileIO<double> io{0.f, 0.f, 0, (D.nBnd && !D.inner64) ? 1 : 0};
         dev::TileMaps mp;
         mp.x = mapOf(p.p, MAP_HALO, true, 0);
         mp.w = mapOf(D.word.p, MAP_WORDS, false, 0);
         mp.y = mapOf(q.p, MAP_TILE, true, 0);
         mp.r = mp.d = mp.inv = mp.y;
-        launch(dev::k_tile<double, dev::TOP_DOT, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double, dev::TOP_DOT>(), stream,
-               D.view, D.c64, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), ctl);
-        if (D.nBnd)
+        if (D.inner64)
+            launch(dev::k_tile<double, dev::TOP_DOT, false, false, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double, dev::TOP_DOT, true>(),
+                   stream, D.view, D.c64, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), ctl);
+        else
+            launch(dev::k_tile<double, dev::TOP_DOT, false, false>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<double, dev::TOP_DOT, false>(),
+                   stream, D.view, D.c64, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), ctl);
+        if (D.nBnd && !D.inner64)
             launch(dev::k_bnd<double, dev::TOP_DOT, false, false>, nodeGrid(D.nBnd), dev::NODE_THREADS, 0, stream, D.view, D.c64,
                    D.blist.as<int>(), D.nBnd, p.as<double>(), q.as<double>(), nullptr, nullptr, 0.f, 0.f, 0, st(), part(), tick(), ctl);
     }
@@ -1979,7 +2006,7 @@ void SolverImpl::recordMixedIteration(dev::Ctl ctl) {
         mp.w = mapOf(D.word.p, MAP_WORDS, false, 0);
         mp.y = mapOf(q32.p, MAP_TILE, false, 0);
         mp.r = mp.d = mp.inv = mp.y;
-        launch(dev::k_tile<float, dev::TOP_DOT, false, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float, dev::TOP_DOT>(), stream, D.view,
+        launch(dev::k_tile<float, dev::TOP_DOT, false, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float, dev::TOP_DOT, true>(), stream, D.view,
                D.c32, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
     }
     launch(dev::k_mx_update, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, x32.as<float>(), W0.r.as<float>(),
