@@ -38,7 +38,7 @@ BYTES_PER_VOXEL = 4
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of that kernel on this
 # model, from an ncu capture of `bench.py --kernel-only cheb32` (the launch moves the algorithmic
 # bytes plus halo re-reads of partial tiles and the inactive node slots of active tiles)
-TRAFFIC_BYTES_CHEB32 = 216.0e6
+TRAFFIC_BYTES_CHEB32 = 211.9e6
 # iterations of the reference's FP64 MG-PCG on this model to 1e-8, measured with its own solver
 # (oracle/_ref, 8 threads): used to turn a bounded CPU sample into a full-solve time
 REFERENCE_ITERATIONS_L_BRACKET = 1181
