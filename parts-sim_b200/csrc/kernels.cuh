@@ -579,27 +579,6 @@ struct TileOp {
             acc[3][d] = A[1][d].y;
         }
     }
-
-    // s * (assembled stencil . x) at tile node (cx, cy, cz)
-    static __device__ __forceinline__ void stencil(const Coefs<T>& C, const T* xs, int cx, int cy, int cz, float s, T acc[3], const T own[3]) {
-        T a0 = 0, a1 = 0, a2 = 0;
-#pragma unroll
-        for (int m = 0; m < 27; m++) {
-            const int ox = m % 3 - 1, oy = (m / 3) % 3 - 1, oz = m / 9 - 1;
-            if (DIFF && m == 13) continue;
-            const T* xp = xs + xOff(cx + ox, cy + oy, cz + oz);
-            const T x0 = xp[0] - own[0], x1 = xp[1] - own[1], x2 = xp[2] - own[2];
-            a0 += C.S[m * 9 + 0] * x0;
-            a1 += C.S[m * 9 + 4] * x1;
-            a2 += C.S[m * 9 + 8] * x2;
-            if (ox && oy) { a0 += C.S[m * 9 + 1] * x1; a1 += C.S[m * 9 + 3] * x0; }
-            if (ox && oz) { a0 += C.S[m * 9 + 2] * x2; a2 += C.S[m * 9 + 6] * x0; }
-            if (oy && oz) { a1 += C.S[m * 9 + 5] * x2; a2 += C.S[m * 9 + 7] * x1; }
-        }
-        acc[0] = T(s) * a0;
-        acc[1] = T(s) * a1;
-        acc[2] = T(s) * a2;
-    }
 };
 
 }  // namespace dev
