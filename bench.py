@@ -98,6 +98,12 @@ def dist_setup(gpus):
     return rank, world, local, pg
 
 
+def job_rate(world, n_dof, solves, seconds):
+    """whole-job solved MDOF/s of a replica run: every rank solved `solves` models of n_dof DOFs,
+    the slowest rank took `seconds`"""
+    return world * n_dof * solves / seconds / 1e6
+
+
 def reduce_max(pg, value, device=None):
     """max over ranks of a float (the driver's rule: time multi-GPU runs as the slowest rank)."""
     if pg is None:
@@ -199,8 +205,9 @@ def cpu_baseline(m, sample_s, kind_pref=("reference", "port")):
 
 
 def run_reference(args):
-    rank, world, local, pg = dist_setup(args.gpus)
-    if rank != 0:
+    # the reference's CPU solver runs on rank 0 only; the other ranks of a torchrun launch exit
+    # at once (no process group: nothing is exchanged)
+    if int(os.environ.get("RANK", "0")) != 0:
         return
     from psfea import workloads as W
     m = W.l_bracket()
@@ -399,8 +406,8 @@ def main():
     t32, per32, it32, k32, res32 = timed("fp32", 1, 1)
     tmx_max = reduce_max(pg, tmx, dev)
     t64_max = reduce_max(pg, t64, dev)
-    value = world * n * args.steps / (tmx_max / 1e3) / 1e6
-    plain = world * n * args.steps / (t64_max / 1e3) / 1e6
+    value = job_rate(world, n, args.steps, tmx_max / 1e3)
+    plain = job_rate(world, n, args.steps, t64_max / 1e3)
 
     # end to end through the C ABI with host buffers (f up, u down, every step)
     f_host = np.ascontiguousarray(m.f)
@@ -413,7 +420,7 @@ def main():
         e2e_t.append(time.perf_counter() - t0)
         assert r.converged
     e2e_total = reduce_max(pg, sum(e2e_t), dev)
-    e2e_value = world * n * len(e2e_t) / e2e_total / 1e6
+    e2e_value = job_rate(world, n, len(e2e_t), e2e_total)
 
     # roofline of the dominant kernel: the finest level's FP32 Chebyshev operator step
     ms_cheb = S.time_kernel(0, 20)
@@ -448,7 +455,7 @@ def main():
         "iterations": {"mixed": itmx, "plain_fp64": it64},
         "residual": {"mixed": max(resmx), "plain_fp64": max(res64)},
         "plain_fp64": {"value": plain, "unit": "MDOF/s", "ms_per_solve": t64_max / args.steps},
-        "fp32_krylov": {"value": world * n / (t32 / 1e3) / 1e6, "unit": "MDOF/s", "ms_per_solve": t32, "iterations": it32[0],
+        "fp32_krylov": {"value": job_rate(world, n, 1, t32 / 1e3), "unit": "MDOF/s", "ms_per_solve": t32, "iterations": it32[0],
                         "residual": res32[0]},
         "mixed_over_plain": value / plain,
         "e2e": {"value": e2e_value, "unit": "MDOF/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
