@@ -2066,6 +2066,9 @@ void SolverImpl::startIterations() {
     check(cudaMemcpyAsync(state.p, hostState, sizeof s, cudaMemcpyHostToDevice, stream), "state");
     if (fDev != f.p) pitch(fDev, f.as<double>(), 0, true);  // a caller's device vector (dense layout)
     launch(dev::k_mask_copy, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, x0Dev, x.as<double>());
+    // the search direction is only ever written at free DOFs: clear what earlier calls left in it
+    // (apply, reactions, stresses and warm starts use it as staging)
+    check(cudaMemsetAsync(p.p, 0, size_t(pd(0)) * 8, stream), "memset");
     const dev::Ctl none{nullptr, nullptr};
     const dev::Ctl ctl{&st()->done, nullptr};
     op64(0, x.as<double>(), q.as<double>(), false, none);

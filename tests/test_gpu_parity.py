@@ -87,6 +87,28 @@ def test_precondition_close_to_oracle_and_linear():
     assert np.allclose([S.lmax(l) for l in range(S.n_levels - 1)], g["lmax"], rtol=1e-9)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32"])
+def test_solve_after_other_calls_on_the_handle(precision):
+    """Calls made before a solve on the same handle (product, preconditioner, stresses, reactions,
+    a warm-started solve) must leave nothing behind that changes the solve: same iterations and
+    bitwise the same displacements as on a fresh handle."""
+    g = golden("gyroid_48x48x24")
+    fresh = make(g).solve(g["f"], tol=1e-8, max_iter=3000, precision=precision)
+    S = make(g)
+    x = np.random.default_rng(5).standard_normal(S.n_dof) * 1e3
+    S.apply(x)
+    S.apply(x, raw=True)
+    S.precondition(x)
+    E, h = float(g["E"]), float(g["h"])
+    S.stresses(x, E, h)
+    S.reactions(x, g["f"])
+    S.solve(g["f"], tol=1e-3, max_iter=3000, x0=x, precision=precision)
+    r = S.solve(g["f"], tol=1e-8, max_iter=3000, precision=precision)
+    assert r.converged and r.iterations == fresh.iterations
+    assert np.array_equal(r.u, fresh.u)
+    assert rel(r.u, g["u"]) < U_TOL
+
+
 def test_warm_start_zero_load_and_errors():
     g = golden("cantilever_32x8x8")
     S = make(g)
