@@ -151,6 +151,34 @@ def test_bitwise_reproducible():
     assert np.array_equal(a.u, b.u) and a.iterations == b.iterations
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_device_pointer_solve_on_a_caller_stream(precision):
+    """ps_fea_solve_dev with f, x0 and u in the caller's device memory (the reference's dense
+    layout), on the caller's stream: the same iterations and bitwise the same displacements as
+    the host-buffer solve."""
+    import torch
+
+    g = golden("lbracket_32x16x16")
+    S = make(g)
+    host = S.solve(g["f"], tol=1e-8, max_iter=3000, precision=precision)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    S.set_stream(stream.cuda_stream)
+    f = torch.from_numpy(g["f"]).to(dev)
+    u = torch.full_like(f, float("nan"))
+    r = S.solve_dev(f.data_ptr(), u.data_ptr(), tol=1e-8, max_iter=3000, precision=precision)
+    torch.cuda.synchronize()
+    assert r.converged and r.iterations == host.iterations
+    assert np.array_equal(u.cpu().numpy(), host.u)
+    # a warm start from the solution, also in device memory
+    u2 = torch.zeros_like(f)
+    r2 = S.solve_dev(f.data_ptr(), u2.data_ptr(), tol=1e-8, max_iter=3000, precision=precision, x0_ptr=u.data_ptr())
+    torch.cuda.synchronize()
+    assert r2.converged and r2.iterations <= 1
+    assert rel(u2.cpu().numpy(), host.u) < 1e-8
+    S.set_stream(0)
+
+
 def test_solve_batch_matches_single():
     m = W.simp(16, 8, 8, nrhs=3)
     S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc)
