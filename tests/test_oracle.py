@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 import oracle
+import known_answers as KA
 from conftest import golden
 from psfea import workloads as W
 
@@ -84,28 +85,48 @@ def test_apply_and_solve_match_reference(name):
     assert np.abs(R - g["reactions"]).max() <= 1e-6 * max(1.0, np.abs(g["reactions"]).max())
 
 
-def test_cantilever_against_beam_theory():
-    """native/tests/test_fea.cpp:59-100: n = 4 through the thickness, tip within 6% of
+@pytest.mark.parametrize("n", [2, 4, 8])
+def test_cantilever_against_beam_theory(n):
+    """native/tests/test_fea.cpp:91-100: n = 2, 4, 8 through the thickness, tip within 6% of
     Timoshenko, reaction 100 N within 0.1%."""
-    n, Lm, b, F, E, nu = 4, 0.1, 0.01, 100.0, 200e9, 0.3
-    h = b / n
-    nx = int(round(Lm / h))
-    NX, NY, NZ = nx + 1, n + 1, n + 1
-    density = np.ones(nx * n * n, np.float32)
-    bc = np.zeros((NZ, NY, NX, 3), np.uint8)
-    bc[:, :, 0, :] = 1
-    f = np.zeros((NZ, NY, NX, 3))
-    w = np.ones(n + 1)
-    w[0] = w[-1] = 0.5
-    f[:, :, nx, 1] = -F * np.outer(w, w) / (n * n)
-    M = oracle.OracleModel("port", (nx, n, n), density, nu, bc.ravel(), 1100)
-    u, it, res, conv = M.solve(f.ravel(), 1e-7, 500)
+    dims, density, bc, f, h = KA.beam(n)
+    M = oracle.OracleModel("port", dims, density, 0.3, bc)
+    u, it, res, conv = M.solve(f, 1e-7, 500)
     assert conv
-    tip = (u.reshape(NZ, NY, NX, 3)[:, :, nx, 1] / (E * h)).mean()
-    I, G = b ** 4 / 12, E / (2 * (1 + nu))
-    expected = -F * Lm ** 3 / (3 * E * I) - F * Lm / ((5 / 6) * G * b * b)
-    assert abs(tip / expected - 1) < 0.06
+    assert abs(KA.beam_tip(u, dims, 200e9, h) / KA.timoshenko_tip() - 1) < 0.06
     assert abs(M.reactions(u)[1] - 100) < 0.1
+    if n == 8:  # test_fea.cpp:102-113: mid-span surface stress M c / I = 30 MPa, peak near 60 MPa
+        vm, _, _ = M.stresses(u / (200e9 * h), 200e9, h)
+        assert abs(vm[KA.beam_mid_node(n, dims[0])] / 30e6 - 1) < 0.05
+        assert 0.95 * 60e6 < vm.max() < 1.4 * 60e6
+
+
+@pytest.mark.parametrize("sigma", [KA.KNOWN_TENSOR, KA.GENERAL_TENSOR])
+def test_principal_stresses_of_a_known_tensor(sigma):
+    """test_fea.cpp:40-47 through the stress recovery: a linear displacement field with the
+    known uniform stress gives that stress's von Mises and principal values at every node."""
+    dims, E, nu, h = (6, 5, 4), 200e9, 0.3, 1e-3
+    bc = np.zeros((5, 6, 7, 3), np.uint8)
+    bc[:, :, 0, :] = 1  # supports play no part in stress recovery
+    M = oracle.OracleModel("port", dims, np.ones(120, np.float32), nu, bc.ravel())
+    vm, p1, p3 = M.stresses(KA.uniform_stress_field(dims, h, sigma, E, nu), E, h)
+    pr = KA.principals(sigma)
+    if sigma is KA.KNOWN_TENSOR:
+        assert np.allclose(pr, KA.KNOWN_PRINCIPALS, rtol=0, atol=1e-3)
+    scale = np.abs(sigma).max()
+    assert np.abs(vm - KA.von_mises(sigma)).max() < 1e-6 * scale
+    assert np.abs(p1 - pr[0]).max() < 1e-6 * scale and np.abs(p3 - pr[2]).max() < 1e-6 * scale
+
+
+def test_reaction_includes_loads_on_held_nodes():
+    """test_fea.cpp:124-132: one voxel, every DOF held, -100 N on a held DOF: the reaction is
+    exactly (0, 100, 0)."""
+    M = oracle.OracleModel("port", (1, 1, 1), np.ones(1, np.float32), 0.3, np.ones(24, np.uint8))
+    f = np.zeros(24)
+    f[1] = -100
+    u, it, res, conv = M.solve(f, 1e-6, 500)
+    assert conv and not u.any()
+    assert list(M.reactions(u, f)) == [0, 100, 0]
 
 
 @pytest.mark.skipif(not oracle.available("reference"), reason="oracle/_ref not built here")
