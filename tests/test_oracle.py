@@ -26,6 +26,15 @@ def test_element_matches_reference(nu):
     assert np.array_equal(K, K.T)  # exact symmetry (native/tests/test_fea.cpp:20-21)
     for d in range(3):  # rigid-body translations (native/tests/test_fea.cpp:14-19)
         assert np.abs(K[:, d::3].sum(axis=1)).max() < 1e-12
+    # the Gauss-point strain matrices reproduce the condensed stiffness (test_fea.cpp:24-38):
+    # K = sum over the 8 points of B^T D B / 8, D the isotropic elasticity matrix for E = 1
+    lam, mu = nu / ((1 + nu) * (1 - 2 * nu)), 1 / (2 * (1 + nu))
+    D = np.zeros((6, 6))
+    D[:3, :3] = lam
+    D[np.arange(3), np.arange(3)] += 2 * mu
+    D[np.arange(3, 6), np.arange(3, 6)] = mu
+    Ks = sum(B.T @ D @ B for B in gb) / 8
+    assert np.abs(Ks - K).max() < 1e-12 * np.abs(K).max()
     if nu == 0.3:
         assert np.abs(cs - g["cornerStress_0.3"]).max() <= 1e-14 * np.abs(cs).max()
         assert np.abs(gb - g["gaussB_0.3"]).max() <= 1e-14 * np.abs(gb).max()
