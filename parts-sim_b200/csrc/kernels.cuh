@@ -198,6 +198,14 @@ __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, c
 }
 
 __device__ __forceinline__ void nodeCoords(const LevelView& L, long long n, int& i, int& j, int& k) {
+    if (n <= 0xffffffffLL) {  // two 32-bit divisions: a 64-bit one is a long software sequence
+        const unsigned u = unsigned(n), px = unsigned(L.PX), ny = unsigned(L.NY);
+        const unsigned row = u / px, kk = row / ny;
+        i = int(u - row * px);
+        j = int(row - kk * ny);
+        k = int(kk);
+        return;
+    }
     const long long row = n / L.PX;
     i = int(n - row * L.PX);
     j = int(row % L.NY);

@@ -1333,6 +1333,7 @@ struct DevLevel {
     DevMem blist;      // tiled levels: the boundary nodes (pitched indices, increasing)
     int nBnd = 0;
     bool inner64 = false;  // 64-bit tiles compute their boundary nodes themselves (else k_bnd does)
+    bool split32 = false;  // 32-bit tiles leave their boundary nodes to k_bnd (else they compute them)
     bool useTiles = false;  // tiled kernel (large levels) or one thread per node (small ones)
     bool use8 = false;      // eight lanes per node (the smallest levels)
     float cf0 = 0, cf1 = 0, cf2 = 0, omega = 0.5f;
@@ -1421,6 +1422,12 @@ void SharedModel::adopt(Hierarchy&& h) {
         set(dev::k_tile<float, dev::TOP_RESID, true, false>, dev::tileSmemBytes<float, dev::TOP_RESID, true>());
         set(dev::k_tile<float, dev::TOP_RESID, true, true>, dev::tileSmemBytes<float, dev::TOP_RESID, true>());
         set(dev::k_tile<float, dev::TOP_DOT, false, true>, dev::tileSmemBytes<float, dev::TOP_DOT, true>());
+        set(dev::k_tile<float, dev::TOP_CHEB, false, false, false>, dev::tileSmemBytes<float, dev::TOP_CHEB, false>());
+        set(dev::k_tile<float, dev::TOP_CHEB, true, false, false>, dev::tileSmemBytes<float, dev::TOP_CHEB, false>());
+        set(dev::k_tile<float, dev::TOP_CHEB, true, true, false>, dev::tileSmemBytes<float, dev::TOP_CHEB, false>());
+        set(dev::k_tile<float, dev::TOP_RESID, false, false, false>, dev::tileSmemBytes<float, dev::TOP_RESID, false>());
+        set(dev::k_tile<float, dev::TOP_RESID, true, false, false>, dev::tileSmemBytes<float, dev::TOP_RESID, false>());
+        set(dev::k_tile<float, dev::TOP_RESID, true, true, false>, dev::tileSmemBytes<float, dev::TOP_RESID, false>());
     });
     L.resize(H.levels.size());
     for (int l = 0; l < int(H.levels.size()); l++) uploadLevel(l);
@@ -1513,6 +1520,13 @@ void SharedModel::uploadLevel(int l) {
                 const int v = std::atoi(e);
                 if (v == 0 || v == 1) D.inner64 = v == 1;
             }
+            // 32-bit tiles of the Galerkin levels (l >= 1) leave their boundary nodes to k_bnd: there
+            // the boundary nodes gather own matrices, and the few hundred tiles of such a level wait
+            // on their heaviest ones (L-bracket level 1: 495 tiles, 36 % boundary nodes; FP64-form
+            // solves 7-10 % faster on the L-bracket and the gyroid, the finest level slower split).
+            // PSFEA_TILE_SPLIT32: bit l set = level l split
+            D.split32 = l > 0;
+            if (const char* e = std::getenv("PSFEA_TILE_SPLIT32")) D.split32 = l < 63 && ((std::atoll(e) >> l) & 1);
         }
     }
     dev::LevelView& v = D.view;
@@ -1786,8 +1800,24 @@ void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev
     mp.r = dev::tileHasR(TM) ? mapOf(rr, MAP_TILE, false, l) : mp.y;
     mp.d = dev::tileHasD(TM) ? mapOf(dd, MAP_TILE, false, l) : mp.y;
     mp.inv = dev::tileHasD(TM) ? mapOf(D.invD.p, MAP_TILE, false, l) : mp.y;
-    const size_t sm = dev::tileSmemBytes<float, TM, true>();
     const uint32_t* tl = D.tiles.as<uint32_t>();
+    if (D.split32) {
+        // uniform nodes in the tiles, boundary nodes from the list at full occupancy (the tiles
+        // store a boundary node's staged d unchanged, and k_bnd overwrites its d and y)
+        const size_t sm = dev::tileSmemBytes<float, TM, false>();
+        const dev::Coefs<float>& c = D.c32;
+        if (diff) launch(dev::k_tile<float, TM, true, true, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
+        else if (o16) launch(dev::k_tile<float, TM, true, false, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
+        else launch(dev::k_tile<float, TM, false, false, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
+        if (!D.nBnd) return;
+        const int g = gridFor(D.nBnd, dev::NODE_THREADS, smCount * 16);
+        const int* bl = D.blist.as<int>();
+        if (diff) launch(dev::k_bnd<float, TM, true, true>, g, dev::NODE_THREADS, 0, stream, D.view, c, bl, D.nBnd, xin, y, rr, dd, c1, c2, 0, st(), part(), tick(), ctl);
+        else if (o16) launch(dev::k_bnd<float, TM, true, false>, g, dev::NODE_THREADS, 0, stream, D.view, c, bl, D.nBnd, xin, y, rr, dd, c1, c2, 0, st(), part(), tick(), ctl);
+        else launch(dev::k_bnd<float, TM, false, false>, g, dev::NODE_THREADS, 0, stream, D.view, c, bl, D.nBnd, xin, y, rr, dd, c1, c2, 0, st(), part(), tick(), ctl);
+        return;
+    }
+    const size_t sm = dev::tileSmemBytes<float, TM, true>();
     if (diff) launch(dev::k_tile<float, TM, true, true>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
     else if (o16) launch(dev::k_tile<float, TM, true, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
     else launch(dev::k_tile<float, TM, false, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);

@@ -210,3 +210,30 @@ def test_full_size_l_bracket_residual():
         assert np.linalg.norm(res) / np.linalg.norm(ff) <= 1e-7
         err[prec] = rel(r.u, truth.u)
     assert err["fp64"] < 1e-3 and err["mixed"] < max(1e-4, 3 * err["fp64"]) and err["fp32"] < max(1e-4, 3 * err["fp64"]), err
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_split_boundary_nodes_in_the_smoother(monkeypatch, precision):
+    """32-bit tiles that leave their boundary nodes to the list kernel (PSFEA_TILE_SPLIT32, a bit
+    per level) give the same V-cycle up to FP32 summation order, and solves that match the
+    oracle. Tiles forced onto levels of any size, so levels 0 and 1 of a 128x64x64 L-bracket
+    both take the tiled path."""
+    m = W.l_bracket(128, 64, 64, holes=16, seed=3)
+    monkeypatch.setenv("PSFEA_TILE_MIN_NODES", "0")
+    monkeypatch.setenv("PSFEA_TILE_SPLIT32", "0")
+    A = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    monkeypatch.setenv("PSFEA_TILE_SPLIT32", "-1")
+    B = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    r = A.apply(np.random.default_rng(7).standard_normal(A.n_dof))
+    za, zb = A.precondition(r), B.precondition(r)
+    assert rel(zb, za) < 1e-5
+    ra = A.solve(m.f, tol=1e-8, max_iter=3000, precision=precision)
+    rb = B.solve(m.f, tol=1e-8, max_iter=3000, precision=precision)
+    assert ra.converged and rb.converged
+    assert abs(ra.iterations - rb.iterations) <= 2
+    P = oracle.OracleModel("port", m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    fixed = P.fixed(0).astype(bool)
+    res = m.f - P.apply(rb.u)
+    res[fixed] = 0
+    assert np.linalg.norm(res) / np.linalg.norm(np.where(fixed, 0, m.f)) <= 1e-7
+    assert rel(rb.u, ra.u) < 1e-5
