@@ -1207,10 +1207,7 @@ struct DevMem {
     DevMem(const DevMem&) = delete;
     DevMem& operator=(const DevMem&) = delete;
     DevMem(DevMem&& o) noexcept : p(o.p), bytes(o.bytes), s(o.s) { o.p = nullptr; o.bytes = 0; }
-    DevMem& operator=(DevMem&& o) noexcept {
-        if (this != &o) { release(); p = o.p; bytes = o.bytes; s = o.s; o.p = nullptr; o.bytes = 0; }
-        return *this;
-    }
+    DevMem& operator=(DevMem&&) = delete;  // buffers move only into new owners (vector growth)
     ~DevMem() { release(); }
     void release() {
         if (p) {
