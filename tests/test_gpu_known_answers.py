@@ -1,11 +1,13 @@
-"""The reference's known-answer tests for the solve (native/tests/test_fea.cpp), run on the CUDA
-path through the C ABI: beam theory for the clamped bar, the mid-span bending stress, the
-principal stresses of a known tensor through the stress recovery, and the reaction of loads put
-directly on held nodes."""
+"""The reference's known-answer tests for the solve (native/tests/test_fea.cpp, test_gpu.cpp,
+test/fea.test.js), run on the CUDA path through the C ABI: beam theory for the clamped bar, the
+mid-span bending stress, the principal stresses of a known tensor through the stress recovery,
+the reaction of loads put directly on held nodes, the GPU solve against the CPU solver, and a
+zero load after a warm start."""
 import numpy as np
 import pytest
 
 import known_answers as KA
+import oracle
 import psfea
 
 pytestmark = pytest.mark.gpu
@@ -65,3 +67,34 @@ def test_reaction_includes_loads_on_held_nodes():
     r = S.solve(f)
     assert r.converged and r.iterations == 0 and not r.u.any()
     assert list(S.reactions(r.u, f)) == [0, 100, 0]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32"])
+@pytest.mark.parametrize("n", [4, 10])
+def test_gpu_matches_cpu_solver(n, precision):
+    """test_gpu.cpp:13-53: the clamped bar with -100 N spread evenly over the tip nodes, at rel.
+    res. 1e-8: the GPU displacements within 1e-6 of the CPU solver's in the max norm."""
+    dims, density, bc, _, h = KA.beam(n)
+    nx = dims[0]
+    NX, NY, NZ = nx + 1, n + 1, n + 1
+    f = np.zeros((NZ, NY, NX, 3))
+    f[:, :, nx, 1] = -100.0 / (NY * NZ)
+    f = f.ravel()
+    P = oracle.OracleModel("port", dims, density, NU, bc)
+    a, _, _, conv = P.solve(f, 1e-8, 500)
+    assert conv
+    S = psfea.VoxelFEA(dims, density, NU, bc)
+    r = S.solve(f, tol=1e-8, max_iter=3000, precision=precision)
+    assert r.converged
+    assert np.abs(r.u - a).max() / np.abs(a).max() < 1e-6
+
+
+def test_zero_load_clears_a_warm_start():
+    """test/fea.test.js:145-152: one voxel, the even corner nodes held, a zero load from a warm
+    start of 10 everywhere: converged, every displacement exactly 0."""
+    bc = np.zeros(24, np.uint8)
+    for node in range(0, 8, 2):
+        bc[3 * node:3 * node + 3] = 1
+    S = psfea.VoxelFEA((1, 1, 1), np.ones(1, np.float32), NU, bc)
+    r = S.solve(np.zeros(24), x0=np.full(24, 10.0))
+    assert r.converged and np.all(r.u == 0)

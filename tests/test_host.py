@@ -40,8 +40,11 @@ def test_element_matrix(nu):
 
 
 def test_invalid_inputs_raise_like_the_reference():
-    with pytest.raises(ValueError, match="Poisson"):
-        psfea.element_matrix(0.5)
+    for nu in (-1, 0.5, float("nan"), float("inf")):  # test/fea.test.js:128
+        with pytest.raises(ValueError, match="Poisson"):
+            psfea.element_matrix(nu)
+        with pytest.raises(ValueError, match="Poisson"):
+            psfea.Hierarchy((1, 1, 1), np.ones(1, np.float32), nu, np.ones(24, np.uint8))
     bc = np.zeros(3 * 5 * 2 * 2, np.uint8)
     with pytest.raises(ValueError, match="between zero and one"):
         psfea.Hierarchy((4, 1, 1), np.array([1, 2, 0, 1], np.float32), 0.3, bc)
