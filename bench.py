@@ -409,14 +409,17 @@ def main():
     value = job_rate(world, n, args.steps, tmx_max / 1e3)
     plain = job_rate(world, n, args.steps, t64_max / 1e3)
 
-    # end to end through the C ABI with host buffers (f up, u down, every step)
-    f_host = np.ascontiguousarray(m.f)
+    # end to end through the C ABI with host buffers (f up, u down, every step), both in pinned
+    # host memory
+    f_host = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    f_host[:] = m.f
+    u_host = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
     e2e_t = []
     for s in range(max(1, args.steps)):
         if pg:
             pg.barrier()
         t0 = time.perf_counter()
-        r = S.solve(f_host, tol=TOL, max_iter=MAX_ITER, precision="mixed")
+        r = S.solve(f_host, tol=TOL, max_iter=MAX_ITER, precision="mixed", out=u_host)
         e2e_t.append(time.perf_counter() - t0)
         assert r.converged
     e2e_total = reduce_max(pg, sum(e2e_t), dev)

@@ -237,17 +237,26 @@ class VoxelFEA:
             raise ValueError("Force or displacement vector has the wrong size.")
         return v
 
-    def solve(self, f, tol=1e-6, max_iter=500, x0=None, precision="fp64", cancel=None, time_limit_s=0.0, smoother_degree=0):
-        """K u = f; returns a SolveResult (u in normalised units: u_phys = u / (E h))."""
+    def solve(self, f, tol=1e-6, max_iter=500, x0=None, precision="fp64", cancel=None, time_limit_s=0.0, smoother_degree=0,
+              out=None):
+        """K u = f; returns a SolveResult (u in normalised units: u_phys = u / (E h)). out: a
+        C-contiguous float64 array of n_dof values that receives u and is returned as the result's
+        u (for instance in pinned host memory, which the device writes at full speed); else a new
+        array."""
         f = self._check_vec(f, "f")
         x0a = None if x0 is None else self._check_vec(x0, "x0")
         o = make_opts(tol, max_iter, precision, _ptr(x0a), None if cancel is None else C.addressof(cancel), time_limit_s, smoother_degree)
-        u = np.zeros(self.n_dof, np.float64)
+        if out is None:
+            u = np.zeros(self.n_dof, np.float64)
+        elif isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous and out.size == self.n_dof:
+            u = out.reshape(-1)
+        else:
+            raise ValueError("out must be a C-contiguous float64 array of n_dof values.")
         r = SolveResultC()
         st = _solve(self.h, f, C.byref(o), u, C.byref(r))
         if st >= PS_EINVAL:
             _raise(st)
-        return SolveResult(u, r.iterations, r.residual, bool(r.converged), st, r.folds, r.seconds, r.kernels)
+        return SolveResult(u if out is None else out, r.iterations, r.residual, bool(r.converged), st, r.folds, r.seconds, r.kernels)
 
     def solve_dev(self, f_ptr, u_ptr, tol=1e-6, max_iter=500, precision="fp64", x0_ptr=None, smoother_degree=0):
         """The solve on device pointers (e.g. ``tensor.data_ptr()`` of CUDA float64 tensors)."""

@@ -237,3 +237,18 @@ def test_split_boundary_nodes_in_the_smoother(monkeypatch, precision):
     res[fixed] = 0
     assert np.linalg.norm(res) / np.linalg.norm(np.where(fixed, 0, m.f)) <= 1e-7
     assert rel(rb.u, ra.u) < 1e-5
+
+
+def test_solve_into_a_pinned_caller_buffer():
+    """solve(out=...) writes u into the caller's array (here pinned host memory) and returns it:
+    bitwise the same as a solve into a new array; a buffer of the wrong type is refused."""
+    import torch
+
+    g = golden("cantilever_32x8x8")
+    S = make(g)
+    a = S.solve(g["f"], tol=1e-8, max_iter=3000)
+    buf = torch.empty(S.n_dof, dtype=torch.float64, pin_memory=True).numpy()
+    b = S.solve(g["f"], tol=1e-8, max_iter=3000, out=buf)
+    assert b.u is buf and np.array_equal(buf, a.u) and b.iterations == a.iterations
+    with pytest.raises(ValueError, match="out"):
+        S.solve(g["f"], out=np.zeros(S.n_dof, np.float32))
