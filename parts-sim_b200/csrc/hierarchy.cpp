@@ -17,6 +17,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <unordered_map>
 
 #include "host_util.hpp"
 
@@ -210,36 +211,100 @@ HostLevel coarsen(const HostLevel& F) {
                 }
     }, 1);
     int64_t nOwn = 0;
-    std::vector<int64_t> ownIdx(C.nVox, -1);
+    std::vector<int64_t> ownVox;  // the voxel of each own matrix, in increasing voxel order
     for (int64_t v = 0; v < C.nVox; v++) {
-        if (isOwn[v]) ownIdx[v] = nOwn++;
+        if (isOwn[v]) {
+            C.word[v] = OWN_BIT | uint32_t(nOwn++);
+            ownVox.push_back(v);
+        }
         if (isOwn[v] || C.word[v]) C.nElems++;
     }
     C.nOwn = nOwn;
-    C.own.assign(size_t(nOwn) * 576, 0.f);
-    parallelFor(C.nVox, [&](int64_t v0, int64_t v1) {
-        std::vector<double> out(576), Kf(576);
-        for (int64_t v = v0; v < v1; v++) {
-            if (!isOwn[v]) continue;
+    C.own.resize(size_t(nOwn) * 576);  // every matrix is written below (its class's first voxel computes it)
+    // the Galerkin matrix of own coarse voxel v, stored 32-bit at dst
+    auto computeOwn = [&](int64_t v, double* out, double* Kf, float* dst) {
+        const int I = int(v % C.nx), J = int((v / C.nx) % C.ny), K = int(v / (int64_t(C.nx) * C.ny));
+        std::fill(out, out + 576, 0.0);
+        for (int c = 0; c < 8; c++) {
+            const uint32_t w = childWord(I, J, K, c);
+            if (!w) continue;
+            if (w & OWN_BIT) {
+                const float* src = F.own.data() + int64_t(w & ~OWN_BIT) * 576;
+                for (int u = 0; u < 576; u++) Kf[u] = double(src[u]);
+                galerkinAdd(out, Kf, c, 1.0);
+            } else {
+                const double s = double(bitsFloat(w));
+                for (int u = 0; u < 576; u++) out[u] += s * M[c][u];
+            }
+        }
+        for (int u = 0; u < 576; u++) dst[u] = float(out[u]);
+    };
+    // Own coarse voxels whose 8 children match (empty, the same uniform word, or own matrices of
+    // one class) have bitwise the same matrix: each class is computed once, at its first voxel, by
+    // the code above, and copied to the others. Lattices and solid/void parts have a few hundred
+    // classes over millions of voxels; on graded grids (nearly all distinct) the search stops
+    // after a sample and every voxel is its own class.
+    struct ChildKey {
+        uint64_t d[8];
+        bool operator==(const ChildKey& o) const { return std::memcmp(d, o.d, sizeof d) == 0; }
+    };
+    struct ChildKeyHash {
+        size_t operator()(const ChildKey& k) const {
+            uint64_t h = 0x9e3779b97f4a7c15ull;
+            for (uint64_t v : k.d) {
+                h ^= v + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+                h *= 0xff51afd7ed558ccdull;
+            }
+            return size_t(h ^ (h >> 32));
+        }
+    };
+    std::vector<ChildKey> keys(static_cast<size_t>(nOwn));
+    parallelFor(nOwn, [&](int64_t o0, int64_t o1) {
+        for (int64_t o = o0; o < o1; o++) {
+            const int64_t v = ownVox[size_t(o)];
             const int I = int(v % C.nx), J = int((v / C.nx) % C.ny), K = int(v / (int64_t(C.nx) * C.ny));
-            std::fill(out.begin(), out.end(), 0.0);
             for (int c = 0; c < 8; c++) {
                 const uint32_t w = childWord(I, J, K, c);
-                if (!w) continue;
-                if (w & OWN_BIT) {
-                    const float* src = F.own.data() + int64_t(w & ~OWN_BIT) * 576;
-                    for (int u = 0; u < 576; u++) Kf[u] = double(src[u]);
-                    galerkinAdd(out.data(), Kf.data(), c, 1.0);
-                } else {
-                    const double s = double(bitsFloat(w));
-                    for (int u = 0; u < 576; u++) out[u] += s * M[c][u];
-                }
+                keys[size_t(o)].d[c] = !w ? 0 : (w & OWN_BIT) ? ((uint64_t(2) << 32) | uint32_t(F.ownClass[w & ~OWN_BIT])) : ((uint64_t(1) << 32) | w);
             }
-            float* dst = C.own.data() + ownIdx[v] * 576;
-            for (int u = 0; u < 576; u++) dst[u] = float(out[u]);
-            C.word[v] = OWN_BIT | uint32_t(ownIdx[v]);
+        }
+    }, 4096);
+    C.ownClass.assign(size_t(nOwn), 0);
+    std::vector<int64_t> rep;  // the first own index of each class
+    {
+        std::unordered_map<ChildKey, int32_t, ChildKeyHash> classOf;
+        const int64_t sample = std::min<int64_t>(nOwn, int64_t(1) << 16);
+        bool shared = true;
+        for (int64_t o = 0; o < nOwn; o++) {
+            const auto it = classOf.try_emplace(keys[size_t(o)], int32_t(rep.size()));
+            if (it.second) rep.push_back(o);
+            C.ownClass[size_t(o)] = it.first->second;
+            if (o + 1 == sample && int64_t(rep.size()) * 2 > sample) {
+                shared = false;
+                break;
+            }
+        }
+        if (!shared) {
+            rep.resize(size_t(nOwn));
+            for (int64_t o = 0; o < nOwn; o++) {
+                rep[size_t(o)] = o;
+                C.ownClass[size_t(o)] = int32_t(o);
+            }
+        }
+    }
+    parallelFor(int64_t(rep.size()), [&](int64_t c0, int64_t c1) {
+        std::vector<double> out(576), Kf(576);
+        for (int64_t c = c0; c < c1; c++) {
+            const int64_t o = rep[size_t(c)];
+            computeOwn(ownVox[size_t(o)], out.data(), Kf.data(), C.own.data() + o * 576);
         }
     }, 256);
+    parallelFor(nOwn, [&](int64_t o0, int64_t o1) {
+        for (int64_t o = o0; o < o1; o++) {
+            const int64_t r = rep[size_t(C.ownClass[size_t(o)])];
+            if (r != o) std::memcpy(C.own.data() + o * 576, C.own.data() + r * 576, 576 * sizeof(float));
+        }
+    }, 4096);
     // held coarse DOFs: fine node i interpolates to coarse i/2 and, when odd, (i+1)/2
     C.bc.assign(C.nDof, 0);
     parallelFor(C.NZ, [&](int64_t K0, int64_t K1) {

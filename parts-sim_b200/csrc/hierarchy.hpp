@@ -3,6 +3,8 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <utility>
 #include <vector>
 
 #include "element.hpp"
@@ -18,12 +20,34 @@ constexpr uint8_t NM_FIXED0 = 1, NM_FIXED1 = 2, NM_FIXED2 = 4;  // DOF d held, i
 constexpr uint8_t NM_ACTIVE = 8;    // the node is a corner of some element
 constexpr uint8_t NM_UNIFORM = 16;  // its 8 voxels are the same s * Kb: the 27-point stencil applies
 
+// An allocator whose new elements are left uninitialised: for large host arrays that parallel
+// loops fill completely right after allocation (no serial zero fill first)
+template <class T>
+struct UninitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = UninitAlloc<U>;
+    };
+    UninitAlloc() = default;
+    template <class U>
+    UninitAlloc(const UninitAlloc<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+
 struct HostLevel {
     int nx = 0, ny = 0, nz = 0, NX = 0, NY = 0, NZ = 0;
     int64_t nVox = 0, nNodes = 0, nDof = 0;
     int64_t nElems = 0, nOwn = 0, freeDof = 0;
     std::vector<uint32_t> word;   // per voxel
-    std::vector<float> own;       // nOwn * 576, row-major 24x24 each (32-bit, as the reference stores them)
+    std::vector<float, UninitAlloc<float>> own;  // nOwn * 576, row-major 24x24 each (32-bit, as the reference stores them)
+    std::vector<int32_t> ownClass;  // per own matrix: equal classes hold bitwise-equal matrices
     double Kb[576];               // the level's uniform element: K0, then the Galerkin sum of 8 children
     double S[27][9];              // Kb assembled into the 27-point stencil: neighbour m = (ox+1) + 3(oy+1) + 9(oz+1), row d, col c
     std::vector<uint8_t> bc;      // per DOF

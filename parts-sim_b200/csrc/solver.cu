@@ -1252,8 +1252,8 @@ std::vector<uint32_t> pitchedWords(const HostLevel& h, int px) {
 }
 inline int pitch4(int n) { return (n + 3) & ~3; }
 
-template <class T>
-void upload(DevMem& m, const std::vector<T>& v, int64_t& total, cudaStream_t s = nullptr) {
+template <class T, class A>
+void upload(DevMem& m, const std::vector<T, A>& v, int64_t& total, cudaStream_t s = nullptr) {
     m.alloc(v.size() * sizeof(T), total, s);
     if (!v.empty()) {
         if (s) check(cudaMemcpyAsync(m.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
