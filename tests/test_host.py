@@ -74,11 +74,16 @@ def test_hierarchy_matches_reference(name):
         assert np.array_equal(np.packbits(H.fixed(l)), g[f"fixed_{l}"])
 
 
-def test_own_matrices_match_oracle():
+@pytest.mark.parametrize("model", ["l_bracket", "gyroid", "simp"])
+def test_own_matrices_match_oracle(model):
+    """Galerkin matrices against the oracle's, on an L-bracket, a gyroid (a few hundred classes of
+    equal child patterns over thousands of voxels: computed once per class, then copied) and the
+    graded SIMP grid (180 k mostly distinct matrices on level 1: the class search stops early)."""
     import oracle
-    m = W.l_bracket(32, 16, 16, holes=3)
-    H = psfea.Hierarchy(m.dims, m.density, m.nu, m.bc)
-    P = oracle.OracleModel("port", m.dims, m.density, m.nu, m.bc)
+    m = {"l_bracket": lambda: W.l_bracket(32, 16, 16, holes=3), "gyroid": lambda: W.gyroid(48, 48, 24),
+         "simp": lambda: W.simp(nrhs=1)}[model]()
+    H = psfea.Hierarchy(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    P = oracle.OracleModel("port", m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
     for l in range(1, H.n_levels):
         a, b = H.own(l), P.own(l)
         assert a.shape == b.shape
