@@ -1367,6 +1367,7 @@ struct SharedModel {
     // may also keep the 32-bit matrices. Tuning knobs: PSFEA_OWN16_DIFF, PSFEA_MIXED_OWN32, PSFEA_FOLD.
     bool ownDiff = false;
     bool mixedOwn16 = true;
+    bool ownDedup = true;  // one device copy per class of equal own matrices (PSFEA_OWN_DEDUP=0: one per voxel)
     double foldFactor = 0.1;  // fold when the FP32 residual is this fraction of its peak
     cudaStream_t ms = nullptr;     // allocation / upload stream of the shared data
     cudaEvent_t readyEv = nullptr; // recorded when the uploads are done; contexts wait on it
@@ -1400,6 +1401,7 @@ void SharedModel::adopt(Hierarchy&& h) {
     if (const char* e = std::getenv("PSFEA_OWN16_DIFF")) ownDiff = std::atoi(e) != 0;
     if (const char* e = std::getenv("PSFEA_FOLD")) foldFactor = std::atof(e);
     if (const char* e = std::getenv("PSFEA_MIXED_OWN32")) mixedOwn16 = std::atoi(e) == 0;
+    if (const char* e = std::getenv("PSFEA_OWN_DEDUP")) ownDedup = std::atoi(e) != 0;
     check(cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking), "stream");
     check(cudaEventCreateWithFlags(&readyEv, cudaEventDisableTiming), "event");
     static std::once_flag attrOnce;
@@ -1449,19 +1451,44 @@ void SharedModel::uploadLevel(int l) {
     const HostLevel& h = H.levels[size_t(l)];
     DevLevel& D = L[size_t(l)];
     const int PX = pitch4(h.NX), px = pitch4(h.nx);
-    upload(D.word, pitchedWords(h, px), bytes, ms);
+    std::vector<uint32_t> words = pitchedWords(h, px);
+    // ownDedup: one device copy per class of bitwise-equal own matrices (the hierarchy's classes),
+    // the voxel words pointing at it. Every kernel reads a matrix through its voxel's word, so the
+    // results do not change; lattices and solid/void parts have tens to hundreds of classes for
+    // 10^4-10^6 matrices (graded grids have none to share and keep their arrays).
+    const std::vector<float, UninitAlloc<float>>* ownSrc = &h.own;
+    std::vector<float, UninitAlloc<float>> classes;
+    if (ownDedup && h.nOwn > 0 && int64_t(h.ownClass.size()) == h.nOwn) {
+        int32_t nClass = 0;
+        for (int32_t c : h.ownClass) nClass = std::max(nClass, c + 1);
+        if (nClass < h.nOwn) {
+            classes.resize(size_t(nClass) * 576);
+            std::vector<uint8_t> seen(size_t(nClass), 0);
+            for (int64_t o = 0; o < h.nOwn; o++) {
+                const int32_t c = h.ownClass[size_t(o)];
+                if (seen[size_t(c)]) continue;
+                seen[size_t(c)] = 1;
+                std::memcpy(classes.data() + size_t(c) * 576, h.own.data() + size_t(o) * 576, 576 * sizeof(float));
+            }
+            for (uint32_t& w : words)
+                if (w & OWN_BIT) w = OWN_BIT | uint32_t(h.ownClass[w & ~OWN_BIT]);
+            ownSrc = &classes;
+        }
+    }
+    const auto& own = *ownSrc;
+    upload(D.word, words, bytes, ms);
     upload(D.nmask, pitched<uint8_t>(h.nmask, 1, h, PX, uint8_t(7)), bytes, ms);  // padding: inactive, all held
     D.hasOwn = h.nOwn > 0;
     if (D.hasOwn) {
-        upload(D.own, h.own, bytes, ms);
+        upload(D.own, own, bytes, ms);
         // halves with a power-of-two level scale keeping the largest entry near 2^14
         double kmax = 0;
-        for (float v : h.own) kmax = std::max(kmax, double(std::fabs(v)));
+        for (float v : own) kmax = std::max(kmax, double(std::fabs(v)));
         const float hs = kmax > 0 ? float(std::exp2(std::ceil(std::log2(kmax / 16384.0)))) : 1.f;
-        std::vector<__half> h16(h.own.size());
+        std::vector<__half> h16(own.size());
         const float inv = 1.f / hs;
-        parallelFor(int64_t(h.own.size()), [&](int64_t lo, int64_t hi) {
-            for (int64_t i = lo; i < hi; i++) h16[size_t(i)] = __float2half_rn(h.own[size_t(i)] * inv);
+        parallelFor(int64_t(own.size()), [&](int64_t lo, int64_t hi) {
+            for (int64_t i = lo; i < hi; i++) h16[size_t(i)] = __float2half_rn(own[size_t(i)] * inv);
         });
         upload(D.own16, h16, bytes, ms);
         D.view.hs = hs;

@@ -252,3 +252,37 @@ def test_solve_into_a_pinned_caller_buffer():
     assert b.u is buf and np.array_equal(buf, a.u) and b.iterations == a.iterations
     with pytest.raises(ValueError, match="out"):
         S.solve(g["f"], out=np.zeros(S.n_dof, np.float32))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32"])
+def test_one_device_copy_per_class_of_galerkin_matrices(monkeypatch, precision):
+    """One device copy per class of bitwise-equal Galerkin matrices (the default; PSFEA_OWN_DEDUP=0
+    uploads one per voxel, as the host holds them) (the
+    gyroid's and the L-bracket's coarse levels hold tens to hundreds of distinct ones among
+    thousands) and points the voxel words at them: the operator on every level and the solves are
+    bitwise the same, in less device memory. The tiled L-bracket puts level 1 (own matrices) on
+    the tiles and the boundary-node list kernel."""
+    g = golden("gyroid_48x48x24")
+    tiled = W.l_bracket(128, 64, 64, holes=16, seed=3)
+    cases = [(lambda: make(g), g["f"], {}),
+             (lambda: psfea.VoxelFEA(tiled.dims, tiled.density, tiled.nu, tiled.bc, tiled.coarsest_max_dof), tiled.f,
+              {"PSFEA_TILE_MIN_NODES": "0"})]
+    rng = np.random.default_rng(3)
+    for build, f, env in cases:
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        monkeypatch.setenv("PSFEA_OWN_DEDUP", "0")
+        A = build()
+        monkeypatch.setenv("PSFEA_OWN_DEDUP", "1")
+        B = build()
+        assert B.device_bytes < A.device_bytes
+        for l in range(A.n_levels):
+            x = rng.standard_normal(A.level_info(l)["nDof"])
+            assert np.array_equal(A.apply(x, level=l), B.apply(x, level=l))
+        r = A.apply(rng.standard_normal(A.n_dof))
+        assert np.array_equal(A.precondition(r), B.precondition(r))
+        ra = A.solve(f, tol=1e-8, max_iter=3000, precision=precision)
+        rb = B.solve(f, tol=1e-8, max_iter=3000, precision=precision)
+        assert ra.converged and rb.iterations == ra.iterations and np.array_equal(ra.u, rb.u)
+        for k in env:
+            monkeypatch.delenv(k)
