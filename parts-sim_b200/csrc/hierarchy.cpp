@@ -71,8 +71,9 @@ inline double entry(const HostLevel& L, uint32_t w, int r, int c) {
 
 // diagonal, masks, inverse diagonal, uniform flags and the boundary node list
 void finishLevel(HostLevel& L) {
-    L.nmask.assign(L.nNodes, 0);
-    L.invDiag.assign(L.nDof, 0.0);
+    // both written in full below (one pass per z plane), so allocated without a serial zero fill
+    L.nmask.resize(size_t(L.nNodes));
+    L.invDiag.resize(size_t(L.nDof));
     std::vector<int64_t> freeCount(size_t(L.NZ), 0);
     parallelFor(L.NZ, [&](int64_t k0, int64_t k1) {
         for (int64_t k = k0; k < k1; k++) {
@@ -104,8 +105,10 @@ void finishLevel(HostLevel& L) {
                     for (int d = 0; d < 3; d++) {
                         double dg = diag[d];
                         if (!L.diagAdd.empty()) dg += L.diagAdd[3 * n + d];
-                        if (!active || L.bc[3 * n + d] || !(dg > 0)) m |= uint8_t(1u << d);
-                        else {
+                        if (!active || L.bc[3 * n + d] || !(dg > 0)) {
+                            m |= uint8_t(1u << d);
+                            L.invDiag[3 * n + d] = 0.0;
+                        } else {
                             L.invDiag[3 * n + d] = 1 / dg;
                             nfree++;
                         }

@@ -52,8 +52,8 @@ struct HostLevel {
     double S[27][9];              // Kb assembled into the 27-point stencil: neighbour m = (ox+1) + 3(oy+1) + 9(oz+1), row d, col c
     std::vector<uint8_t> bc;      // per DOF
     std::vector<double> diagAdd;  // per DOF, or empty
-    std::vector<double> invDiag;  // per DOF, 0 where fixed
-    std::vector<uint8_t> nmask;   // per node
+    std::vector<double, UninitAlloc<double>> invDiag;  // per DOF, 0 where fixed
+    std::vector<uint8_t, UninitAlloc<uint8_t>> nmask;  // per node
     std::vector<int32_t> boundary;  // active nodes without NM_UNIFORM, increasing
     double lmax = 0;              // largest eigenvalue estimate of D^-1 K (smoother), 0 = not yet
 

@@ -1236,8 +1236,8 @@ struct DevMem {
 
 // a level's per-node (comps 1) or per-DOF (comps 3) host array in the pitched device layout,
 // padding entries `fill`
-template <class T>
-std::vector<T> pitched(const std::vector<T>& v, int comps, const HostLevel& h, int PX, T fill) {
+template <class T, class A>
+std::vector<T> pitched(const std::vector<T, A>& v, int comps, const HostLevel& h, int PX, T fill) {
     std::vector<T> o(size_t(PX) * h.NY * h.NZ * comps, fill);
     const size_t rowIn = size_t(h.NX) * comps, rowOut = size_t(PX) * comps;
     for (int64_t row = 0; row < int64_t(h.NY) * h.NZ; row++)
