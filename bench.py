@@ -1,7 +1,7 @@
-"""Benchmark: solved MDOF/s to relative residual 1e-8 on the L-bracket model (256x128x128 voxels,
-12.8 M DOF), mixed-precision MG-PCG (FP64 Krylov, V-cycle on FP16 element matrices) next to the
-plain FP64 MG-PCG and the FP32-Krylov form, on one B200 per rank; plus the batched SIMP multi-RHS
-and serving-stream workloads.
+"""Benchmark: solved MDOF/s to relative residual 1e-8 on the gyroid sheet lattice (384x384x192
+voxels, 85.8 M DOF, the largest configuration; it takes ~7 GB of one B200), the mixed-precision
+MG-PCG next to the plain FP64 MG-PCG (the drop-in), on one B200 per rank; plus legs for the
+L-bracket (256x128x128), the batched SIMP multi-RHS grid and the serving stream.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl psfea|reference]
 
@@ -11,7 +11,8 @@ replicas (one model per GPU, no collective in the data path); the value is the w
 N * nDOF * K / (max over ranks of the timed region). Prints one JSON line on rank 0.
 
 ``--impl reference`` times the reference's own CPU solver (oracle/_ref, compiled from its sources;
-the CPU restatement in oracle/ when that library is absent) on the host cores instead.
+the CPU restatement in oracle/ when that library is absent) on the host cores: one complete solve
+of the same model, timed whole (the K steps partition it). That arm never loads the product library.
 """
 import argparse
 import json
@@ -35,26 +36,33 @@ MAX_ITER = 5000
 # mask byte, r, d, 1/diag read and d written: 4x12 B) and per solid voxel (its 4-byte word)
 BYTES_PER_NODE_CHEB32 = 12 + 12 + 1 + 4 * 12
 BYTES_PER_VOXEL = 4
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of that kernel on this
-# model, from an ncu capture of `bench.py --kernel-only cheb32` (the launch moves the algorithmic
-# bytes plus halo re-reads of partial tiles and the inactive node slots of active tiles)
-TRAFFIC_BYTES_CHEB32 = 211.9e6
-# iterations of the reference's FP64 MG-PCG on this model to 1e-8, measured with its own solver
-# (oracle/_ref, 8 threads): used to turn a bounded CPU sample into a full-solve time
-REFERENCE_ITERATIONS_L_BRACKET = 1181
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of that kernel on the
+# headline model, from an ncu capture of `bench.py --kernel-only cheb32 --kernel-workload gyroid`
+# (None until captured)
+TRAFFIC_BYTES_CHEB32 = None
+
+HEADLINE = "gyroid"
+WORKLOADS = {
+    "gyroid": "gyroid sheet 384x384x192 voxels (1 mm, period 24, |g| < 0.3), titanium, bottom held, 5 MPa top, rtol 1e-8",
+    "l_bracket": "l_bracket 256x128x128 voxels (0.5 mm), 64 y-holes, y=0 held, 500 N tip patch, rtol 1e-8",
+}
 
 
-WORKLOAD = "l_bracket 256x128x128 voxels (0.5 mm), 64 y-holes, y=0 held, 500 N tip patch, rtol 1e-8"
+MODELS = ("gyroid", "l_bracket", "simp", "gyroid_small")
 
 
-def bench_config(m, world, levels=None, free_dof=None):
-    """the `config` object of both arms' lines"""
-    c = {"workload": WORKLOAD, "n_dof": m.n_dof, "parallelism": f"replicas x{world}",
-         "l2": "inputs > L2 (126 MB): x/r/d/1/diag at 51 MB each per level-0 vector"}
-    if levels is not None:
-        c["levels"] = levels
-        c["free_dof"] = free_dof
-    return c
+def make_model(name):
+    """the named benchmark model (gyroid_small: the same lattice on 256x256x128 voxels, 25.6 M DOF,
+    a profiler-sized case whose level-0 vectors still exceed L2)"""
+    import voxel_models as W
+    return {"l_bracket": W.l_bracket, "simp": lambda: W.simp(nrhs=1), "gyroid": W.gyroid,
+            "gyroid_small": lambda: W.gyroid(256, 256, 128)}[name]()
+
+
+def bench_config(m, world):
+    """the `config` object of both arms' lines (identical in both)"""
+    return {"workload": WORKLOADS[HEADLINE], "n_dof": m.n_dof, "parallelism": f"replicas x{world}",
+            "l2": "inputs > L2 (126 MB): every level-0 vector is 343 MB (FP32) or 686 MB (FP64)"}
 
 
 def parse():
@@ -63,21 +71,21 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="psfea", choices=["psfea", "reference"])
-    ap.add_argument("--cpu-sample-s", type=float, default=15.0, help="CPU baseline budget (seconds of CPU work)")
+    ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="CPU baseline budget (seconds of CPU work)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel-only", choices=["cheb32", "apply64"], default=None,
                     help="build the model and launch only this level-0 operator kernel --reps times (a small, fixed "
                          "launch sequence for profilers); prints its mean CUDA-event time")
     ap.add_argument("--reps", type=int, default=5)
-    ap.add_argument("--kernel-workload", choices=["l_bracket", "simp", "gyroid"], default="l_bracket",
+    ap.add_argument("--kernel-workload", choices=MODELS, default=HEADLINE,
                     help="the model of --kernel-only")
-    ap.add_argument("--solve-only", choices=["l_bracket", "simp", "gyroid"], default=None,
+    ap.add_argument("--solve-only", choices=MODELS, default=None,
                     help="build the model, run one warm-up solve and one solve of --precision (a fixed launch "
                          "sequence for profilers); prints its time and iterations")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp32"])
     ap.add_argument("--batch-rhs", type=int, default=32, help="load cases of the batched SIMP leg (0: skip the leg)")
-    ap.add_argument("--serve-requests", type=int, default=64, help="requests of the serving leg (0: skip the leg)")
-    ap.add_argument("--large", type=int, default=1, help="1: the 85.8 M-DOF gyroid leg, 0: skip it")
+    ap.add_argument("--serve-requests", type=int, default=512, help="requests of the serving leg (0: skip the leg)")
+    ap.add_argument("--lbracket-steps", type=int, default=3, help="solves per form of the L-bracket leg (0: skip the leg)")
     return ap.parse_args()
 
 
@@ -177,51 +185,68 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(m, sample_s, kind_pref=("reference", "port")):
-    """The reference's CPU solve on this host's cores, on a bounded sample: after one warm-up solve
-    (which also estimates the smoothers), a solve capped at S iterations is timed and the
-    per-iteration time scaled to the full iteration count."""
+def reference_kind():
     import oracle
-    kind = next(k for k in kind_pref if oracle.available(k))
+    return next(k for k in ("reference", "port") if oracle.available(k))
+
+
+def cpu_baseline(m, sample_s, iterations):
+    """The reference's CPU solve on this host's cores, on a bounded sample: the model is built,
+    one solve capped at 2 iterations warms it up (and estimates the smoothers), then a solve capped
+    at S iterations is timed (S sized to about `sample_s` seconds); its per-iteration time times
+    `iterations` (the FP64 drop-in's count measured on the GPU in the same run: the reference's
+    algorithm, whose counts agree with the reference's) gives the full-solve rate."""
+    import oracle
+    kind = reference_kind()
     cores = os.cpu_count() or 1
     os.environ.setdefault("PARTS_SIM_THREADS", str(cores))
     M = oracle.OracleModel(kind, m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
-    M.solve(m.f, TOL, 1)
     t0 = time.perf_counter()
-    M.solve(m.f, TOL, 3)
-    t3 = time.perf_counter() - t0
-    per = max(t3 / 4, 1e-3)
-    S = int(max(4, min(200, sample_s / per)))
+    M.solve(m.f, TOL, 2)
+    per = max((time.perf_counter() - t0) / 3, 1e-3)
+    S = int(max(2, min(iterations, sample_s / per)))
     t0 = time.perf_counter()
     _, it, _, _ = M.solve(m.f, TOL, S)
     ts = time.perf_counter() - t0
     per_it = ts / max(it, 1)
-    full = per_it * REFERENCE_ITERATIONS_L_BRACKET
     M.close()
-    return {"value": m.n_dof / full / 1e6, "unit": "MDOF/s", "cores": int(os.environ["PARTS_SIM_THREADS"]), "kind": kind,
+    return {"value": m.n_dof / (per_it * iterations) / 1e6, "unit": "MDOF/s", "cores": int(os.environ["PARTS_SIM_THREADS"]), "kind": kind,
             "sample": f"{it} CG iterations of the {m.dims[0]}x{m.dims[1]}x{m.dims[2]} solve timed ({ts:.1f} s), scaled to the "
-                      f"{REFERENCE_ITERATIONS_L_BRACKET} iterations the reference needs for rel. res. 1e-8",
-            "s_per_iteration": per_it}
+                      f"{iterations} iterations the FP64 drop-in needed in this run"}
 
 
 def run_reference(args):
-    # the reference's CPU solver runs on rank 0 only; the other ranks of a torchrun launch exit
-    # at once (no process group: nothing is exchanged)
+    """The reference arm: the reference's own CPU solver (oracle/_ref) on all host cores, on the
+    headline model. After W warm-up iterations (a solve capped at W CG iterations, which also runs
+    the smoother estimation), ONE complete solve to rel. res. 1e-8 is timed whole; the K steps of
+    the line partition it (ms_per_step = its time / K). Nothing is extrapolated. Rank 0 only; the
+    other ranks of a torchrun launch exit at once (no process group: nothing is exchanged). The
+    product library is never loaded here."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    from psfea import workloads as W
-    m = W.l_bracket()
-    vals = []
-    for s in range(args.warmup + args.steps):
-        cb = cpu_baseline(m, args.cpu_sample_s / 2)
-        if s >= args.warmup:
-            vals.append(cb["value"])
-    v = statistics.median(vals)
+    import oracle
+    m = make_model(HEADLINE)
+    kind = reference_kind()
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("PARTS_SIM_THREADS", str(cores))
+    t0 = time.perf_counter()
+    M = oracle.OracleModel(kind, m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    build_s = time.perf_counter() - t0
+    M.solve(m.f, TOL, max(1, args.warmup))
+    t0 = time.perf_counter()
+    _, it, res, conv = M.solve(m.f, TOL, MAX_ITER)
+    t = time.perf_counter() - t0
+    M.close()
+    v = m.n_dof / t / 1e6
+    sample = (f"one complete VoxelFEA::solve of the {m.dims[0]}x{m.dims[1]}x{m.dims[2]} model to rel. res. {TOL:g} "
+              f"({it} CG iterations, true residual {res:.3g}, converged {conv}) timed whole in {t:.1f} s; the {args.steps} "
+              f"steps partition it; model build {build_s:.1f} s outside")
     line = {"metric": METRIC, "value": v, "unit": "MDOF/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": m.n_dof / v / 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "ms_per_step": t * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
             "config": bench_config(m, args.gpus),
-            "cpu_baseline": {"value": v, "unit": "MDOF/s", "cores": cb["cores"], "kind": cb["kind"], "sample": cb["sample"]},
+            "iterations": it, "residual": res, "converged": bool(conv),
+            "cpu_baseline": {"value": v, "unit": "MDOF/s", "cores": int(os.environ["PARTS_SIM_THREADS"]), "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": "MDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -233,7 +258,7 @@ def batched_leg(nrhs):
     each call sequence, host buffers in and out; solved MDOF/s = nrhs * nDOF / time."""
     import torch
     import psfea
-    from psfea import workloads as W
+    import voxel_models as W
     m = W.simp(nrhs=nrhs)
     S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
     F = np.ascontiguousarray(m.f)
@@ -258,44 +283,46 @@ def batched_leg(nrhs):
     return out
 
 
-def large_leg():
-    """The capacity workload: the gyroid sheet lattice 384x384x192 (85.8 M DOF, titanium, bottom
-    face held, 5 MPa on the top face), one solve per form after a warm-up, f and u resident in HBM;
+def l_bracket_leg(steps):
+    """The L-bracket (256x128x128, 12.8 M DOF, 1181 iterations to 1e-8: an ill-conditioned model
+    with thin ligaments): `steps` solves per form after a warm-up, f and u resident in HBM;
     CUDA-event time on the solver's stream."""
     import torch
     import psfea
-    from psfea import workloads as W
-    m = W.gyroid()
+    m = make_model("l_bracket")
     S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
     dev = torch.device("cuda", torch.cuda.current_device())
     stream = torch.cuda.Stream(device=dev)
     S.set_stream(stream.cuda_stream)
     f_dev = torch.from_numpy(m.f).to(dev)
     u_dev = torch.zeros(m.n_dof, dtype=torch.float64, device=dev)
-    out = {"workload": "gyroid 384x384x192 (period 24, |g| < 0.3), bottom held, 5 MPa top, rtol 1e-8", "n_dof": m.n_dof,
-           "device_bytes": S.device_bytes}
+    out = {"workload": WORKLOADS["l_bracket"], "n_dof": m.n_dof, "device_bytes": S.device_bytes}
     for prec in ("fp64", "mixed"):
         S.solve_dev(f_dev.data_ptr(), u_dev.data_ptr(), tol=TOL, max_iter=MAX_ITER, precision=prec)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
-        r = S.solve_dev(f_dev.data_ptr(), u_dev.data_ptr(), tol=TOL, max_iter=MAX_ITER, precision=prec)
+        its = []
+        for _ in range(steps):
+            r = S.solve_dev(f_dev.data_ptr(), u_dev.data_ptr(), tol=TOL, max_iter=MAX_ITER, precision=prec)
+            its.append(r.iterations)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        out[prec] = {"value": m.n_dof / (ms / 1e3) / 1e6, "unit": "MDOF/s", "ms": ms, "iterations": r.iterations, "converged": r.converged}
+        ms = e0.elapsed_time(e1) / steps
+        out[prec] = {"value": m.n_dof / (ms / 1e3) / 1e6, "unit": "MDOF/s", "ms": ms, "iterations": its, "converged": r.converged}
+    out["mixed_over_plain"] = out["mixed"]["value"] / out["fp64"]["value"]
     S.set_stream(0)
     S.close()
     return out
 
 
 def serving_leg(n):
-    """The serving stream: the first `n` requests of the Poisson stream (200 requests/s; box grids
-    24-160 voxels per axis with spherical voids, random material, face and traction; rtol 1e-8,
-    mixed precision), submitted at their arrival times to the continuous-batching server; latency =
-    submit to result, per request."""
+    """The serving stream: `n` requests of the Poisson stream (200 requests/s; box grids 24-160
+    voxels per axis with spherical voids, random material, face and traction; rtol 1e-8, mixed
+    precision), submitted at their arrival times to the continuous-batching server; latency =
+    submit to result, per request, split into host build, wait for admission and solve."""
     import psfea
-    from psfea import workloads as W
+    import voxel_models as W
     reqs = list(W.serving_stream(n=n))
     srv = psfea.Server()
     t0 = time.perf_counter()
@@ -310,20 +337,28 @@ def serving_leg(n):
     span = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
+    pct = lambda a, q: float(np.percentile(a, q))
     lat = np.array([r["total_s"] for r in res]) * 1e3
+    parts = {k: np.array([r[k] for r in res]) * 1e3 for k in ("build_s", "wait_s", "solve_s")}
+    its = np.array([r["iterations"] for r in res])
     dofs = sum(nd for _, nd in ids)
-    return {"workload": f"serving stream, first {n} requests at 200 req/s (box grids 24-160 voxels per axis), rtol 1e-8, mixed",
-            "requests": n, "converged": int(sum(r["converged"] for r in res)), "MDOF_per_s": dofs / span / 1e6, "makespan_s": span,
-            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
-            "solve_ms_p50": float(np.percentile([r["solve_s"] * 1e3 for r in res], 50)),
+    return {"workload": f"serving stream, {n} requests, Poisson arrivals at 200 req/s (box grids 24-160 voxels per axis), "
+                        f"rtol 1e-8, mixed", "requests": n, "converged": int(sum(r["converged"] for r in res)),
+            "MDOF_per_s": dofs / span / 1e6, "makespan_s": span, "arrival_span_s": reqs[-1][0],
+            "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99), "max": float(lat.max())},
+            "build_ms": {"p50": pct(parts["build_s"], 50), "p99": pct(parts["build_s"], 99)},
+            "wait_ms": {"p50": pct(parts["wait_s"], 50), "p99": pct(parts["wait_s"], 99)},
+            "solve_ms": {"p50": pct(parts["solve_s"], 50), "p99": pct(parts["solve_s"], 99)},
+            "iterations": {"p50": pct(its, 50), "max": int(its.max()), "mean": float(its.mean())},
+            "n_dof": {"p50": pct([nd for _, nd in ids], 50), "max": int(max(nd for _, nd in ids))},
             "peak_active": int(st["peak_active"]), "peak_device_bytes": int(st["peak_device_bytes"])}
 
 
 def kernel_only(args):
     import torch
     import psfea
-    from psfea import workloads as W
-    m = {"l_bracket": W.l_bracket, "simp": lambda: W.simp(nrhs=1), "gyroid": W.gyroid}[args.kernel_workload]()
+    import voxel_models as W
+    m = make_model(args.kernel_workload)
     S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
     ms = S.time_kernel(0 if args.kernel_only == "cheb32" else 1, args.reps)
     torch.cuda.synchronize()
@@ -333,8 +368,8 @@ def kernel_only(args):
 def solve_only(args):
     import torch
     import psfea
-    from psfea import workloads as W
-    m = {"l_bracket": W.l_bracket, "simp": lambda: W.simp(nrhs=1), "gyroid": W.gyroid}[args.solve_only]()
+    import voxel_models as W
+    m = make_model(args.solve_only)
     f = m.f if m.f.ndim == 1 else m.f[0]
     t0 = time.perf_counter()
     S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
@@ -363,10 +398,9 @@ def main():
     rank, world, local, pg = dist_setup(args.gpus)
     import torch
     import psfea
-    from psfea import workloads as W
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    m = W.l_bracket()
+    m = make_model(HEADLINE)
     n = m.n_dof
     t_setup = time.perf_counter()
     S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)  # host hierarchy + device upload
@@ -400,12 +434,10 @@ def main():
         total = ev[0].elapsed_time(ev[steps])
         return total, per, its, kern, res
 
-    # plain FP64 MG-PCG (the drop-in), then the mixed-precision form (the headline), then one solve
-    # of the FP32-Krylov form for reference
+    # plain FP64 MG-PCG (the drop-in), then the mixed-precision form (the headline)
     t64, per64, it64, k64, res64 = timed("fp64", args.steps, args.warmup)
     with Clocks(local) as clk:
         tmx, permx, itmx, kmx, resmx = timed("mixed", args.steps, args.warmup)
-    t32, per32, it32, k32, res32 = timed("fp32", 1, 1)
     tmx_max = reduce_max(pg, tmx, dev)
     t64_max = reduce_max(pg, t64, dev)
     value = job_rate(world, n, args.steps, tmx_max / 1e3)
@@ -416,6 +448,7 @@ def main():
     f_host = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
     f_host[:] = m.f
     u_host = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    S.solve(f_host, tol=TOL, max_iter=MAX_ITER, precision="mixed", out=u_host)
     e2e_t = []
     for s in range(max(1, args.steps)):
         if pg:
@@ -434,43 +467,46 @@ def main():
     alg_bytes = act_nodes * BYTES_PER_NODE_CHEB32 + act_vox * BYTES_PER_VOXEL
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ms_cheb / 1e3) / 1e9
+    model_info = {"levels": S.n_levels, "free_dof": int(S.level_info(0)["freeDof"]), "active_nodes": act_nodes,
+                  "solid_voxels": act_vox, "device_bytes": S.device_bytes}
+    S.set_stream(0)
+    S.close()
+    del f_dev, u_dev
     if rank != 0:
         if pg:
             pg.barrier()
             pg.destroy_process_group()
         return
-    # the multi-RHS and serving workloads, on one GPU (rank 0 of a replica run skips them)
+    # the other workloads, on one GPU (rank 0 of a replica run skips them)
+    lbr = l_bracket_leg(args.lbracket_steps) if args.lbracket_steps > 0 and world == 1 else None
     batched = batched_leg(args.batch_rhs) if args.batch_rhs > 0 and world == 1 else None
     serving = serving_leg(args.serve_requests) if args.serve_requests > 0 and world == 1 else None
-    large = large_leg() if args.large and world == 1 else None
     cb = None
     if world == 1 and not args.no_cpu_baseline:
         try:
-            cb = cpu_baseline(m, args.cpu_sample_s)
-            cb.pop("s_per_iteration", None)
+            cb = cpu_baseline(m, args.cpu_sample_s, max(it64))
         except Exception as e:  # the oracle build is missing: say so instead of guessing
             cb = {"value": None, "unit": "MDOF/s", "cores": os.cpu_count(), "kind": "port", "sample": f"unavailable: {e}"}
     line = {
         "metric": METRIC, "value": value, "unit": "MDOF/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": tmx_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 Krylov + f32 V-cycle on f16-scaled element matrices", "data": "synthetic",
-        "config": bench_config(m, world, S.n_levels, int(S.level_info(0)["freeDof"])),
+        "config": bench_config(m, world),
+        "model": model_info,
         "latency_ms": {"p50": float(np.percentile(permx, 50)), "p99": float(np.percentile(permx, 99)),
                        "plain_fp64_p50": float(np.percentile(per64, 50))},
         "iterations": {"mixed": itmx, "plain_fp64": it64},
         "residual": {"mixed": max(resmx), "plain_fp64": max(res64)},
         "plain_fp64": {"value": plain, "unit": "MDOF/s", "ms_per_solve": t64_max / args.steps},
-        "fp32_krylov": {"value": job_rate(world, n, 1, t32 / 1e3), "unit": "MDOF/s", "ms_per_solve": t32, "iterations": it32[0],
-                        "residual": res32[0]},
         "mixed_over_plain": value / plain,
         "setup_s": setup_s,  # model creation (outside the timed solves): the setup path
         "e2e": {"value": e2e_value, "unit": "MDOF/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": TRAFFIC_BYTES_CHEB32,
-                     "kernel": "k_tile<float,TOP_CHEB> level 0 (FP32 Chebyshev step)", "ms": ms_cheb,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": TRAFFIC_BYTES_CHEB32, "kernel": "k_tile<float,TOP_CHEB> level 0 (FP32 Chebyshev step)", "ms": ms_cheb,
                      "algorithmic_bytes": alg_bytes, "peak_kind": peak_kind, "fp64_apply_ms": ms_apply64},
+        "l_bracket": lbr,
         "batched": batched,
         "serving": serving,
-        "large": large,
         "cpu_baseline": cb,
         "gpu_launches": int(kmx),
         "clocks": clk.summary(),

@@ -150,8 +150,11 @@ ps_status ps_fea_time_kernel(ps_fea_t* h, int32_t which, int32_t reps, double* m
  * is a static 32.25 KiB device array in the library (at most 4096 reduction blocks; a device whose
  * launch shape needs more gets PS_EINVAL). The first call on each device looks up that array's
  * address and should come before any stream capture. All calls on a device share the array, so
- * calls that overlap on the GPU race. Stream-ordered on `cuda_stream` (NULL = the handle's stream);
- * returns without waiting for the GPU. */
+ * calls that overlap on the GPU race. Stream-ordered on `cuda_stream` (NULL = the handle's own
+ * stream; pass cudaStreamLegacy, (void*)1, for the legacy default stream, which is the stream
+ * PyTorch reports as 0): a caller's stream is made to wait for the handle's uploads, but not for
+ * other work the caller left queued on the handle's own stream. Call it with the handle's device
+ * current (PS_EINVAL otherwise). Returns without waiting for the GPU. */
 ps_status ps_fea_apply_dot_noalloc(ps_fea_t* h, const double* x_dev, double* y_dev, double* dot_dev, void* cuda_stream);
 
 /* Device kernels the handle has launched since it was created. */

@@ -1357,6 +1357,7 @@ struct SharedModel {
     int m = 0;
     int64_t bytes = 0;
     int smCount = 148;
+    int devId = 0;  // the CUDA device the model's data lives on
     int maxTiles = 0;
     // smoother coefficients (shared; `version` changes whenever they do, so contexts re-record)
     bool smoothersReady = false;
@@ -1395,7 +1396,6 @@ void SharedModel::build(const int32_t dims[3], const float* density, double nu, 
 
 void SharedModel::adopt(Hierarchy&& h) {
     H = std::move(h);
-    int devId = 0;
     check(cudaGetDevice(&devId), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, devId), "attribute");
     if (const char* e = std::getenv("PSFEA_OWN16_DIFF")) ownDiff = std::atoi(e) != 0;
@@ -2634,14 +2634,12 @@ __global__ void __launch_bounds__(NODE_THREADS) k_apply_dot_static(LevelView L, 
 
 namespace {
 
-// device address of g_noallocScratch per device, looked up once per device with that device
-// current (the first call on a device does it, so that first call should come before any stream
+// device address of g_noallocScratch on device devId (the current device), looked up once per
+// device (the first call on a device does it, so that first call should come before any stream
 // capture)
-unsigned char* noallocScratch() {
+unsigned char* noallocScratch(int devId) {
     static std::mutex mu;
     static std::vector<unsigned char*> addr;
-    int devId = 0;
-    check(cudaGetDevice(&devId), "cudaGetDevice");
     std::lock_guard<std::mutex> lock(mu);
     if (int(addr.size()) <= devId) addr.resize(size_t(devId) + 1, nullptr);
     if (!addr[size_t(devId)]) {
@@ -2662,8 +2660,15 @@ void Solver::applyDotStatic(const double* xDev, double* yDev, double* dotDev, vo
     if (grid > NOALLOC_BLOCKS)
         throw Error(PS_EINVAL, "this device needs " + std::to_string(grid) + " reduction blocks; the static scratch holds " +
                                    std::to_string(NOALLOC_BLOCKS));
+    int cur = -1;
+    check(cudaGetDevice(&cur), "cudaGetDevice");
+    if (cur != I.M->devId)
+        throw Error(PS_EINVAL, "the current CUDA device is " + std::to_string(cur) + "; the handle lives on device " +
+                                   std::to_string(I.M->devId));
     cudaStream_t st = s ? static_cast<cudaStream_t>(s) : I.stream;
-    unsigned char* scratch = noallocScratch();
+    // a caller's stream is ordered after the model's uploads (the handle's own stream already is)
+    if (st != I.stream) check(cudaStreamWaitEvent(st, I.M->readyEv, 0), "wait for the model");
+    unsigned char* scratch = noallocScratch(cur);
     check(cudaMemsetAsync(scratch, 0, 256, st), "ticket clear");
     I.launch(dev::k_apply_dot_static, grid, dev::NODE_THREADS, 0, st, D.view, D.c64, xDev, yDev, dotDev, scratch);
     check(cudaGetLastError(), "apply_dot_static");

@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(HERE, "libpsfea.so")
 PS_OK, PS_NOT_CONVERGED, PS_BREAKDOWN, PS_CANCELLED, PS_TIMEOUT, PS_PENDING = 0, 1, 2, 3, 4, 5
 PS_EINVAL, PS_ENONFINITE, PS_EOOM, PS_ECUDA, PS_ENODEV = 10, 11, 12, 13, 14
 PREC = {"fp64": 0, "mixed": 1, "fp32": 2}
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the legacy default stream (PyTorch's default stream, reported as 0)
 STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "CANCELLED", 4: "TIMEOUT", 5: "PENDING", 10: "EINVAL", 11: "ENONFINITE",
                 12: "EOOM", 13: "ECUDA", 14: "ENODEV"}
 
@@ -298,9 +299,16 @@ class VoxelFEA:
 
     def apply_dot_noalloc(self, x_ptr, y_ptr, dot_ptr, stream_ptr=None):
         """y = K x and x.y on device pointers without allocating (see ps_fea_apply_dot_noalloc);
-        stream-ordered, returns before the GPU has finished."""
-        st = _apply_dot_noalloc(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), C.c_void_p(dot_ptr),
-                                C.c_void_p(stream_ptr) if stream_ptr else None)
+        stream-ordered, returns before the GPU has finished. stream_ptr is a CUDA stream handle
+        such as ``torch.cuda.current_stream().cuda_stream``: 0 is the legacy default stream (what
+        PyTorch reports for its default stream) and None the handle's own stream."""
+        if stream_ptr is None:
+            stream = None
+        elif stream_ptr == 0:
+            stream = C.c_void_p(CUDA_STREAM_LEGACY)
+        else:
+            stream = C.c_void_p(stream_ptr)
+        st = _apply_dot_noalloc(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), C.c_void_p(dot_ptr), stream)
         if st != PS_OK:
             _raise(st)
 

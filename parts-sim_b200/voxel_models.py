@@ -91,31 +91,28 @@ def held_nodes(dims, bc):
     return (np.asarray(bc).reshape(-1, 3).max(axis=1) > 0).astype(np.uint8)
 
 
-def prune_floating(dims, density, bc):
+def prune_floating(dims, density, held_node):
     """Voxels face-connected (6-neighbourhood) to a voxel with a held corner node survive; the
-    rest become empty (the rule of native/src/fea/voxel_fea.cpp:1086-1119), by label propagation."""
+    rest become empty (the rule of native/src/fea/voxel_fea.cpp:1086-1119). The reference walks the
+    voxels breadth-first from the held ones; the same set is every 6-connected component of the
+    solid that contains such a voxel, found here by connected-component labelling.
+    ``held_node``: per node, nonzero where any DOF is held. Returns (density, removed)."""
+    from scipy import ndimage
     nx, ny, nz = dims
     d = np.asarray(density, np.float32).reshape(nz, ny, nx)
-    held = held_nodes(dims, bc).reshape(nz + 1, ny + 1, nx + 1)
+    held = np.asarray(held_node).reshape(nz + 1, ny + 1, nx + 1) > 0
     touch = np.zeros((nz, ny, nx), bool)
     for dk in (0, 1):
         for dj in (0, 1):
             for di in (0, 1):
-                touch |= held[dk:dk + nz, dj:dj + ny, di:di + nx] > 0
+                touch |= held[dk:dk + nz, dj:dj + ny, di:di + nx]
     solid = d > 0
-    reach = solid & touch
-    while True:
-        grow = reach.copy()
-        grow[1:] |= reach[:-1]
-        grow[:-1] |= reach[1:]
-        grow[:, 1:] |= reach[:, :-1]
-        grow[:, :-1] |= reach[:, 1:]
-        grow[:, :, 1:] |= reach[:, :, :-1]
-        grow[:, :, :-1] |= reach[:, :, 1:]
-        grow &= solid
-        if (grow == reach).all():
-            break
-        reach = grow
+    labels, _ = ndimage.label(solid)  # default structure: the 6 face neighbours
+    keep_ids = np.unique(labels[solid & touch])
+    keep = np.zeros(int(labels.max()) + 1, bool)
+    keep[keep_ids] = True
+    keep[0] = False
+    reach = keep[labels]
     out = np.where(reach, d, 0).astype(np.float32).ravel()
     return out, int(solid.sum() - reach.sum())
 
@@ -185,7 +182,7 @@ def l_bracket(nx=256, ny=128, nz=128, holes=64, seed=2, h=0.5e-3, E=70e9, nu=0.3
     NX, NY, NZ = nx + 1, ny + 1, nz + 1
     bc = np.zeros((NZ, NY, NX, 3), np.uint8)
     bc[:, 0, :, :] = 1
-    density, removed = prune_floating((nx, ny, nz), density, bc.ravel())
+    density, removed = prune_floating((nx, ny, nz), density, held_nodes((nx, ny, nz), bc))
     # load patch on top of the arm: voxel layer just below z = zq, x in [nx-8, nx), y centred
     kz = int(round(zq)) - 1
     d3 = density.reshape(nz, ny, nx)
@@ -258,13 +255,11 @@ def gyroid(nx=384, ny=384, nz=192, period=24, thickness=0.3, pressure=5e6, h=1e-
     y = t(ny)[None, :, None]
     z = t(nz)[:, None, None]
     val = np.sin(x) * np.cos(y) + np.sin(y) * np.cos(z) + np.sin(z) * np.cos(x)
-    from . import prune_floating as _prune  # the library's breadth-first search (label propagation
-    #                                          would need as many sweeps as the sheet is long)
     density = (np.abs(val) < thickness).astype(np.float32).ravel()
     NX, NY, NZ = nx + 1, ny + 1, nz + 1
     bc = np.zeros((NZ, NY, NX, 3), np.uint8)
     bc[0] = 1
-    density, removed = _prune((nx, ny, nz), density, bc.reshape(-1, 3).max(axis=1))
+    density, removed = prune_floating((nx, ny, nz), density, held_nodes((nx, ny, nz), bc))
     f, nface = _face_load((nx, ny, nz), density, 2, 1, (0.0, 0.0, -pressure * h * h))
     return Model("gyroid", (nx, ny, nz), density, bc.ravel(), f, nu, E, h, 1100, {"removed": removed, "loaded_faces": nface})
 
@@ -277,7 +272,6 @@ def box_with_voids(rng, lo=24, hi=160, solid_target=0.6, h=1e-3):
     radius U[2, 10] voxels placed until the solid fraction reaches ``solid_target``, material
     drawn from MATERIALS, one random face held and a uniform traction with a random direction and
     log-uniform magnitude in [0.1, 10] MPa on the opposite face; floating fragments pruned."""
-    from . import prune_floating as _prune  # the library's breadth-first search
     u = rng.uniform(3)
     dims = tuple(int(round(np.exp(np.log(lo) + (np.log(hi) - np.log(lo)) * v))) for v in u)
     nx, ny, nz = dims
@@ -310,7 +304,7 @@ def box_with_voids(rng, lo=24, hi=160, solid_target=0.6, h=1e-3):
     sl[2 - axis] = 0 if side == 0 else dims[axis]
     bc[tuple(sl)] = 1
     held = bc.reshape(-1, 3).max(axis=1)
-    density, nrem = _prune(dims, solid.astype(np.float32).ravel(), held)
+    density, nrem = prune_floating(dims, solid.astype(np.float32).ravel(), held)
     d = rng.normal(3)
     d /= np.linalg.norm(d)
     mag = np.exp(np.log(0.1e6) + (np.log(10e6) - np.log(0.1e6)) * rng.uniform(1)[0])

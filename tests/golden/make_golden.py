@@ -19,7 +19,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "parts-sim_b200"))
 
 import oracle  # noqa: E402
-from psfea import workloads as W  # noqa: E402
+import voxel_models as W  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
 

@@ -7,7 +7,7 @@ import pytest
 import oracle
 import psfea
 from conftest import golden
-from psfea import workloads as W
+import voxel_models as W
 
 pytestmark = pytest.mark.gpu
 

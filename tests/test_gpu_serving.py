@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import psfea
-from psfea import workloads as W
+import voxel_models as W
 
 pytestmark = pytest.mark.gpu
 

@@ -8,7 +8,7 @@ import pytest
 
 import psfea
 from conftest import ROOT, golden
-from psfea import workloads as W
+import voxel_models as W
 
 MODELS = ["cantilever_32x8x8", "cantilever_64x16x16", "lbracket_32x16x16", "simp_16x8x8", "lbracket_24x12x12_loose", "gyroid_48x48x24",
           "box_request_20_28"]
@@ -60,6 +60,34 @@ def test_prune_matches_reference():
     assert np.array_equal(o1, g["o1"]) and r1 == 1
     o2, r2 = psfea.prune_floating(tuple(g["dims2"]), g["d2"], g["h2"])
     assert np.array_equal(o2, g["o2"]) and r2 == int(g["r2"])
+
+
+def test_model_generators_prune_like_the_library():
+    """The generators' pruning (connected-component labelling, no library needed, so the reference
+    arm of the benchmark can build its inputs without loading the product) keeps exactly the voxels
+    the library's breadth-first search keeps: on the reference's prune cases, on a gyroid sheet with
+    floating fragments and on random sparse grids."""
+    g = golden("prune")
+    for d, h, dims in ((g["d1"], g["h1"], (4, 1, 1)), (g["d2"], g["h2"], tuple(g["dims2"]))):
+        o, r = W.prune_floating(dims, d, h)
+        o_lib, r_lib = psfea.prune_floating(dims, d, h)
+        assert np.array_equal(o, o_lib) and r == r_lib
+    rng = np.random.default_rng(4)
+    for dims in ((48, 48, 24), (17, 9, 13), (1, 1, 1)):
+        nx, ny, nz = dims
+        for frac in (0.35, 0.6):
+            d = (rng.random(nx * ny * nz) < frac).astype(np.float32) * rng.random(nx * ny * nz).astype(np.float32)
+            held = (rng.random((nx + 1) * (ny + 1) * (nz + 1)) < 0.02).astype(np.uint8)
+            o, r = W.prune_floating(dims, d, held)
+            o_lib, r_lib = psfea.prune_floating(dims, d, held)
+            assert np.array_equal(o, o_lib) and r == r_lib, (dims, frac)
+    m = W.gyroid(48, 48, 24)
+    t = lambda n: 2 * np.pi * (np.arange(n) + 0.5) / 24
+    val = (np.sin(t(48))[None, None, :] * np.cos(t(48))[None, :, None] + np.sin(t(48))[None, :, None] * np.cos(t(24))[:, None, None]
+           + np.sin(t(24))[:, None, None] * np.cos(t(48))[None, None, :])
+    raw = (np.abs(val) < 0.3).astype(np.float32).ravel()
+    o_lib, r_lib = psfea.prune_floating((48, 48, 24), raw, W.held_nodes((48, 48, 24), m.bc))
+    assert np.array_equal(m.density, o_lib) and m.meta["removed"] == r_lib
 
 
 @pytest.mark.parametrize("name", MODELS)

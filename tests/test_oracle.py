@@ -7,7 +7,7 @@ import pytest
 import oracle
 import known_answers as KA
 from conftest import golden
-from psfea import workloads as W
+import voxel_models as W
 
 MODELS = ["cantilever_32x8x8", "cantilever_64x16x16", "lbracket_32x16x16", "simp_16x8x8", "lbracket_24x12x12_loose", "gyroid_48x48x24",
           "box_request_20_28"]
