@@ -113,12 +113,22 @@ ps_status ps_fea_solve_dev(ps_fea_t* h, const double* f_dev, const ps_solve_opts
 /* nrhs solves on one hierarchy (the multi-load-case form: the sizing study's load groups,
  * study_runner.cpp:453-465, run as one batch). f and u_out: nrhs consecutive nDof vectors.
  * results: nrhs entries or NULL. opts->x0 (if set) holds nrhs warm starts. Returns the worst
- * outcome status. */
+ * outcome status. The FP64-Krylov forms run in blocks of up to 32 right-hand sides whose kernels
+ * take the whole block (each element matrix and voxel word read once per block); every right-hand
+ * side keeps its own CG scalars and stops on its own. PS_PREC_FP32 runs as concurrent single
+ * solves. */
 ps_status ps_fea_solve_batch(ps_fea_t* h, int32_t nrhs, const double* f, const ps_solve_opts* opts,
                              double* u_out, ps_solve_result* results);
 
 /* One V-cycle as a preconditioner, z ~ K^-1 r (voxel_fea.cpp:830-861; gpu_fea.cpp:431-450). */
 ps_status ps_fea_precondition(ps_fea_t* h, const double* r, double* z);
+
+/* The same preconditioner applied to a block of nvec vectors at once, as LOBPCG applies it to its
+ * block of residuals (eigen.cpp:508-513): r_dev, z_dev are nvec consecutive nDof-vectors in device
+ * memory; each z_k = V-cycle(r_k / max|r_k|) * max|r_k|. The V-cycle kernels take up to 32 vectors
+ * per launch. Stream-ordered on cuda_stream (NULL = the handle's stream); returns without waiting
+ * for the GPU. */
+ps_status ps_fea_precondition_block(ps_fea_t* h, int32_t nvec, const double* r_dev, double* z_dev, void* cuda_stream);
 
 /* y = K x on level `level` in FP64; held/inactive DOFs of y zeroed unless raw
  * (voxel_fea.cpp:388). */

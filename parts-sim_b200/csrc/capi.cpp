@@ -127,6 +127,15 @@ ps_status ps_fea_precondition(ps_fea_t* h, const double* r, double* z) {
     });
 }
 
+ps_status ps_fea_precondition_block(ps_fea_t* h, int32_t nvec, const double* r_dev, double* z_dev, void* cuda_stream) {
+    return guarded([&] {
+        if (!h || nvec < 0 || (nvec > 0 && (!r_dev || !z_dev))) return fail(PS_EINVAL, "NULL vector");
+        if (nvec == 0) return PS_OK;
+        h->solver.preconditionBlock(nvec, r_dev, z_dev, cuda_stream);
+        return PS_OK;
+    });
+}
+
 ps_status ps_fea_apply(ps_fea_t* h, int32_t level, const double* x, double* y, int32_t raw) {
     return guarded([&] {
         if (!h || !x || !y) return fail(PS_EINVAL, "NULL vector");

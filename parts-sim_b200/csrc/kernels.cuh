@@ -115,8 +115,10 @@ __device__ __forceinline__ void own16Rows(const __half* M, const T xe[24], T t[3
 // translation-free term and always uses x_n itself.
 //
 // x is read at node index n with row pitch XP (L.PX for the level's own vectors); the diagonal
-// shift at the level's node index nm.
-template <class T, bool OWN16, bool DIFF = false>
+// shift at the level's node index nm. S: the stride between consecutive DOFs of x (1 for one
+// vector; the block width for the RHS-minor layout of a multi-RHS block, x then pointing at the
+// lane's right-hand side).
+template <class T, bool OWN16, bool DIFF = false, int S = 1>
 __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, const T* __restrict__ x, int i, int j, int k,
                                         long long n, uint8_t mask, T acc[3], long long XP, long long nm) {
     acc[0] = acc[1] = acc[2] = T(0);
@@ -124,9 +126,9 @@ __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, c
     const long long NX = XP, NXY = XP * L.NY;
     T own0 = 0, own1 = 0, own2 = 0;
     if (DIFF) {
-        own0 = __ldg(x + 3 * n);
-        own1 = __ldg(x + 3 * n + 1);
-        own2 = __ldg(x + 3 * n + 2);
+        own0 = __ldg(x + 3 * S * n);
+        own1 = __ldg(x + 3 * S * n + S);
+        own2 = __ldg(x + 3 * S * n + 2 * S);
     }
     if (mask & NM_UNIFORM) {
         const float s = __uint_as_float(__ldg(L.word + L.wi(i - 1, j - 1, k - 1)));
@@ -135,8 +137,8 @@ __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, c
         for (int m = 0; m < 27; m++) {
             const int ox = m % 3 - 1, oy = (m / 3) % 3 - 1, oz = m / 9 - 1;
             if (DIFF && m == 13) continue;  // the node itself: a zero difference
-            const T* xp = x + 3 * (n + ox + oy * NX + oz * NXY);
-            const T x0 = __ldg(xp) - own0, x1 = __ldg(xp + 1) - own1, x2 = __ldg(xp + 2) - own2;
+            const T* xp = x + 3 * S * (n + ox + oy * NX + oz * NXY);
+            const T x0 = __ldg(xp) - own0, x1 = __ldg(xp + S) - own1, x2 = __ldg(xp + 2 * S) - own2;
             a0 += C.S[m * 9 + 0] * x0;
             a1 += C.S[m * 9 + 4] * x1;
             a2 += C.S[m * 9 + 8] * x2;
@@ -161,10 +163,10 @@ __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, c
 #pragma unroll
             for (int b = 0; b < 8; b++) {
                 const int bx = (b == 1 || b == 2 || b == 5 || b == 6), by = (b == 2 || b == 3 || b == 6 || b == 7), bz = b >> 2;
-                const T* xp = x + 3 * (n + (di + bx - 1) + (dj + by - 1) * NX + (dk + bz - 1) * NXY);
+                const T* xp = x + 3 * S * (n + (di + bx - 1) + (dj + by - 1) * NX + (dk + bz - 1) * NXY);
                 xe[3 * b] = __ldg(xp) - own0;
-                xe[3 * b + 1] = __ldg(xp + 1) - own1;
-                xe[3 * b + 2] = __ldg(xp + 2) - own2;
+                xe[3 * b + 1] = __ldg(xp + S) - own1;
+                xe[3 * b + 2] = __ldg(xp + 2 * S) - own2;
             }
             if (!(w & OWN_BIT)) {
                 T t[3];
@@ -193,7 +195,7 @@ __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, c
     }
     if (L.dadd) {
 #pragma unroll
-        for (int d = 0; d < 3; d++) acc[d] += (sizeof(T) == 8 ? T(L.dadd[3 * nm + d]) : T(L.dadd32[3 * nm + d])) * x[3 * n + d];
+        for (int d = 0; d < 3; d++) acc[d] += (sizeof(T) == 8 ? T(L.dadd[3 * nm + d]) : T(L.dadd32[3 * nm + d])) * x[(3 * n + d) * S];
     }
 }
 

@@ -1183,6 +1183,11 @@ __global__ void k_reactions(long long nNodes, const uint8_t* __restrict__ nmask,
 }
 
 }  // namespace dev
+}  // namespace psfea
+
+#include "block_kernels.cuh"  // the multi-RHS kernels (they use the control helpers above)
+
+namespace psfea {
 
 // ==================================================================== host side
 
@@ -1374,6 +1379,7 @@ struct SharedModel {
     cudaEvent_t readyEv = nullptr; // recorded when the uploads are done; contexts wait on it
 
     ~SharedModel() {
+        for (auto& a : act) a.release();
         for (auto& D : L) D.release();
         cDof.release();
         cInv.release();
@@ -1384,9 +1390,15 @@ struct SharedModel {
         if (readyEv) cudaEventDestroy(readyEv);
     }
 
+    // per level, the pitched indices of its active nodes in increasing order (the block kernels walk
+    // them); built on the first block solve
+    std::vector<DevMem> act;
+    std::vector<int> nAct;
+
     void build(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsest, const double* diagAdd);
     void adopt(Hierarchy&& h);  // upload a hierarchy built on the host beforehand
     void uploadLevel(int l);
+    void ensureActiveLists();
     bool exactOneLevel() const { return L.size() == 1 && H.hasFactor(); }
 };
 
@@ -1575,6 +1587,27 @@ void SharedModel::uploadLevel(int l) {
             D.c32.S[m * 9 + e] = float(h.S[m][e]);
             D.c32.S2[m * 9 + e] = make_float2(float(h.S[m][e]), float(h.S[m][e]));
         }
+}
+
+void SharedModel::ensureActiveLists() {
+    if (!act.empty()) return;
+    act.reserve(L.size());
+    nAct.resize(L.size());
+    for (size_t l = 0; l < L.size(); l++) {
+        const HostLevel& h = H.levels[l];
+        const int PX = pitch4(h.NX);
+        std::vector<int32_t> list;
+        for (int64_t row = 0; row < int64_t(h.NY) * h.NZ; row++) {
+            const uint8_t* mk = h.nmask.data() + row * h.NX;
+            for (int i = 0; i < h.NX; i++)
+                if (mk[i] & NM_ACTIVE) list.push_back(int32_t(i + int64_t(PX) * row));
+        }
+        if (int64_t(PX) * h.NY * h.NZ > int64_t(INT32_MAX)) throw Error(PS_EINVAL, "level too large for 32-bit node lists");
+        act.emplace_back();
+        nAct[l] = int(list.size());
+        upload(act.back(), list, bytes, ms);
+    }
+    check(cudaEventRecord(readyEv, ms), "event");
 }
 
 // One solve context: work vectors, control state, stream and recorded iteration graphs over a
@@ -2274,13 +2307,439 @@ bool SolverImpl::advance(bool block, ps_solve_result& res) {
     return true;
 }
 
+// ==================================================================== block (multi-RHS) solves
+//
+// Up to RB right-hand sides of one model solved together (the sizing study's load groups,
+// native/src/fea/study_runner.cpp:453-465, and LOBPCG's block preconditioning, native/src/fea/
+// eigen.cpp:508-513): every kernel of the iteration takes the whole block, so voxel words, masks and
+// Galerkin matrices are read once per block instead of once per right-hand side. Each right-hand
+// side keeps its own flexible CG (FP64 Krylov, FP32 V-cycle as in the single solve).
+
+struct BlockBase {
+    virtual ~BlockBase() = default;
+    virtual int width() const = 0;
+    virtual int64_t deviceBytes() const = 0;
+    virtual int64_t launchCount() const = 0;
+    // nrhs <= width() solves; f and u: nrhs consecutive dense vectors (host when host, else device);
+    // x0 (same place as f) or null
+    virtual ps_status solve(int nrhs, const double* f, const double* x0, bool host, const ps_solve_opts& o, double* u,
+                            ps_solve_result* res) = 0;
+    // z = one V-cycle applied to each of nvec <= width() dense device vectors r (voxel_fea.cpp:830-861)
+    virtual void precondition(int nvec, const double* rDev, double* zDev, cudaStream_t caller) = 0;
+};
+
+template <int RB>
+struct BlockImpl final : BlockBase {
+    std::shared_ptr<SharedModel> M;
+    Hierarchy& H;
+    std::vector<DevLevel>& L;
+    int smCount;
+    std::vector<LevelWork> W;     // FP32 V-cycle vectors per level, RB wide
+    DevMem f, x, r, p, q, z64;    // FP64 vectors of the finest level, RB wide
+    DevMem state, partials, ticket;
+    dev::BlockState* hostState = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    int64_t bytes = 0, launches = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int64_t graphKernels[2] = {0, 0};
+    int64_t graphVersion[2] = {-1, -1};
+
+    BlockImpl(std::shared_ptr<SharedModel> model) : M(std::move(model)), H(M->H), L(M->L), smCount(M->smCount) {
+        M->ensureActiveLists();
+        check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+        check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+        check(cudaMallocHost(&hostState, sizeof(dev::BlockState)), "cudaMallocHost");
+        W.resize(L.size());
+        for (size_t l = 0; l < W.size(); l++) {
+            const size_t n = size_t(pd(int(l))) * RB * 4;
+            W[l].r.alloc(n, bytes, stream);
+            W[l].z.alloc(n, bytes, stream);
+            W[l].t.alloc(n, bytes, stream);
+            W[l].d.alloc(n, bytes, stream);
+        }
+        const size_t n = size_t(pd(0)) * RB * 8;
+        for (DevMem* b : {&f, &x, &r, &p, &q}) b->alloc(n, bytes, stream);
+        if (M->exactOneLevel()) z64.alloc(n, bytes, stream);
+        state.alloc(sizeof(dev::BlockState), bytes, stream);
+        partials.alloc(size_t(smCount) * 16 * RB * 3 * sizeof(double) + 4096, bytes, stream);
+        ticket.alloc(64, bytes, stream);
+        check(cudaStreamWaitEvent(stream, M->readyEv, 0), "wait");
+    }
+    ~BlockImpl() override {
+        cudaStreamSynchronize(stream);
+        for (auto& g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        for (auto& w : W) w.release();
+        for (DevMem* b : {&f, &x, &r, &p, &q, &z64, &state, &partials, &ticket}) b->release();
+        if (ev) cudaEventDestroy(ev);
+        if (hostState) cudaFreeHost(hostState);
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+    }
+
+    static int64_t bytesFor(const Hierarchy& H) {
+        int64_t b = 0;
+        for (const HostLevel& h : H.levels) b += 16 * int64_t(3) * pitch4(h.NX) * h.NY * h.NZ * RB;
+        const HostLevel& h0 = H.levels[0];
+        b += 6 * 8 * int64_t(3) * pitch4(h0.NX) * h0.NY * h0.NZ * RB;
+        return b;
+    }
+
+    int width() const override { return RB; }
+    int64_t deviceBytes() const override { return bytes; }
+    int64_t launchCount() const override { return launches; }
+
+    template <class... KArgs, class... Args>
+    void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, Args&&... args) {
+        kernel<<<grid, block, smem, stream>>>(std::forward<Args>(args)...);
+        ++launches;
+    }
+    int64_t pn(int l) const { return L[size_t(l)].view.nNodes; }
+    int64_t pd(int l) const { return 3 * pn(l); }
+    const int* act(int l) const { return M->act[size_t(l)].template as<int>(); }
+    int nAct(int l) const { return M->nAct[size_t(l)]; }
+    // grid of a kernel with one lane per (active node, right-hand side)
+    int laneGrid(int l) const { return gridFor(int64_t(nAct(l)) * RB, dev::BLOCK_THREADS, smCount * 8); }
+    int elemGrid(int l) const { return gridFor(int64_t(nAct(l)) * 3 * RB, dev::BLOCK_THREADS, smCount * 8); }
+    dev::BlockState* bs() const { return state.as<dev::BlockState>(); }
+    double* part() const { return partials.as<double>(); }
+    unsigned* tick() const { return ticket.as<unsigned>(); }
+
+    template <class T, int MODE>
+    void op(int l, const T* xin, T* y, float c1, float c2, bool raw, bool own16, dev::Ctl ctl) {
+        DevLevel& D = L[size_t(l)];
+        if (!nAct(l)) return;
+        float* rr = W[size_t(l)].r.template as<float>();
+        float* dd = W[size_t(l)].d.template as<float>();
+        const auto& C = [&]() -> const dev::Coefs<T>& {
+            if constexpr (sizeof(T) == 8) return D.c64;
+            else return D.c32;
+        }();
+        if (own16 && D.hasOwn)
+            launch(dev::kb_op<T, MODE, true, RB>, laneGrid(l), dev::BLOCK_THREADS, 0, D.view, C, act(l), nAct(l), xin, y, rr, dd, c1, c2,
+                   raw ? 1 : 0, bs(), part(), tick(), ctl);
+        else
+            launch(dev::kb_op<T, MODE, false, RB>, laneGrid(l), dev::BLOCK_THREADS, 0, D.view, C, act(l), nAct(l), xin, y, rr, dd, c1, c2,
+                   raw ? 1 : 0, bs(), part(), tick(), ctl);
+    }
+
+    void coarse(const float* rin, float* zout, dev::Ctl ctl) {
+        const int warpsNeeded = (M->m + (32 / RB) - 1) / (32 / RB);
+        const int grid = std::max(1, std::min(smCount * 8, (warpsNeeded + 7) / 8));
+        launch(dev::kb_coarse<float, float, RB>, grid, dev::BLOCK_THREADS, 0, M->m, M->cDof.template as<int>(), M->cInv.template as<double>(),
+               rin, zout, ctl);
+    }
+
+    // the block V-cycle on level l from W[l].r (voxel_fea.cpp:817-828); returns the result buffer
+    float* vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
+        DevLevel& D = L[size_t(l)];
+        LevelWork& Wl = W[size_t(l)];
+        float *z = Wl.z.template as<float>(), *t = Wl.t.template as<float>(), *rl = Wl.r.template as<float>(), *d = Wl.d.template as<float>();
+        const int last = int(L.size()) - 1;
+        if (l == last) {
+            if (H.hasFactor()) {
+                coarse(rl, z, ctl);
+                return z;
+            }
+            if (!firstDone)
+                launch(dev::kb_cheb_first<RB>, elemGrid(l), dev::BLOCK_THREADS, 0, act(l), nAct(l), D.invD.template as<float>(), rl, d, z, D.omega,
+                       ctl);
+            float* a = z;
+            float* b = t;
+            for (int s = 1; s < 40; s++) {
+                op<float, dev::BOP_CHEB>(l, a, b, 0.f, D.omega, false, own16, ctl);
+                std::swap(a, b);
+            }
+            return a;
+        }
+        DevLevel& C = L[size_t(l + 1)];
+        LevelWork& Wc = W[size_t(l + 1)];
+        if (!firstDone)
+            launch(dev::kb_cheb_first<RB>, elemGrid(l), dev::BLOCK_THREADS, 0, act(l), nAct(l), D.invD.template as<float>(), rl, d, z, D.cf0, ctl);
+        float* a = z;
+        float* b = t;
+        for (size_t k = 0; k < D.chebC1.size(); k++) {
+            op<float, dev::BOP_CHEB>(l, a, b, D.chebC1[k], D.chebC2[k], false, own16, ctl);
+            std::swap(a, b);
+        }
+        op<float, dev::BOP_RESID>(l, a, b, 0.f, 0.f, false, own16, ctl);
+        const bool fuse = !(l + 1 == last && H.hasFactor());
+        const float c0c = (l + 1 == last) ? C.omega : C.cf0;
+        launch(dev::kb_restrict<RB>, laneGrid(l + 1), dev::BLOCK_THREADS, 0, D.view, C.view, act(l + 1), nAct(l + 1), b, Wc.r.template as<float>(),
+               fuse ? Wc.d.template as<float>() : nullptr, fuse ? Wc.z.template as<float>() : nullptr, c0c, ctl);
+        float* zc = vcycle(l + 1, ctl, own16, fuse);
+        launch(dev::kb_prolong<RB>, laneGrid(l), dev::BLOCK_THREADS, 0, D.view, C.view.PX, C.view.NY, act(l), nAct(l), zc, a, ctl);
+        op<float, dev::BOP_CHEB>(l, a, b, 0.f, D.cf0, false, own16, ctl);
+        std::swap(a, b);
+        for (size_t k = 0; k < D.chebC1.size(); k++) {
+            op<float, dev::BOP_CHEB>(l, a, b, D.chebC1[k], D.chebC2[k], false, own16, ctl);
+            std::swap(a, b);
+        }
+        return a;
+    }
+
+    // z of the finest level: the V-cycle (from the fused first step) or the direct solve
+    const float* precond(dev::Ctl ctl, bool own16) {
+        if (M->exactOneLevel()) {
+            const int warpsNeeded = (M->m + (32 / RB) - 1) / (32 / RB);
+            const int grid = std::max(1, std::min(smCount * 8, (warpsNeeded + 7) / 8));
+            launch(dev::kb_coarse<double, double, RB>, grid, dev::BLOCK_THREADS, 0, M->m, M->cDof.template as<int>(),
+                   M->cInv.template as<double>(), r.template as<double>(), z64.template as<double>(), ctl);
+            return nullptr;
+        }
+        return vcycle(0, ctl, own16, true);
+    }
+
+    void recordIteration(dev::Ctl ctl, bool own16) {
+        DevLevel& D = L[0];
+        LevelWork& W0 = W[0];
+        op<double, dev::BOP_DOT>(0, p.template as<double>(), q.template as<double>(), 0.f, 0.f, false, false, ctl);
+        const bool one = M->exactOneLevel();
+        launch(dev::kb_cg_update<RB>, laneGrid(0), dev::BLOCK_THREADS, 0, act(0), nAct(0), D.view.nmask, x.template as<double>(),
+               r.template as<double>(), p.template as<double>(), q.template as<double>(), W0.r.template as<float>(), D.invD.template as<float>(),
+               W0.d.template as<float>(), W0.z.template as<float>(), one ? 0.f : D.cf0, bs(), part(), tick(), ctl);
+        const float* z32 = precond(ctl, own16);
+        launch(dev::kb_cg_dots<RB>, laneGrid(0), dev::BLOCK_THREADS, 0, act(0), nAct(0), D.view.nmask, r.template as<double>(), z32,
+               one ? z64.template as<double>() : nullptr, q.template as<double>(), bs(), part(), tick(), ctl);
+        launch(dev::kb_cg_p<RB>, laneGrid(0), dev::BLOCK_THREADS, 0, act(0), nAct(0), D.view.nmask, z32, one ? z64.template as<double>() : nullptr,
+               p.template as<double>(), bs(), ctl);
+    }
+
+    // dense <-> block (device to device); scale per right-hand side or null
+    void pack(const double* dense, int nrhs, double* blk, bool toBlock, const double* scale = nullptr) {
+        const dev::LevelView& v = L[0].view;
+        const int64_t nDense = int64_t(3) * v.NX * v.NY * v.NZ;
+        launch(dev::kb_pack<RB>, gridFor(nDense, 32, smCount * 16), 256, 0, const_cast<double*>(dense), nrhs, (long long)nDense, blk, v.NX,
+               v.NY, v.PX, toBlock ? 1 : 0, scale);
+    }
+
+    void readState() {
+        check(cudaMemcpyAsync(hostState, state.p, sizeof(dev::BlockState), cudaMemcpyDeviceToHost, stream), "state read");
+        check(cudaEventRecord(ev, stream), "event");
+        check(cudaEventSynchronize(ev), "sync");
+    }
+
+    ps_status solve(int nrhs, const double* fIn, const double* x0In, bool host, const ps_solve_opts& o, double* uOut,
+                    ps_solve_result* res) override {
+        const auto t0 = std::chrono::steady_clock::now();
+        const int64_t launches0 = launches;
+        DevLevel& D = L[0];
+        LevelWork& W0 = W[0];
+        const HostLevel& h0 = H.levels[0];
+        const size_t nDense = size_t(h0.nDof);
+        const bool own16 = o.precision == PS_PREC_MIXED && M->mixedOwn16;
+        const dev::Ctl none{nullptr, nullptr};
+        const dev::Ctl ctl{&bs()->allDone, nullptr};
+        // inputs: q holds the dense staging (RB >= nrhs vectors fit in one block vector)
+        double* stage = q.template as<double>();
+        auto bring = [&](const double* src, double* dst) {
+            if (host) {
+                check(cudaMemcpyAsync(stage, src, nDense * nrhs * 8, cudaMemcpyHostToDevice, stream), "upload");
+                pack(stage, nrhs, dst, true);
+            } else {
+                pack(src, nrhs, dst, true);
+            }
+        };
+        check(cudaMemsetAsync(x.p, 0, x.bytes, stream), "memset");
+        check(cudaMemsetAsync(p.p, 0, p.bytes, stream), "memset");
+        bring(fIn, f.template as<double>());
+        if (x0In) {
+            bring(x0In, x.template as<double>());
+            launch(dev::kb_mask_fixed<RB>, gridFor(pn(0) * 3 * RB, dev::BLOCK_THREADS, smCount * 8), dev::BLOCK_THREADS, 0, pn(0), D.view.nmask,
+                   x.template as<double>());
+        }
+        dev::BlockState s{};
+        s.tol = o.tol;
+        s.maxIter = o.max_iter;
+        s.first = 1;
+        s.nrhs = nrhs;
+        *hostState = s;
+        check(cudaMemcpyAsync(state.p, hostState, sizeof s, cudaMemcpyHostToDevice, stream), "state");
+        op<double, dev::BOP_APPLY>(0, x.template as<double>(), q.template as<double>(), 0.f, 0.f, false, false, none);
+        launch(dev::kb_cg_init<RB>, laneGrid(0), dev::BLOCK_THREADS, 0, act(0), nAct(0), D.view.nmask, f.template as<double>(),
+               q.template as<double>(), r.template as<double>(), bs(), part(), tick());
+        const bool one = M->exactOneLevel();
+        launch(dev::kb_vc_load<RB>, laneGrid(0), dev::BLOCK_THREADS, 0, act(0), nAct(0), D.view.nmask, r.template as<double>(),
+               W0.r.template as<float>(), D.invD.template as<float>(), W0.d.template as<float>(), W0.z.template as<float>(), one ? 0.f : D.cf0,
+               bs(), ctl);
+        const float* z32 = precond(ctl, own16);
+        launch(dev::kb_cg_dots<RB>, laneGrid(0), dev::BLOCK_THREADS, 0, act(0), nAct(0), D.view.nmask, r.template as<double>(), z32,
+               one ? z64.template as<double>() : nullptr, q.template as<double>(), bs(), part(), tick(), ctl);
+        launch(dev::kb_cg_p<RB>, laneGrid(0), dev::BLOCK_THREADS, 0, act(0), nAct(0), D.view.nmask, z32, one ? z64.template as<double>() : nullptr,
+               p.template as<double>(), bs(), ctl);
+        launch(dev::kb_clear_first, 1, 1, 0, bs());
+        check(cudaGetLastError(), "block solve setup");
+        const int gi = own16 ? 1 : 0;
+        if (graph[gi] && graphVersion[gi] != M->version) {
+            cudaGraphExecDestroy(graph[gi]);
+            graph[gi] = nullptr;
+        }
+        if (!graph[gi]) {
+            cudaGraph_t gr;
+            check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
+            recordIteration(ctl, own16);
+            check(cudaStreamEndCapture(stream, &gr), "capture end");
+            size_t nodes = 0;
+            check(cudaGraphGetNodes(gr, nullptr, &nodes), "graph nodes");
+            graphKernels[gi] = int64_t(nodes);
+            launches -= int64_t(nodes);
+            check(cudaGraphInstantiate(&graph[gi], gr, 0), "instantiate");
+            cudaGraphDestroy(gr);
+            graphVersion[gi] = M->version;
+        }
+        readState();
+        ps_status outcome = PS_OK;
+        int batch = 2, lastIt = 0;
+        double lastRel = 0;
+        while (!hostState->allDone) {
+            if (o.cancel && *o.cancel) {
+                outcome = PS_CANCELLED;
+                break;
+            }
+            if (o.time_limit_s > 0 && std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o.time_limit_s) {
+                outcome = PS_TIMEOUT;
+                break;
+            }
+            // the next batch of iterations, sized from the slowest right-hand side's convergence
+            double rel = 0;
+            for (int k = 0; k < nrhs; k++)
+                if (!hostState->done[k]) rel = std::max(rel, hostState->rel[k]);
+            const int it = hostState->iter;
+            if (lastIt > 0 && it > lastIt && rel > 0 && lastRel > 0) {
+                const double rate = std::pow(rel / lastRel, 1.0 / (it - lastIt));
+                int need = 32;
+                if (rate < 0.999) need = int(std::ceil(std::log(o.tol / rel) / std::log(rate)));
+                batch = std::max(1, std::min({need, 32, 2 * batch}));
+            }
+            lastRel = rel;
+            lastIt = it;
+            const int nb = std::max(1, std::min(batch, o.max_iter - it + 1));
+            for (int b = 0; b < nb; b++) check(cudaGraphLaunch(graph[gi], stream), "graph launch");
+            launches += int64_t(nb) * graphKernels[gi];
+            readState();
+        }
+        // zero loads: u = 0 (x holds 0 there unless a warm start was given)
+        dev::BlockState fin = *hostState;
+        for (int k = 0; k < nrhs; k++)
+            if (fin.done[k] == 2) launch(dev::kb_zero_rhs<RB>, gridFor(pn(0) * 3, dev::BLOCK_THREADS, smCount * 8), dev::BLOCK_THREADS, 0, pn(0),
+                                         x.template as<double>(), k);
+        op<double, dev::BOP_APPLY>(0, x.template as<double>(), q.template as<double>(), 0.f, 0.f, false, false, none);
+        launch(dev::kb_final<RB>, laneGrid(0), dev::BLOCK_THREADS, 0, act(0), nAct(0), D.view.nmask, f.template as<double>(),
+               q.template as<double>(), bs(), part(), tick());
+        if (host) {
+            pack(stage, nrhs, x.template as<double>(), false);
+            check(cudaMemcpyAsync(uOut, stage, nDense * nrhs * 8, cudaMemcpyDeviceToHost, stream), "download");
+        } else {
+            pack(uOut, nrhs, x.template as<double>(), false);
+        }
+        readState();
+        check(cudaGetLastError(), "block solve");
+        const dev::BlockState& hs = *hostState;
+        ps_status worst = PS_OK;
+        const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        for (int k = 0; k < nrhs; k++) {
+            ps_solve_result rr{};
+            rr.iterations = hs.it[k];
+            rr.residual = hs.rel[k];
+            rr.converged = outcome == PS_OK && std::isfinite(hs.rel[k]) && hs.rel[k] <= o.tol * 10;
+            ps_status st = outcome;
+            if (st == PS_OK) {
+                if (hs.status[k] == dev::ST_BREAKDOWN && !rr.converged) st = PS_BREAKDOWN;
+                else if (!rr.converged) st = PS_NOT_CONVERGED;
+            }
+            rr.status = st;
+            rr.seconds = secs;
+            rr.kernels = (launches - launches0);
+            if (res) res[k] = rr;
+            if (st > worst) worst = st;
+        }
+        return worst;
+    }
+
+    void precondition(int nvec, const double* rDev, double* zDev, cudaStream_t caller) override {
+        DevLevel& D = L[0];
+        LevelWork& W0 = W[0];
+        const dev::Ctl none{nullptr, nullptr};
+        if (caller && caller != stream) {
+            check(cudaEventRecord(ev, caller), "event");
+            check(cudaStreamWaitEvent(stream, ev, 0), "wait");
+        }
+        dev::BlockState s{};
+        s.nrhs = nvec;
+        *hostState = s;
+        check(cudaMemcpyAsync(state.p, hostState, sizeof s, cudaMemcpyHostToDevice, stream), "state");
+        check(cudaMemsetAsync(r.p, 0, r.bytes, stream), "memset");
+        pack(rDev, nvec, r.template as<double>(), true);
+        launch(dev::kb_rmax<RB>, laneGrid(0), dev::BLOCK_THREADS, 0, act(0), nAct(0), D.view.nmask, r.template as<double>(), bs(), part(), tick());
+        check(cudaMemsetAsync(q.p, 0, q.bytes, stream), "memset");
+        if (z64.p) check(cudaMemsetAsync(z64.p, 0, z64.bytes, stream), "memset");
+        if (M->exactOneLevel()) {
+            // the whole model is the coarsest level: its direct FP64 solve (voxel_fea.cpp:838-842)
+            precond(none, false);
+            pack(zDev, nvec, z64.template as<double>(), false);
+        } else {
+            launch(dev::kb_vc_load<RB>, laneGrid(0), dev::BLOCK_THREADS, 0, act(0), nAct(0), D.view.nmask, r.template as<double>(),
+                   W0.r.template as<float>(), D.invD.template as<float>(), W0.d.template as<float>(), W0.z.template as<float>(), D.cf0, bs(),
+                   none);
+            const float* z32 = vcycle(0, none, false, true);
+            launch(dev::kb_vc_store<RB>, elemGrid(0), dev::BLOCK_THREADS, 0, act(0), nAct(0), z32, q.template as<double>(), bs());
+            pack(zDev, nvec, q.template as<double>(), false);
+        }
+        check(cudaGetLastError(), "block precondition");
+        if (caller && caller != stream) {
+            check(cudaEventRecord(ev, stream), "event");
+            check(cudaStreamWaitEvent(caller, ev, 0), "wait");
+        }
+    }
+};
+
 // ==================================================================== Solver
 
 struct SolverHandle {
     std::shared_ptr<SharedModel> model;
     std::unique_ptr<SolverImpl> main;
     std::vector<std::unique_ptr<SolverImpl>> extra;  // batch contexts, created on demand
+    std::unique_ptr<BlockBase> block;                // the multi-RHS block context, created on demand
 };
+
+namespace {
+
+// the block width for nrhs right-hand sides: the narrowest of 8, 16, 32 that holds them (or 32),
+// narrowed while its vectors do not fit the free device memory (less 1 GB); 0 if none fits
+int chooseBlockWidth(const Hierarchy& H, int nrhs) {
+    size_t freeB = 0, totalB = 0;
+    check(cudaMemGetInfo(&freeB, &totalB), "cudaMemGetInfo");
+    const int64_t avail = int64_t(freeB) - (int64_t(1) << 30);
+    int want = nrhs <= 8 ? 8 : (nrhs <= 16 ? 16 : 32);
+    for (; want >= 8; want /= 2) {
+        const int64_t need = want == 32 ? BlockImpl<32>::bytesFor(H) : (want == 16 ? BlockImpl<16>::bytesFor(H) : BlockImpl<8>::bytesFor(H));
+        if (need <= avail) return want;
+    }
+    return 0;
+}
+
+std::unique_ptr<BlockBase> makeBlock(std::shared_ptr<SharedModel> M, int width) {
+    if (width == 32) return std::make_unique<BlockImpl<32>>(std::move(M));
+    if (width == 16) return std::make_unique<BlockImpl<16>>(std::move(M));
+    return std::make_unique<BlockImpl<8>>(std::move(M));
+}
+
+}  // namespace
+
+BlockBase* Solver::blockFor(int nrhs) {
+    SolverHandle& Hd = *handle_;
+    const int fits = Hd.block ? Hd.block->width() : 0;
+    const int want = nrhs <= 8 ? 8 : (nrhs <= 16 ? 16 : 32);
+    if (Hd.block && fits >= std::min(want, 32)) return Hd.block.get();
+    Hd.block.reset();  // its memory first
+    check(cudaStreamSynchronize(impl_->stream), "sync");
+    const int w = chooseBlockWidth(impl_->H, nrhs);
+    if (!w) return nullptr;
+    impl_->prepareSmoothers();
+    Hd.block = makeBlock(impl_->M, w);
+    return Hd.block.get();
+}
 
 Solver::Solver(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsestMaxDof, const double* diagAdd) {
     int count = 0;
@@ -2341,6 +2800,7 @@ int64_t Solver::nDof() const { return impl_->H.levels[0].nDof; }
 int64_t Solver::deviceBytes() const {
     int64_t b = impl_->M->bytes + impl_->bytes;
     for (auto& c : handle_->extra) b += c->bytes;
+    if (handle_->block) b += handle_->block->deviceBytes();
     return b;
 }
 int64_t Solver::contextBytes() const { return impl_->bytes; }
@@ -2403,6 +2863,23 @@ ps_status Solver::solveBatch(int32_t nrhs, const double* f, const ps_solve_opts&
     const int64_t n = nDof();
     validateF(f, nullptr, n * nrhs);
     if (base.x0) validateF(base.x0, nullptr, n * nrhs);
+    const char* mode = std::getenv("PSFEA_BATCH_MODE");
+    const bool contexts = mode && std::string(mode) == "contexts";
+    if (base.precision != PS_PREC_FP32 && nrhs >= 2 && !contexts) {
+        impl_->setDegree(base.smoother_degree > 0 ? base.smoother_degree : 2);
+        if (BlockBase* B = blockFor(nrhs)) {
+            ps_status worst = PS_OK;
+            for (int c = 0; c < nrhs; c += B->width()) {
+                const int k = std::min(B->width(), nrhs - c);
+                ps_solve_opts o = base;
+                o.x0 = nullptr;
+                const ps_status st = B->solve(k, f + int64_t(c) * n, base.x0 ? base.x0 + int64_t(c) * n : nullptr, true, o, u + int64_t(c) * n,
+                                              results ? results + c : nullptr);
+                if (st > worst) worst = st;
+            }
+            return worst;
+        }
+    }
     // contexts: the handle's own plus extra ones, as many as free memory allows
     size_t freeB = 0, totalB = 0;
     check(cudaMemGetInfo(&freeB, &totalB), "cudaMemGetInfo");
@@ -2485,6 +2962,18 @@ void Solver::precondition(const double* rHost, double* zHost) {
     check(cudaStreamSynchronize(I.stream), "precondition");
 }
 
+void Solver::preconditionBlock(int32_t nvec, const double* rDev, double* zDev, void* s) {
+    impl_->setDegree(2);  // the reference's preconditioner
+    BlockBase* B = blockFor(nvec);
+    if (!B) throw Error(PS_EOOM, "the block vectors do not fit the free device memory");
+    const int64_t n = nDof();
+    cudaStream_t caller = s ? static_cast<cudaStream_t>(s) : impl_->stream;
+    for (int c = 0; c < nvec; c += B->width()) {
+        const int k = std::min(B->width(), nvec - c);
+        B->precondition(k, rDev + int64_t(c) * n, zDev + int64_t(c) * n, caller);
+    }
+}
+
 void Solver::setStream(void* s) {
     SolverImpl& I = *impl_;
     cudaStream_t want = s ? static_cast<cudaStream_t>(s) : I.ownStream;
@@ -2523,6 +3012,7 @@ double Solver::timeKernel(int which, int reps) {
 int64_t Solver::launches() const {
     int64_t n = impl_->launches;
     for (auto& c : handle_->extra) n += c->launches;
+    if (handle_->block) n += handle_->block->launchCount();
     return n;
 }
 

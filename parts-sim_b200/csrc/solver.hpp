@@ -11,6 +11,7 @@ namespace psfea {
 
 struct SolverImpl;
 struct SolverHandle;
+struct BlockBase;
 
 class Solver {
 public:
@@ -30,9 +31,13 @@ public:
     ps_status solve(const double* f, const ps_solve_opts& o, double* u, ps_solve_result& res);
     // device vectors in/out (o.x0 is a device pointer)
     ps_status solveDevice(const double* fDev, const ps_solve_opts& o, double* uDev, ps_solve_result& res);
-    // nrhs solves on this hierarchy, up to `concurrency` at once on separate streams (each solve its
-    // own context), refilled as solves finish
+    // nrhs solves on this hierarchy: in blocks of up to 32 right-hand sides whose kernels take the
+    // whole block (FP64-Krylov forms), or up to `concurrency` at once on separate streams, each its
+    // own context (the FP32-Krylov form, or PSFEA_BATCH_MODE=contexts)
     ps_status solveBatch(int32_t nrhs, const double* f, const ps_solve_opts& o, double* u, ps_solve_result* results, int concurrency);
+    // z_k = one V-cycle applied to r_k for nvec dense device vectors (consecutive), in blocks of up
+    // to 32; stream-ordered on s (nullptr = the handle's stream)
+    void preconditionBlock(int32_t nvec, const double* rDev, double* zDev, void* s);
     // non-blocking solve for a serving loop: begin() enqueues it (f and u stay valid until poll()
     // returns true), poll() moves it on without waiting for the GPU
     void begin(const double* fHost, const ps_solve_opts& o, double* uHost);
@@ -52,6 +57,7 @@ public:
     void applyDotStatic(const double* xDev, double* yDev, double* dotDev, void* s);
 
 private:
+    BlockBase* blockFor(int nrhs);  // the block context for nrhs right-hand sides (null: none fits)
     std::unique_ptr<SolverImpl> impl_;
     std::unique_ptr<SolverHandle> handle_;
 };

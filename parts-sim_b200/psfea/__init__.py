@@ -75,6 +75,7 @@ _solve = _sig("ps_fea_solve", C.c_int, _P, _F64P, C.POINTER(SolveOpts), _F64P, C
 _solve_dev = _sig("ps_fea_solve_dev", C.c_int, _P, C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.POINTER(SolveResultC))
 _solve_batch = _sig("ps_fea_solve_batch", C.c_int, _P, C.c_int32, _F64P, C.POINTER(SolveOpts), _F64P, C.c_void_p)
 _precondition = _sig("ps_fea_precondition", C.c_int, _P, _F64P, _F64P)
+_precondition_block = _sig("ps_fea_precondition_block", C.c_int, _P, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p)
 _apply = _sig("ps_fea_apply", C.c_int, _P, C.c_int32, _F64P, _F64P, C.c_int32)
 _stresses = _sig("ps_fea_stresses", C.c_int, _P, _F64P, C.c_double, C.c_double, C.c_int32, _F32P, C.c_void_p, C.c_void_p)
 _reactions = _sig("ps_fea_reactions", C.c_int, _P, _F64P, C.c_void_p, _F64P)
@@ -113,7 +114,7 @@ EXPORTS = ("ps_solve_opts_default", "ps_fea_create", "ps_fea_solve", "ps_fea_sol
            "ps_fea_level_fixed", "ps_fea_level_lmax", "ps_fea_device_bytes", "ps_fea_destroy", "ps_element_matrix",
            "ps_prune_floating", "ps_last_error", "ps_hierarchy_create", "ps_hierarchy_num_levels", "ps_hierarchy_level_info",
            "ps_hierarchy_level_fixed", "ps_hierarchy_level_own", "ps_hierarchy_level_kb", "ps_hierarchy_destroy",
-           "ps_fea_set_stream", "ps_fea_time_kernel", "ps_fea_kernel_launches", "ps_fea_apply_dot_noalloc",
+           "ps_fea_set_stream", "ps_fea_time_kernel", "ps_fea_kernel_launches", "ps_fea_apply_dot_noalloc", "ps_fea_precondition_block",
            "ps_server_create", "ps_server_submit", "ps_server_poll", "ps_server_wait", "ps_server_release", "ps_server_get_stats",
            "ps_server_destroy")
 
@@ -323,6 +324,20 @@ class VoxelFEA:
         if st != PS_OK:
             _raise(st)
         return z
+
+    def precondition_block(self, nvec, r_ptr, z_ptr, stream_ptr=None):
+        """z_k = V-cycle preconditioner of r_k for nvec consecutive device vectors (pointers, e.g.
+        ``tensor.data_ptr()``); stream-ordered on stream_ptr (0: the legacy default stream, None:
+        the handle's stream), returns before the GPU has finished."""
+        if stream_ptr is None:
+            stream = None
+        elif stream_ptr == 0:
+            stream = C.c_void_p(CUDA_STREAM_LEGACY)
+        else:
+            stream = C.c_void_p(stream_ptr)
+        st = _precondition_block(self.h, int(nvec), C.c_void_p(r_ptr), C.c_void_p(z_ptr), stream)
+        if st != PS_OK:
+            _raise(st)
 
     def apply(self, x, level=0, raw=False):
         x = np.ascontiguousarray(x, np.float64).ravel()

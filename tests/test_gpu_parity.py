@@ -179,7 +179,10 @@ def test_device_pointer_solve_on_a_caller_stream(precision):
     S.set_stream(0)
 
 
-def test_solve_batch_matches_single():
+def test_solve_batch_contexts_match_single(monkeypatch):
+    """The batch as concurrent single-solve contexts (the FP32-Krylov form's batch, and any form's
+    with PSFEA_BATCH_MODE=contexts): each result is the single solve's."""
+    monkeypatch.setenv("PSFEA_BATCH_MODE", "contexts")
     m = W.simp(16, 8, 8, nrhs=3)
     S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc)
     rs = S.solve_batch(m.f, tol=1e-8, max_iter=3000)
