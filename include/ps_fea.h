@@ -207,6 +207,66 @@ ps_status ps_element_matrix(double nu, double K[576], double* corner_stress);
 ps_status ps_prune_floating(const int32_t dims[3], const float* density, const uint8_t* held_node,
                             float* out, int32_t* removed);
 
+/* ---- Study loops on the device: the solve of every iteration warm-started from the previous
+ * displacements in device memory, the loops' per-voxel work (density filter, element energies,
+ * optimality-criteria update and its volume bisection, failure measure) as kernels beside it. */
+
+typedef struct ps_topology_opts {
+    double vol_frac;     /* volume budget, fraction of the design domain (0.4) */
+    double penal;        /* SIMP penalty p (3) */
+    double rmin;         /* density-filter radius in voxels (1.5) */
+    double move;         /* optimality-criteria move limit (0.2) */
+    double tol;          /* stop once the largest design change is below it, after 5 iterations (0.01) */
+    int32_t max_iter;    /* 40 */
+    double solve_tol;    /* relative residual of each iteration's solve (1e-5, study_runner.cpp:413) */
+    int32_t precision;   /* ps_precision of the solves */
+} ps_topology_opts;
+
+typedef struct ps_topology_step {
+    int32_t it;
+    int32_t solve_iterations;
+    int32_t solve_status;  /* ps_status of the iteration's solve */
+    double compliance;     /* f . u */
+    double volume;         /* used volume / design volume */
+    double change;         /* largest design change of the previous update */
+    double seconds;
+} ps_topology_step;
+
+/* defaults of native/src/fea/topology.hpp:38-48 */
+void ps_topology_opts_default(ps_topology_opts* opts);
+
+/* SIMP compliance minimisation (optimizeTopology, native/src/fea/topology.cpp:103-183): design
+ * voxels are those with fill > 0 (fill: nx ny nz values in (0, 1]); keep (or NULL) marks voxels
+ * that stay solid; bc and f as for ps_fea_create / ps_fea_solve. density_out: nx ny nz final
+ * physical densities; history: opts->max_iter entries, *n_steps of them filled. */
+ps_status ps_topology_run(const int32_t dims[3], const float* fill, const uint8_t* keep, double nu, const uint8_t* bc, const double* f,
+                          const ps_topology_opts* opts, float* density_out, ps_topology_step* history, int32_t* n_steps);
+
+typedef enum ps_break_reason {
+    PS_BREAK_STEP_LIMIT = 0, PS_BREAK_SEPARATED = 1, PS_BREAK_UNSUPPORTED = 2, PS_BREAK_NOT_CONVERGED = 3, PS_BREAK_NO_STRESS = 4
+} ps_break_reason;
+
+typedef struct ps_break_step {
+    int32_t step;
+    int32_t voxels;            /* solved voxels */
+    int32_t solve_iterations;
+    int32_t cracked;           /* voxels removed as failed in this step */
+    int32_t detached;          /* voxels that fell off with them (pruned) */
+    double lambda;             /* load factor at which the most stressed voxel reaches the strength */
+    double max_disp;           /* largest displacement magnitude at that load factor [m] */
+    double seconds;
+} ps_break_step;
+
+/* Progressive failure (breakTest, native/src/fea/static_study.cpp:199-279): solve (warm-started),
+ * nodal von Mises (principal = 0) or first principal stress, voxel measure = worst corner stress,
+ * the most stressed voxels (within 5 % of the peak, at most 2 % of n^(2/3)) removed, floating parts
+ * pruned, repeat for max_steps. steps: max_steps entries, *n_steps filled; cracked (or NULL): the
+ * removed voxels of all steps in order, room for cracked_cap; density_out: the density left;
+ * *peak: the largest load factor; *reason: ps_break_reason. E [Pa] and h [m] scale the stresses. */
+ps_status ps_break_test(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, const double* f, double E, double h,
+                        double strength, int32_t principal, int32_t max_steps, ps_break_step* steps, int32_t* n_steps, int32_t* cracked,
+                        int64_t cracked_cap, float* density_out, double* peak, int32_t* reason);
+
 /* ---- Serving: many independent solves on one GPU with continuous batching (no counterpart in the
  * reference, which runs one job at a time behind a GPU lock, native/src/gpu/gpu.hpp:43).
  * Requests are submitted at any time; host threads build their hierarchies; a scheduler admits

@@ -247,6 +247,30 @@ def element(kind, nu, modes=True):
     return K.reshape(24, 24), cs.reshape(8, 6, 24), gb.reshape(8, 6, 24)
 
 
+def topology(dims, fill, nu, bc, f, keep=None, vol_frac=0.4, penal=3.0, rmin=1.5, move=0.2, tol=0.01, max_iter=40, solve_tol=1e-5):
+    """The reference's own optimizeTopology (native/src/fea/topology.cpp:103-183) with runTopology's
+    solve (study_runner.cpp:403-419): (final density, [(it, compliance, volume, change), ...])."""
+    path, _ = _LIBS["reference"]
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"oracle library {path} is not built (make -C oracle REF=...)")
+    lib = C.CDLL(path)
+    fn = lib.ref_topology
+    fn.restype = C.c_int
+    fn.argtypes = [_I32P, _F32P, C.c_void_p, C.c_double, _U8P, _F64P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                   C.c_double, _F32P, _F64P, C.POINTER(C.c_int), C.c_char_p, C.c_int]
+    fill = np.ascontiguousarray(fill, np.float32).ravel()
+    keep = None if keep is None else np.ascontiguousarray(keep, np.uint8).ravel()
+    out = np.zeros_like(fill)
+    hist = np.zeros(4 * max(1, max_iter), np.float64)
+    n = C.c_int()
+    err = C.create_string_buffer(512)
+    rc = fn(np.asarray(dims, np.int32), fill, _ptr(keep), float(nu), np.ascontiguousarray(bc, np.uint8).ravel(),
+            np.ascontiguousarray(f, np.float64).ravel(), vol_frac, penal, rmin, move, tol, int(max_iter), solve_tol, out, hist, C.byref(n), err, 512)
+    if rc:
+        raise ValueError(err.value.decode())
+    return out, [tuple(hist[4 * k:4 * k + 4]) for k in range(n.value)]
+
+
 def prune(kind, dims, density, held_node):
     L = _lib(kind)
     density = np.ascontiguousarray(density, np.float32).ravel()

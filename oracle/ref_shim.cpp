@@ -8,7 +8,10 @@
 #include <stdexcept>
 #include <vector>
 
+#include <memory>
+
 #include "fea/hex8.hpp"
+#include "fea/topology.hpp"
 #include "fea/voxel_fea.hpp"
 
 extern "C" {
@@ -127,6 +130,54 @@ int ref_prune(const int32_t dims[3], const float* density, const uint8_t* heldNo
     const auto r = ps::pruneFloating({dims[0], dims[1], dims[2]}, d, held);
     std::memcpy(out, r.density.data(), size_t(nE) * 4);
     return r.removed;
+}
+
+// optimizeTopology (native/src/fea/topology.cpp:103-183) with the solve of runTopology
+// (native/src/fea/study_runner.cpp:403-419: a fresh VoxelFEA per iteration, coarsest 1100 DOFs,
+// tol solveTol, 3000 iterations, warm start). hist: maxIter rows of (it, compliance, volume, change).
+int ref_topology(const int32_t dims[3], const float* fill, const uint8_t* keep, double nu, const uint8_t* bc, const double* f, double volFrac,
+                 double penal, double rmin, double move, double tol, int maxIter, double solveTol, float* densityOut, double* hist, int* nHist,
+                 char* err, int errlen) {
+    try {
+        const int64_t nE = int64_t(dims[0]) * dims[1] * dims[2];
+        const int64_t nDof = 3 * int64_t(dims[0] + 1) * (dims[1] + 1) * (dims[2] + 1);
+        ps::TopologyOptions o;
+        o.dims = {dims[0], dims[1], dims[2]};
+        o.fill.assign(fill, fill + nE);
+        o.keep.assign(size_t(nE), 0);
+        if (keep) o.keep.assign(keep, keep + nE);
+        o.volFrac = volFrac;
+        o.penal = penal;
+        o.rmin = rmin;
+        o.move = move;
+        o.tol = tol;
+        o.maxIter = maxIter;
+        const std::vector<uint8_t> bcv(bc, bc + nDof);
+        const std::vector<double> fv(f, f + nDof);
+        std::unique_ptr<ps::VoxelFEA> fea;
+        o.solve = [&](const std::vector<float>& density, const std::vector<double>* x0) {
+            fea = std::make_unique<ps::VoxelFEA>(o.dims, density, nu, bcv, 1100);
+            ps::SolveOptions so;
+            so.tol = solveTol;
+            so.maxIter = 3000;
+            so.x0 = x0;
+            auto sol = fea->solve(fv, so);
+            return ps::TopologySolve{std::move(sol.u), fv, fea.get()};
+        };
+        const auto res = ps::optimizeTopology(o);
+        std::memcpy(densityOut, res.density.data(), size_t(nE) * 4);
+        *nHist = int(res.history.size());
+        for (size_t k = 0; k < res.history.size(); k++) {
+            hist[4 * k] = res.history[k].it;
+            hist[4 * k + 1] = res.history[k].compliance;
+            hist[4 * k + 2] = res.history[k].volume;
+            hist[4 * k + 3] = res.history[k].change;
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        setErr(err, errlen, e.what());
+        return 1;
+    }
 }
 
 }  // extern "C"

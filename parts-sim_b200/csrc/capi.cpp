@@ -10,6 +10,7 @@
 #include "host_util.hpp"
 #include "ps_fea.h"
 #include "solver.hpp"
+#include "study.hpp"
 
 struct ps_fea {
     psfea::Solver solver;
@@ -123,6 +124,77 @@ ps_status ps_fea_precondition(ps_fea_t* h, const double* r, double* z) {
     return guarded([&] {
         if (!h || !r || !z) return fail(PS_EINVAL, "NULL vector");
         h->solver.precondition(r, z);
+        return PS_OK;
+    });
+}
+
+void ps_topology_opts_default(ps_topology_opts* o) {
+    if (!o) return;
+    const psfea::TopologyOptions d;
+    o->vol_frac = d.volFrac;
+    o->penal = d.penal;
+    o->rmin = d.rmin;
+    o->move = d.move;
+    o->tol = d.tol;
+    o->max_iter = d.maxIter;
+    o->solve_tol = d.solveTol;
+    o->precision = d.precision;
+}
+
+ps_status ps_topology_run(const int32_t dims[3], const float* fill, const uint8_t* keep, double nu, const uint8_t* bc, const double* f,
+                          const ps_topology_opts* opts, float* density_out, ps_topology_step* history, int32_t* n_steps) {
+    return guarded([&] {
+        if (!dims || !fill || !bc || !f || !density_out) return fail(PS_EINVAL, "NULL argument");
+        ps_topology_opts o;
+        ps_topology_opts_default(&o);
+        if (opts) o = *opts;
+        if (!(o.vol_frac > 0 && o.vol_frac <= 1) || !(o.penal >= 1) || !(o.rmin > 0) || !(o.move > 0) || o.max_iter < 0 || !(o.solve_tol > 0) ||
+            o.precision < PS_PREC_FP64 || o.precision > PS_PREC_FP32)
+            return fail(PS_EINVAL, "invalid topology options");
+        if (!psfea::deviceAvailable()) return fail(PS_ENODEV, "no CUDA device is available");
+        psfea::TopologyOptions to;
+        to.volFrac = o.vol_frac;
+        to.penal = o.penal;
+        to.rmin = o.rmin;
+        to.move = o.move;
+        to.tol = o.tol;
+        to.maxIter = o.max_iter;
+        to.solveTol = o.solve_tol;
+        to.precision = o.precision;
+        std::vector<psfea::TopologyStep> hist;
+        psfea::topologyRun(dims, fill, keep, nu, bc, f, to, density_out, hist);
+        for (size_t k = 0; k < hist.size(); k++)
+            if (history)
+                history[k] = ps_topology_step{hist[k].it, hist[k].solveIterations, hist[k].solveStatus, hist[k].compliance, hist[k].volume,
+                                              hist[k].change, hist[k].seconds};
+        if (n_steps) *n_steps = int32_t(hist.size());
+        return PS_OK;
+    });
+}
+
+ps_status ps_break_test(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, const double* f, double E, double h,
+                        double strength, int32_t principal, int32_t max_steps, ps_break_step* steps, int32_t* n_steps, int32_t* cracked,
+                        int64_t cracked_cap, float* density_out, double* peak, int32_t* reason) {
+    return guarded([&] {
+        if (!dims || !density || !bc || !f || !density_out || max_steps < 0) return fail(PS_EINVAL, "NULL argument");
+        if (!(E > 0) || !(h > 0)) return fail(PS_EINVAL, "E and h must be positive");
+        if (!(strength > 0)) return fail(PS_EINVAL, "Failure strength must be positive.");
+        if (!psfea::deviceAvailable()) return fail(PS_ENODEV, "no CUDA device is available");
+        std::vector<psfea::BreakStep> st;
+        double pk = 0;
+        const psfea::BreakReason why =
+            psfea::breakTest(dims, density, nu, bc, f, E, h, strength, principal != 0, max_steps, st, density_out, pk);
+        int64_t at = 0;
+        for (size_t k = 0; k < st.size(); k++) {
+            if (steps)
+                steps[k] = ps_break_step{st[k].step, st[k].voxels, st[k].solveIterations, int32_t(st[k].cracked.size()),
+                                         int32_t(st[k].detached.size()), st[k].lambda, st[k].maxDisp, st[k].seconds};
+            for (int e : st[k].cracked)
+                if (cracked && at < cracked_cap) cracked[at++] = e;
+        }
+        if (n_steps) *n_steps = int32_t(st.size());
+        if (peak) *peak = pk;
+        if (reason) *reason = int32_t(why);
         return PS_OK;
     });
 }

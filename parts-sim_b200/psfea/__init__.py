@@ -45,6 +45,24 @@ class PsRequestResult(C.Structure):
                 ("total_s", C.c_double)]
 
 
+class TopologyOpts(C.Structure):
+    _fields_ = [("vol_frac", C.c_double), ("penal", C.c_double), ("rmin", C.c_double), ("move", C.c_double), ("tol", C.c_double),
+                ("max_iter", C.c_int32), ("solve_tol", C.c_double), ("precision", C.c_int32)]
+
+
+class TopologyStepC(C.Structure):
+    _fields_ = [("it", C.c_int32), ("solve_iterations", C.c_int32), ("solve_status", C.c_int32), ("compliance", C.c_double),
+                ("volume", C.c_double), ("change", C.c_double), ("seconds", C.c_double)]
+
+
+class BreakStepC(C.Structure):
+    _fields_ = [("step", C.c_int32), ("voxels", C.c_int32), ("solve_iterations", C.c_int32), ("cracked", C.c_int32), ("detached", C.c_int32),
+                ("lambda_", C.c_double), ("max_disp", C.c_double), ("seconds", C.c_double)]
+
+
+BREAK_REASONS = {0: "step limit", 1: "separated", 2: "unsupported load", 3: "solver did not converge", 4: "no stress"}
+
+
 class PsServerStats(C.Structure):
     _fields_ = [("queued", C.c_int64), ("active", C.c_int64), ("completed", C.c_int64), ("device_bytes_in_use", C.c_int64),
                 ("peak_device_bytes", C.c_int64), ("budget_bytes", C.c_int64), ("peak_active", C.c_int64)]
@@ -97,6 +115,11 @@ _srv_stats = _sig("ps_server_get_stats", C.c_int, _P, C.POINTER(PsServerStats))
 _srv_destroy = _sig("ps_server_destroy", None, _P)
 _apply_dot_noalloc = _sig("ps_fea_apply_dot_noalloc", C.c_int, _P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
 _element = _sig("ps_element_matrix", C.c_int, C.c_double, _F64P, C.c_void_p)
+_topo_default = _sig("ps_topology_opts_default", None, C.POINTER(TopologyOpts))
+_topo_run = _sig("ps_topology_run", C.c_int, _I32P, _F32P, C.c_void_p, C.c_double, _U8P, _F64P, C.POINTER(TopologyOpts), _F32P, C.c_void_p,
+                 C.POINTER(C.c_int32))
+_break_test = _sig("ps_break_test", C.c_int, _I32P, _F32P, C.c_double, _U8P, _F64P, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                   C.c_void_p, C.POINTER(C.c_int32), C.c_void_p, C.c_int64, _F32P, C.POINTER(C.c_double), C.POINTER(C.c_int32))
 _prune = _sig("ps_prune_floating", C.c_int, _I32P, _F32P, _U8P, _F32P, C.POINTER(C.c_int32))
 _last_error = _sig("ps_last_error", C.c_char_p)
 _opts_default = _sig("ps_solve_opts_default", None, C.POINTER(SolveOpts))
@@ -115,6 +138,7 @@ EXPORTS = ("ps_solve_opts_default", "ps_fea_create", "ps_fea_solve", "ps_fea_sol
            "ps_prune_floating", "ps_last_error", "ps_hierarchy_create", "ps_hierarchy_num_levels", "ps_hierarchy_level_info",
            "ps_hierarchy_level_fixed", "ps_hierarchy_level_own", "ps_hierarchy_level_kb", "ps_hierarchy_destroy",
            "ps_fea_set_stream", "ps_fea_time_kernel", "ps_fea_kernel_launches", "ps_fea_apply_dot_noalloc", "ps_fea_precondition_block",
+           "ps_topology_opts_default", "ps_topology_run", "ps_break_test",
            "ps_server_create", "ps_server_submit", "ps_server_poll", "ps_server_wait", "ps_server_release", "ps_server_get_stats",
            "ps_server_destroy")
 
@@ -439,6 +463,59 @@ def prune_floating(dims, density, held_node):
     if st != PS_OK:
         _raise(st)
     return out, int(removed.value)
+
+
+def topology_run(dims, fill, nu, bc, f, keep=None, vol_frac=0.4, penal=3.0, rmin=1.5, move=0.2, tol=0.01, max_iter=40, solve_tol=1e-5,
+                 precision="fp64"):
+    """SIMP topology optimisation on the device (the reference's optimizeTopology,
+    native/src/fea/topology.cpp:103-183). Returns (density, history): the final physical density per
+    voxel and one dict per iteration (it, compliance, volume, change, solve_iterations, seconds)."""
+    dims = np.ascontiguousarray(dims, np.int32)
+    fill = np.ascontiguousarray(fill, np.float32).ravel()
+    bc = np.ascontiguousarray(bc, np.uint8).ravel()
+    f = np.ascontiguousarray(f, np.float64).ravel()
+    keep = None if keep is None else np.ascontiguousarray(keep, np.uint8).ravel()
+    o = TopologyOpts()
+    _topo_default(C.byref(o))
+    o.vol_frac, o.penal, o.rmin, o.move, o.tol = float(vol_frac), float(penal), float(rmin), float(move), float(tol)
+    o.max_iter, o.solve_tol = int(max_iter), float(solve_tol)
+    o.precision = PREC[precision] if isinstance(precision, str) else int(precision)
+    out = np.zeros(fill.size, np.float32)
+    hist = (TopologyStepC * max(1, int(max_iter)))()
+    n = C.c_int32()
+    st = _topo_run(dims, fill, _ptr(keep), float(nu), bc, f, C.byref(o), out, C.cast(hist, C.c_void_p), C.byref(n))
+    if st != PS_OK:
+        _raise(st)
+    return out, [{k: getattr(hist[q], k) for k, _ in TopologyStepC._fields_} for q in range(n.value)]
+
+
+def break_test(dims, density, nu, bc, f, E, h, strength, principal=False, max_steps=10, cracked_cap=1 << 20):
+    """Progressive failure on the device (the reference's breakTest, native/src/fea/static_study.cpp:
+    199-279). Returns a dict: steps (one dict each), cracked (voxel lists per step), density left,
+    peak load factor and the stop reason."""
+    dims = np.ascontiguousarray(dims, np.int32)
+    density = np.ascontiguousarray(density, np.float32).ravel()
+    bc = np.ascontiguousarray(bc, np.uint8).ravel()
+    f = np.ascontiguousarray(f, np.float64).ravel()
+    steps = (BreakStepC * max(1, int(max_steps)))()
+    n = C.c_int32()
+    cracked = np.zeros(int(cracked_cap), np.int32)
+    out = np.zeros_like(density)
+    peak = C.c_double()
+    reason = C.c_int32()
+    st = _break_test(dims, density, float(nu), bc, f, float(E), float(h), float(strength), int(bool(principal)), int(max_steps),
+                     C.cast(steps, C.c_void_p), C.byref(n), cracked.ctypes.data_as(C.c_void_p), int(cracked_cap), out, C.byref(peak),
+                     C.byref(reason))
+    if st != PS_OK:
+        _raise(st)
+    rows, lists, at = [], [], 0
+    for q in range(n.value):
+        s = steps[q]
+        rows.append({"step": s.step, "voxels": s.voxels, "solve_iterations": s.solve_iterations, "cracked": s.cracked, "detached": s.detached,
+                     "lambda": s.lambda_, "max_disp": s.max_disp, "seconds": s.seconds})
+        lists.append(cracked[at:at + s.cracked].copy())
+        at += s.cracked
+    return {"steps": rows, "cracked": lists, "density": out, "peak": peak.value, "reason": BREAK_REASONS.get(reason.value, str(reason.value))}
 
 
 class Server:

@@ -144,3 +144,22 @@ def test_server_needs_a_device(have_gpu):
         pytest.skip("a GPU is present")
     with pytest.raises(psfea.SolverError, match="ENODEV"):
         psfea.Server()
+
+
+def test_study_loops_validate_their_inputs_then_need_a_device(have_gpu):
+    """The study entry points reject invalid options with the reference's messages before they
+    look for a device (topology.hpp:38-48; static_study.cpp:201)."""
+    if have_gpu:
+        pytest.skip("a GPU is present")
+    m = W.cantilever(8, 2, 2, coarsest_max_dof=1100)
+    fill = np.ones(8 * 2 * 2, np.float32)
+    with pytest.raises(ValueError, match="invalid topology options"):
+        psfea.topology_run(m.dims, fill, m.nu, m.bc, m.f, vol_frac=0)
+    with pytest.raises(ValueError, match="invalid topology options"):
+        psfea.topology_run(m.dims, fill, m.nu, m.bc, m.f, rmin=-1)
+    with pytest.raises(psfea.SolverError, match="ENODEV"):
+        psfea.topology_run(m.dims, fill, m.nu, m.bc, m.f, max_iter=2)
+    with pytest.raises(ValueError, match="Failure strength must be positive"):
+        psfea.break_test(m.dims, m.density, m.nu, m.bc, m.f, 200e9, 1e-3, strength=0)
+    with pytest.raises(psfea.SolverError, match="ENODEV"):
+        psfea.break_test(m.dims, m.density, m.nu, m.bc, m.f, 200e9, 1e-3, strength=100e6)
