@@ -167,6 +167,32 @@ ps_status ps_fea_time_kernel(ps_fea_t* h, int32_t which, int32_t reps, double* m
  * current (PS_EINVAL otherwise). Returns without waiting for the GPU. */
 ps_status ps_fea_apply_dot_noalloc(ps_fea_t* h, const double* x_dev, double* y_dev, double* dot_dev, void* cuda_stream);
 
+/* ---- Autotuning (no counterpart in the reference, which fixes a degree-2 Chebyshev smoother,
+ * voxel_fea.cpp:692-725, and the coarsest size, voxel_fea.cpp:174-180) */
+typedef struct ps_tune_result {
+    int32_t smoother_degree;   /* chosen Chebyshev degree per V-cycle half (1-4) */
+    int32_t inner64;           /* the finest level's FP64 tiles compute their boundary nodes in the tile */
+    int64_t split_levels;      /* bit l: level l's FP32 tiles leave boundary nodes to the list kernel */
+    int64_t coarsest_max_dof;  /* ps_fea_create_tuned: the chosen coarsening depth (else 0) */
+    int32_t trials;            /* solves timed (0: taken from the process's cache of tuned models) */
+    int32_t cached;
+    double best_seconds;       /* solve time of the chosen configuration */
+    double default_seconds;    /* solve time of the configuration before tuning */
+} ps_tune_result;
+
+#define PS_TUNE_FORCE 1        /* ignore the cache of tuned models */
+
+/* Times complete solves of f (host, nDof values) to opts->tol over smoother degrees 1-4 and the
+ * tile-path choices of the tiled levels, keeps the fastest configuration on the handle (solves whose
+ * smoother_degree is 0 use the tuned degree) and caches it for models with the same voxel words,
+ * masks and depth. opts->precision and max_iter apply to the trials. */
+ps_status ps_fea_autotune(ps_fea_t* h, const double* f, const ps_solve_opts* opts, int32_t flags, ps_tune_result* out);
+
+/* ps_fea_create for several coarsening depths (coarsest_max_dof 300, 1100 and 3000, the last the
+ * largest dense coarsest solve the hierarchy takes), each autotuned on f; keeps the fastest handle. */
+ps_status ps_fea_create_tuned(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, const double* diag_add,
+                              const double* f, const ps_solve_opts* opts, int32_t flags, ps_tune_result* out, ps_fea_t** handle);
+
 /* Device kernels the handle has launched since it was created. */
 int64_t ps_fea_kernel_launches(const ps_fea_t* h);
 

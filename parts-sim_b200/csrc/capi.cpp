@@ -199,6 +199,73 @@ ps_status ps_break_test(const int32_t dims[3], const float* density, double nu, 
     });
 }
 
+namespace {
+void toC(const psfea::TuneResult& t, int64_t coarsest, ps_tune_result* out) {
+    if (!out) return;
+    out->smoother_degree = t.degree;
+    out->inner64 = t.inner64;
+    out->split_levels = t.splitLevels;
+    out->coarsest_max_dof = coarsest;
+    out->trials = t.trials;
+    out->cached = t.cached;
+    out->best_seconds = t.bestSeconds;
+    out->default_seconds = t.defaultSeconds;
+}
+bool validOpts(const ps_solve_opts& o) {
+    return o.tol >= 0 && o.max_iter >= 0 && o.precision >= PS_PREC_FP64 && o.precision <= PS_PREC_FP32 && o.smoother_degree >= 0 &&
+           o.smoother_degree <= 8;
+}
+}  // namespace
+
+ps_status ps_fea_autotune(ps_fea_t* h, const double* f, const ps_solve_opts* opts, int32_t flags, ps_tune_result* out) {
+    return guarded([&] {
+        if (!h || !f) return fail(PS_EINVAL, "NULL argument");
+        const ps_solve_opts o = resolve(opts);
+        if (!validOpts(o)) return fail(PS_EINVAL, "invalid solve options");
+        toC(h->solver.autotune(f, o, (flags & PS_TUNE_FORCE) != 0), 0, out);
+        return PS_OK;
+    });
+}
+
+ps_status ps_fea_create_tuned(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, const double* diag_add,
+                              const double* f, const ps_solve_opts* opts, int32_t flags, ps_tune_result* out, ps_fea_t** handle) {
+    return guarded([&] {
+        if (!handle || !f) return fail(PS_EINVAL, "NULL argument");
+        *handle = nullptr;
+        if (!dims) return fail(PS_EINVAL, "The structural grid must have three positive dimensions.");
+        const ps_solve_opts o = resolve(opts);
+        if (!validOpts(o)) return fail(PS_EINVAL, "invalid solve options");
+        ps_fea_t* best = nullptr;
+        psfea::TuneResult bestT;
+        int64_t bestC = 0;
+        int32_t levelsSeen[3] = {-1, -1, -1};
+        const int64_t depths[3] = {300, 1100, 3000};
+        for (int c = 0; c < 3; c++) {
+            auto* cand = new ps_fea(dims, density, nu, bc, depths[c], diag_add);
+            const int32_t nl = int32_t(cand->solver.hierarchy().levels.size());
+            bool same = false;
+            for (int k = 0; k < c; k++) same = same || levelsSeen[k] == nl;  // the same hierarchy as a depth already timed
+            levelsSeen[c] = nl;
+            if (same) {
+                delete cand;
+                continue;
+            }
+            const psfea::TuneResult t = cand->solver.autotune(f, o, (flags & PS_TUNE_FORCE) != 0);
+            if (!best || t.bestSeconds < bestT.bestSeconds) {
+                delete best;
+                best = cand;
+                bestT = t;
+                bestC = depths[c];
+            } else {
+                delete cand;
+            }
+        }
+        toC(bestT, bestC, out);
+        *handle = best;
+        return PS_OK;
+    });
+}
+
 ps_status ps_fea_precondition_block(ps_fea_t* h, int32_t nvec, const double* r_dev, double* z_dev, void* cuda_stream) {
     return guarded([&] {
         if (!h || nvec < 0 || (nvec > 0 && (!r_dev || !z_dev))) return fail(PS_EINVAL, "NULL vector");

@@ -1367,6 +1367,7 @@ struct SharedModel {
     // smoother coefficients (shared; `version` changes whenever they do, so contexts re-record)
     bool smoothersReady = false;
     int degree = 2;  // Chebyshev smoother degree (the reference's is 2)
+    int defaultDegree = 2;  // the degree of solves that leave it open (an autotuned model's choice)
     int64_t version = 0;
     // FP16 own matrices (mixed precision) may be applied to neighbour differences, keeping rigid
     // translations in their null space exactly despite the rounding of the entries; the mixed form
@@ -2118,7 +2119,7 @@ void SolverImpl::startSolve(const double* fDev, const double* x0Dev, const ps_so
     pend.fDev = fDev;
     pend.x0Dev = x0Dev;
     pend.active = true;
-    setDegree(o.smoother_degree > 0 ? o.smoother_degree : 2);
+    setDegree(o.smoother_degree > 0 ? o.smoother_degree : M->defaultDegree);
     if (!M->smoothersReady) {
         // the smoother bounds first: their scalars come back with an event (advance() waits for it)
         if (enqueueAllLanczos()) {
@@ -2866,7 +2867,7 @@ ps_status Solver::solveBatch(int32_t nrhs, const double* f, const ps_solve_opts&
     const char* mode = std::getenv("PSFEA_BATCH_MODE");
     const bool contexts = mode && std::string(mode) == "contexts";
     if (base.precision != PS_PREC_FP32 && nrhs >= 2 && !contexts) {
-        impl_->setDegree(base.smoother_degree > 0 ? base.smoother_degree : 2);
+        impl_->setDegree(base.smoother_degree > 0 ? base.smoother_degree : impl_->M->defaultDegree);
         if (BlockBase* B = blockFor(nrhs)) {
             ps_status worst = PS_OK;
             for (int c = 0; c < nrhs; c += B->width()) {
@@ -2911,7 +2912,7 @@ ps_status Solver::solveBatch(int32_t nrhs, const double* f, const ps_solve_opts&
         job[size_t(k)] = q;
     };
     // the smoothers are estimated once, before the contexts run side by side
-    impl_->setDegree(base.smoother_degree > 0 ? base.smoother_degree : 2);
+    impl_->setDegree(base.smoother_degree > 0 ? base.smoother_degree : impl_->M->defaultDegree);
     impl_->prepareSmoothers();
     for (int k = 0; k < K && next < nrhs; k++) startOn(k, next++);
     while (left > 0) {
@@ -3014,6 +3015,134 @@ int64_t Solver::launches() const {
     for (auto& c : handle_->extra) n += c->launches;
     if (handle_->block) n += handle_->block->launchCount();
     return n;
+}
+
+namespace {
+
+// FNV-1a over the model's level-0 voxel words and node masks, its size, nu and level count: equal
+// signatures mean the same operator, masks and hierarchy depth
+uint64_t modelSignature(const Hierarchy& H) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](const void* p, size_t n) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < n; i++) {
+            h ^= b[i];
+            h *= 1099511628211ull;
+        }
+    };
+    const HostLevel& L0 = H.levels[0];
+    const int d[3] = {L0.nx, L0.ny, L0.nz};
+    mix(d, sizeof d);
+    mix(&H.nu, sizeof H.nu);
+    const size_t nl = H.levels.size();
+    mix(&nl, sizeof nl);
+    mix(L0.word.data(), L0.word.size() * 4);
+    mix(L0.nmask.data(), L0.nmask.size());
+    return h;
+}
+
+std::mutex tuneMu;
+std::map<uint64_t, TuneResult>& tuneCache() {
+    static std::map<uint64_t, TuneResult> c;
+    return c;
+}
+
+}  // namespace
+
+TuneResult Solver::autotune(const double* fHost, const ps_solve_opts& base, bool force) {
+    SolverImpl& I = *impl_;
+    SharedModel& M = *I.M;
+    const uint64_t sig = modelSignature(I.H);
+    auto apply = [&](const TuneResult& t) {
+        M.defaultDegree = t.degree;
+        for (size_t l = 0; l < M.L.size(); l++) {
+            DevLevel& D = M.L[l];
+            if (!D.useTiles) continue;
+            D.split32 = (t.splitLevels >> l) & 1;
+            if (l == 0) D.inner64 = t.inner64 != 0;
+        }
+        M.version++;  // the iteration graphs are recorded again
+    };
+    if (!force) {
+        std::lock_guard<std::mutex> g(tuneMu);
+        auto it = tuneCache().find(sig);
+        if (it != tuneCache().end()) {
+            TuneResult t = it->second;
+            apply(t);
+            t.trials = 0;
+            t.cached = 1;
+            return t;
+        }
+    }
+    const int64_t n = nDof();
+    validateF(fHost, nullptr, n);
+    int64_t scratch = 0;
+    DevMem fDev, uDev;
+    fDev.alloc(size_t(n) * 8, scratch);
+    uDev.alloc(size_t(n) * 8, scratch);
+    check(cudaMemcpy(fDev.p, fHost, size_t(n) * 8, cudaMemcpyHostToDevice), "upload");
+    TuneResult cur;
+    cur.degree = M.defaultDegree;
+    for (size_t l = 0; l < M.L.size(); l++)
+        if (M.L[l].useTiles && M.L[l].split32) cur.splitLevels |= int64_t(1) << l;
+    cur.inner64 = (!M.L.empty() && M.L[0].inner64) ? 1 : 0;
+    int trials = 0;
+    auto timeOf = [&](const TuneResult& t) {
+        apply(t);
+        ps_solve_opts o = base;
+        o.smoother_degree = t.degree;
+        o.x0 = nullptr;
+        ps_solve_result r{};
+        I.runSolve(fDev.as<double>(), nullptr, o, uDev.as<double>(), r);  // records the graph, estimates smoothers
+        const auto t0 = std::chrono::steady_clock::now();
+        I.runSolve(fDev.as<double>(), nullptr, o, uDev.as<double>(), r);
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        trials++;
+        return r.converged ? sec : 1e300;
+    };
+    const double t0 = timeOf(cur);
+    TuneResult best = cur;
+    double bestT = t0;
+    for (int deg = 1; deg <= 4; deg++) {
+        if (deg == cur.degree) continue;
+        TuneResult t = best;
+        t.degree = deg;
+        const double s = timeOf(t);
+        if (s < bestT) {
+            bestT = s;
+            best = t;
+        }
+    }
+    // each tiled level's 32-bit split, then the finest level's 64-bit in-tile boundary nodes
+    for (size_t l = 0; l < M.L.size(); l++) {
+        if (!M.L[l].useTiles || !M.L[l].nBnd) continue;
+        TuneResult t = best;
+        t.splitLevels ^= int64_t(1) << l;
+        const double s = timeOf(t);
+        if (s < bestT) {
+            bestT = s;
+            best = t;
+        }
+    }
+    if (!M.L.empty() && M.L[0].useTiles && M.L[0].nBnd) {
+        TuneResult t = best;
+        t.inner64 ^= 1;
+        const double s = timeOf(t);
+        if (s < bestT) {
+            bestT = s;
+            best = t;
+        }
+    }
+    apply(best);
+    best.trials = trials;
+    best.bestSeconds = bestT;
+    best.defaultSeconds = t0;
+    best.cached = 0;
+    {
+        std::lock_guard<std::mutex> g(tuneMu);
+        tuneCache()[sig] = best;
+    }
+    return best;
 }
 
 void Solver::apply(int level, const double* xHost, double* yHost, bool raw) {

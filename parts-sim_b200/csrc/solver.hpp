@@ -13,6 +13,17 @@ struct SolverImpl;
 struct SolverHandle;
 struct BlockBase;
 
+// the configuration an autotune run chose for a model (and what it measured)
+struct TuneResult {
+    int degree = 2;           // Chebyshev smoother degree per V-cycle half
+    int64_t splitLevels = 0;  // bit l: level l's 32-bit tiles leave boundary nodes to the list kernel
+    int inner64 = 0;          // the finest level's 64-bit tiles compute boundary nodes in the tile
+    int trials = 0;           // solves timed (0: taken from the cache)
+    double bestSeconds = 0;   // the chosen configuration's solve time
+    double defaultSeconds = 0;  // the configuration before tuning
+    int cached = 0;
+};
+
 class Solver {
 public:
     // builds the hierarchy on the host and uploads it; throws Error
@@ -52,6 +63,11 @@ public:
     // Chebyshev step of the V-cycle, 1 = the FP64 product of the CG
     double timeKernel(int which, int reps);
     int64_t launches() const;
+    // times solves of f (host) to o.tol over smoother degrees 1-4 and the tile-path choices of the
+    // tiled levels (coordinate descent: degree first, then each tile flag), keeps the fastest
+    // configuration on this handle (solves that leave the degree open use it) and caches it by the
+    // model's signature; force: ignore the cache
+    TuneResult autotune(const double* f, const ps_solve_opts& o, bool force);
     // y = K x and x.y on the finest level, device pointers, with no allocation (scratch in a
     // static device array); stream-ordered on s (nullptr = the handle's stream), no host sync
     void applyDotStatic(const double* xDev, double* yDev, double* dotDev, void* s);

@@ -63,6 +63,14 @@ class BreakStepC(C.Structure):
 BREAK_REASONS = {0: "step limit", 1: "separated", 2: "unsupported load", 3: "solver did not converge", 4: "no stress"}
 
 
+class TuneResultC(C.Structure):
+    _fields_ = [("smoother_degree", C.c_int32), ("inner64", C.c_int32), ("split_levels", C.c_int64), ("coarsest_max_dof", C.c_int64),
+                ("trials", C.c_int32), ("cached", C.c_int32), ("best_seconds", C.c_double), ("default_seconds", C.c_double)]
+
+
+PS_TUNE_FORCE = 1
+
+
 class PsServerStats(C.Structure):
     _fields_ = [("queued", C.c_int64), ("active", C.c_int64), ("completed", C.c_int64), ("device_bytes_in_use", C.c_int64),
                 ("peak_device_bytes", C.c_int64), ("budget_bytes", C.c_int64), ("peak_active", C.c_int64)]
@@ -115,6 +123,9 @@ _srv_stats = _sig("ps_server_get_stats", C.c_int, _P, C.POINTER(PsServerStats))
 _srv_destroy = _sig("ps_server_destroy", None, _P)
 _apply_dot_noalloc = _sig("ps_fea_apply_dot_noalloc", C.c_int, _P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
 _element = _sig("ps_element_matrix", C.c_int, C.c_double, _F64P, C.c_void_p)
+_autotune = _sig("ps_fea_autotune", C.c_int, _P, _F64P, C.POINTER(SolveOpts), C.c_int32, C.POINTER(TuneResultC))
+_create_tuned = _sig("ps_fea_create_tuned", C.c_int, _I32P, _F32P, C.c_double, _U8P, C.c_void_p, _F64P, C.POINTER(SolveOpts), C.c_int32,
+                     C.POINTER(TuneResultC), C.POINTER(C.c_void_p))
 _topo_default = _sig("ps_topology_opts_default", None, C.POINTER(TopologyOpts))
 _topo_run = _sig("ps_topology_run", C.c_int, _I32P, _F32P, C.c_void_p, C.c_double, _U8P, _F64P, C.POINTER(TopologyOpts), _F32P, C.c_void_p,
                  C.POINTER(C.c_int32))
@@ -138,7 +149,7 @@ EXPORTS = ("ps_solve_opts_default", "ps_fea_create", "ps_fea_solve", "ps_fea_sol
            "ps_prune_floating", "ps_last_error", "ps_hierarchy_create", "ps_hierarchy_num_levels", "ps_hierarchy_level_info",
            "ps_hierarchy_level_fixed", "ps_hierarchy_level_own", "ps_hierarchy_level_kb", "ps_hierarchy_destroy",
            "ps_fea_set_stream", "ps_fea_time_kernel", "ps_fea_kernel_launches", "ps_fea_apply_dot_noalloc", "ps_fea_precondition_block",
-           "ps_topology_opts_default", "ps_topology_run", "ps_break_test",
+           "ps_topology_opts_default", "ps_topology_run", "ps_break_test", "ps_fea_autotune", "ps_fea_create_tuned",
            "ps_server_create", "ps_server_submit", "ps_server_poll", "ps_server_wait", "ps_server_release", "ps_server_get_stats",
            "ps_server_destroy")
 
@@ -348,6 +359,38 @@ class VoxelFEA:
         if st != PS_OK:
             _raise(st)
         return z
+
+    def autotune(self, f, tol=1e-8, max_iter=5000, precision="fp64", force=False):
+        """Times solves of f over smoother degrees and tile paths, keeps the fastest on this handle
+        (see ps_fea_autotune); returns the choice as a dict."""
+        f = self._check_vec(f, "f")
+        o = make_opts(tol, max_iter, precision)
+        t = TuneResultC()
+        st = _autotune(self.h, f, C.byref(o), PS_TUNE_FORCE if force else 0, C.byref(t))
+        if st != PS_OK:
+            _raise(st)
+        return {k: getattr(t, k) for k, _ in TuneResultC._fields_}
+
+    @classmethod
+    def create_tuned(cls, dims, density, nu, bc, f, tol=1e-8, max_iter=5000, precision="fp64", force=False, diag_add=None):
+        """A handle built for the fastest of several coarsening depths, each autotuned on f (see
+        ps_fea_create_tuned); returns (handle, choice)."""
+        self = cls.__new__(cls)
+        self.dims = np.ascontiguousarray(dims, np.int32)
+        density = np.ascontiguousarray(density, np.float32).ravel()
+        bc = np.ascontiguousarray(bc, np.uint8).ravel()
+        f = np.ascontiguousarray(f, np.float64).ravel()
+        self._diag = None if diag_add is None else np.ascontiguousarray(diag_add, np.float64).ravel()
+        o = make_opts(tol, max_iter, precision)
+        t = TuneResultC()
+        h = C.c_void_p()
+        st = _create_tuned(self.dims, density, float(nu), bc, _ptr(self._diag), f, C.byref(o), PS_TUNE_FORCE if force else 0, C.byref(t),
+                           C.byref(h))
+        if st != PS_OK:
+            _raise(st)
+        self.h = h
+        self.nu = nu
+        return self, {k: getattr(t, k) for k, _ in TuneResultC._fields_}
 
     def precondition_block(self, nvec, r_ptr, z_ptr, stream_ptr=None):
         """z_k = V-cycle preconditioner of r_k for nvec consecutive device vectors (pointers, e.g.
