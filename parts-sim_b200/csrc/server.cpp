@@ -5,10 +5,13 @@
 //   1. builder threads (host cores) build each request's multigrid hierarchy and stage its load
 //      vector and result buffer in pinned memory;
 //   2. one scheduler thread admits built requests in arrival order while their estimated device
-//      footprint fits the HBM budget and an active slot is free, uploads each to the GPU and
-//      starts its solve on its own stream (the solve is a non-blocking state machine);
-//   3. the same thread polls every active solve without waiting, launches their next iteration
-//      batches, retires finished ones (device memory freed at once) and back-fills from the queue.
+//      footprint fits the HBM budget and an active slot is free; uploader threads put each
+//      admitted hierarchy on the GPU and start its solve on its own stream (the solve is a
+//      non-blocking state machine), so uploads never hold up the running solves;
+//   3. the scheduler polls every active solve without waiting, launches their next iteration
+//      batches, retires finished ones (device memory back to the stream-ordered pool at once,
+//      which keeps it for the next request instead of returning it to the driver) and back-fills
+//      from the queue.
 // Solves of different requests therefore overlap on the device; each result is computed exactly
 // as a lone solve of the same model would be (same kernels, same launch shapes, deterministic
 // reductions).
@@ -54,7 +57,7 @@ struct Request {
     std::unique_ptr<Hierarchy> hier;
     std::unique_ptr<Solver> solver;
     int64_t need = 0;
-    enum State { QUEUED, BUILT, ACTIVE, DONE } state = QUEUED;
+    enum State { QUEUED, BUILT, ADMITTED, ACTIVE, DONE } state = QUEUED;
     ps_status status = PS_OK;
     std::string error;
     ps_solve_result res{};
@@ -69,10 +72,13 @@ struct ps_server {
     int maxActive = 0;
     int device = 0;
     std::mutex mu;
-    std::condition_variable cvBuild, cvSched, cvDone;
+    std::condition_variable cvBuild, cvSched, cvDone, cvUpload;
     std::deque<psfea::Request*> buildQueue;
     std::deque<psfea::Request*> ready;  // built, in arrival order
+    std::deque<psfea::Request*> uploads;  // admitted, waiting for an uploader
+    int uploading = 0;
     std::vector<psfea::Request*> active;
+    std::vector<std::thread> uploaders;
     std::map<int64_t, std::unique_ptr<psfea::Request>> all;
     std::vector<std::thread> builders;
     std::thread scheduler;
@@ -144,47 +150,67 @@ void builderLoop(ps_server* S) {
     }
 }
 
+// an admitted request's hierarchy to the GPU and its solve started; then it is active
+void uploaderLoop(ps_server* S) {
+    cudaSetDevice(S->device);
+    for (;;) {
+        Request* R = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cvUpload.wait(lk, [&] { return S->stop || !S->uploads.empty(); });
+            if (S->stop) return;
+            R = S->uploads.front();
+            S->uploads.pop_front();
+        }
+        try {
+            R->solver = std::make_unique<Solver>(std::move(*R->hier));
+            R->hier.reset();
+            R->solver->begin(R->fPinned, R->opts, R->uPinned);
+            std::lock_guard<std::mutex> lk(S->mu);
+            R->state = Request::ACTIVE;
+            S->uploading--;
+            S->active.push_back(R);
+            S->peakActive = std::max(S->peakActive, int(S->active.size()));
+        } catch (const Error& e) {
+            R->solver.reset();
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->uploading--;
+            S->used -= R->need;
+            fail(S, R, e.status, e.what());
+            S->cvDone.notify_all();
+        }
+        S->cvSched.notify_all();
+    }
+}
+
 void schedulerLoop(ps_server* S) {
     cudaSetDevice(S->device);
     for (;;) {
-        std::vector<Request*> admit;
+        bool admitted = false;
         {
             std::unique_lock<std::mutex> lk(S->mu);
             if (S->stop) return;
             // admission: arrival order, HBM footprint and slots; an oversized request runs alone
-            while (!S->ready.empty() && int(S->active.size() + admit.size()) < S->maxActive) {
+            while (!S->ready.empty() && int(S->active.size()) + S->uploading < S->maxActive) {
                 Request* R = S->ready.front();
-                const bool alone = S->active.empty() && admit.empty();
+                const bool alone = S->active.empty() && S->uploading == 0;
                 if (S->used + R->need > S->budget && !alone) break;
                 S->ready.pop_front();
                 S->used += R->need;
                 S->peakUsed = std::max(S->peakUsed, S->used);
-                admit.push_back(R);
+                R->state = Request::ADMITTED;
+                R->tAdmit = Clock::now();
+                S->uploading++;
+                S->uploads.push_back(R);
+                admitted = true;
             }
-            if (S->active.empty() && admit.empty()) {
-                S->cvSched.wait_for(lk, std::chrono::milliseconds(2));
+            if (admitted) S->cvUpload.notify_all();
+            if (S->active.empty()) {
+                S->cvSched.wait_for(lk, std::chrono::milliseconds(admitted ? 0 : 2));
                 continue;
             }
         }
-        for (Request* R : admit) {
-            R->tAdmit = Clock::now();
-            try {
-                R->solver = std::make_unique<Solver>(std::move(*R->hier));
-                R->hier.reset();
-                R->solver->begin(R->fPinned, R->opts, R->uPinned);
-                std::lock_guard<std::mutex> lk(S->mu);
-                R->state = Request::ACTIVE;
-                S->active.push_back(R);
-                S->peakActive = std::max(S->peakActive, int(S->active.size()));
-            } catch (const Error& e) {
-                R->solver.reset();
-                std::lock_guard<std::mutex> lk(S->mu);
-                S->used -= R->need;
-                fail(S, R, e.status, e.what());
-                S->cvDone.notify_all();
-            }
-        }
-        bool progressed = !admit.empty();
+        bool progressed = admitted;
         std::vector<Request*> act;
         {
             std::lock_guard<std::mutex> lk(S->mu);
@@ -258,8 +284,17 @@ ps_status ps_server_create(int64_t device_budget_bytes, int32_t max_active, int3
     cudaMemGetInfo(&freeB, &totalB);
     S->budget = device_budget_bytes > 0 ? device_budget_bytes : int64_t(double(freeB) * 0.8);
     S->maxActive = max_active > 0 ? max_active : 4;
+    // freed device memory stays in the stream-ordered allocator's pool for the next request (the
+    // default would hand it back to the driver at every synchronisation)
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, S->device) == cudaSuccess) {
+        uint64_t keep = uint64_t(S->budget);
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
     const int nb = build_threads > 0 ? build_threads : int(std::max(1u, psfea::hostThreads() / 2));
     for (int t = 0; t < nb; t++) S->builders.emplace_back(psfea::builderLoop, S);
+    for (int t = 0; t < 2; t++) S->uploaders.emplace_back(psfea::uploaderLoop, S);
     S->scheduler = std::thread(psfea::schedulerLoop, S);
     *out = S;
     return PS_OK;
@@ -351,7 +386,9 @@ void ps_server_destroy(ps_server_t* S) {
     }
     S->cvBuild.notify_all();
     S->cvSched.notify_all();
+    S->cvUpload.notify_all();
     for (auto& t : S->builders) t.join();
+    for (auto& t : S->uploaders) t.join();
     S->scheduler.join();
     for (auto& kv : S->all) {
         kv.second->solver.reset();
