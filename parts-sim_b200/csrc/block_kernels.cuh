@@ -113,6 +113,92 @@ __device__ __forceinline__ void blockAllDone(BlockState* bs) {
 
 enum { BOP_APPLY = 0, BOP_CHEB = 1, BOP_RESID = 2, BOP_DOT = 3 };
 
+// (K x) at node (i, j, k) of a block vector (stride S, x at the lane's right-hand side) with the
+// node's 27 neighbours read once into registers: the same sums in the same order as applyAt (so
+// bitwise the same), with 81 loads instead of up to 192 on nodes that take the per-voxel gather.
+// Neighbours outside the grid read 0; they only ever meet empty voxels.
+template <bool OWN16, int S>
+__device__ __forceinline__ void applyNbr(const LevelView& L, const Coefs<float>& C, const float* __restrict__ x, int i, int j, int k,
+                                         long long n, uint8_t mask, float acc[3]) {
+    acc[0] = acc[1] = acc[2] = 0.f;
+    if (!(mask & NM_ACTIVE)) return;
+    const long long NX = L.PX, NXY = (long long)L.PX * L.NY;
+    float v[27][3];
+#pragma unroll
+    for (int m = 0; m < 27; m++) {
+        const int ox = m % 3 - 1, oy = (m / 3) % 3 - 1, oz = m / 9 - 1;
+        const bool in = i + ox >= 0 && j + oy >= 0 && k + oz >= 0 && i + ox < L.NX && j + oy < L.NY && k + oz < L.NZ;
+        const float* xp = x + 3 * S * (n + ox + oy * NX + oz * NXY);
+        v[m][0] = in ? __ldg(xp) : 0.f;
+        v[m][1] = in ? __ldg(xp + S) : 0.f;
+        v[m][2] = in ? __ldg(xp + 2 * S) : 0.f;
+    }
+    if (mask & NM_UNIFORM) {
+        const float s = __uint_as_float(__ldg(L.word + L.wi(i - 1, j - 1, k - 1)));
+        float a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+        for (int m = 0; m < 27; m++) {
+            const int ox = m % 3 - 1, oy = (m / 3) % 3 - 1, oz = m / 9 - 1;
+            const float x0 = v[m][0], x1 = v[m][1], x2 = v[m][2];
+            a0 += C.S[m * 9 + 0] * x0;
+            a1 += C.S[m * 9 + 4] * x1;
+            a2 += C.S[m * 9 + 8] * x2;
+            if (ox && oy) { a0 += C.S[m * 9 + 1] * x1; a1 += C.S[m * 9 + 3] * x0; }
+            if (ox && oz) { a0 += C.S[m * 9 + 2] * x2; a2 += C.S[m * 9 + 6] * x0; }
+            if (oy && oz) { a1 += C.S[m * 9 + 5] * x2; a2 += C.S[m * 9 + 7] * x1; }
+        }
+        acc[0] = s * a0;
+        acc[1] = s * a1;
+        acc[2] = s * a2;
+    } else {
+#pragma unroll
+        for (int vv = 0; vv < 8; vv++) {
+            const int di = vv & 1, dj = (vv >> 1) & 1, dk = vv >> 2;
+            const int ei = i - 1 + di, ej = j - 1 + dj, ek = k - 1 + dk;
+            if (ei < 0 || ej < 0 || ek < 0 || ei >= L.nx || ej >= L.ny || ek >= L.nz) continue;
+            const uint32_t w = __ldg(L.word + L.wi(ei, ej, ek));
+            if (w == 0) continue;
+            const int a = cornerOf(1 - di, 1 - dj, 1 - dk);
+            float xe[24];
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                const int bx = (b == 1 || b == 2 || b == 5 || b == 6), by = (b == 2 || b == 3 || b == 6 || b == 7), bz = b >> 2;
+                const int m = (di + bx) + 3 * (dj + by) + 9 * (dk + bz);
+                xe[3 * b] = v[m][0];
+                xe[3 * b + 1] = v[m][1];
+                xe[3 * b + 2] = v[m][2];
+            }
+            if (!(w & OWN_BIT)) {
+                float t[3];
+                kbRows<float>(C.Kb, a, xe, t);
+                const float s = __uint_as_float(w);
+                acc[0] += s * t[0];
+                acc[1] += s * t[1];
+                acc[2] += s * t[2];
+            } else if (OWN16) {
+                float t[3];
+                own16Rows<float>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a, xe, t);
+                acc[0] += L.hs * t[0];
+                acc[1] += L.hs * t[1];
+                acc[2] += L.hs * t[2];
+            } else {
+                const float4* K4 = reinterpret_cast<const float4*>(L.own + (long long)(w & ~OWN_BIT) * 576 + 72 * a);
+#pragma unroll
+                for (int d = 0; d < 3; d++)
+#pragma unroll
+                    for (int q = 0; q < 6; q++) {
+                        const float4 kv = __ldg(K4 + d * 6 + q);
+                        acc[d] += kv.x * xe[4 * q] + kv.y * xe[4 * q + 1] + kv.z * xe[4 * q + 2] + kv.w * xe[4 * q + 3];
+                    }
+            }
+        }
+    }
+    if (L.dadd) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) acc[d] += L.dadd32[3 * n + d] * v[13][d];
+    }
+}
+
 // One pass over the level's active nodes of y = K x for every right-hand side, with a per-DOF epilogue:
 //   BOP_APPLY  y = K x (held DOFs 0 unless raw)
 //   BOP_CHEB   d = c1 d + c2 D^-1 (r - K x); y = x + d        (Chebyshev / Jacobi step, 32-bit)
@@ -121,7 +207,7 @@ enum { BOP_APPLY = 0, BOP_CHEB = 1, BOP_RESID = 2, BOP_DOT = 3 };
 //              ends that right-hand side as a breakdown (voxel_fea.cpp:902-905)
 // The product is the single-vector one (applyAt, voxel_fea.cpp:422-486) with the block's stride.
 template <class T, int MODE, bool OWN16, int RB>
-__global__ void __launch_bounds__(BLOCK_THREADS) kb_op(LevelView L, Coefs<T> C, const int* __restrict__ act, int nAct,
+__global__ void __launch_bounds__(BLOCK_THREADS, 2) kb_op(LevelView L, Coefs<T> C, const int* __restrict__ act, int nAct,
                                                        const T* __restrict__ x, T* __restrict__ y, const float* __restrict__ r,
                                                        float* __restrict__ d, float c1, float c2, int raw, BlockState* bs, double* partials,
                                                        unsigned* ticket, Ctl ctl) {
@@ -136,7 +222,8 @@ __global__ void __launch_bounds__(BLOCK_THREADS) kb_op(LevelView L, Coefs<T> C, 
         int i, j, k;
         nodeCoords(L, n, i, j, k);
         T acc[3];
-        applyAt<T, OWN16, false, RB>(L, C, x + q, i, j, k, n, mask, acc, L.PX, n);
+        if constexpr (sizeof(T) == 4) applyNbr<OWN16, RB>(L, C, x + q, i, j, k, n, mask, acc);
+        else applyAt<T, OWN16, false, RB>(L, C, x + q, i, j, k, n, mask, acc, L.PX, n);
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const long long id = (3 * n + c) * RB + q;
