@@ -86,6 +86,7 @@ def parse():
     ap.add_argument("--batch-rhs", type=int, default=32, help="load cases of the batched SIMP leg (0: skip the leg)")
     ap.add_argument("--serve-requests", type=int, default=512, help="requests of the serving leg (0: skip the leg)")
     ap.add_argument("--lbracket-steps", type=int, default=3, help="solves per form of the L-bracket leg (0: skip the leg)")
+    ap.add_argument("--tensor-trial", type=int, default=1, help="1: the tensor-core element-block trial leg, 0: skip it")
     return ap.parse_args()
 
 
@@ -316,6 +317,53 @@ def l_bracket_leg(steps):
     return out
 
 
+def tensor_leg(names=("gyroid", "simp")):
+    """The tensor-core element-block operator (tcgen05 TF32, 1- and 3-term splits) on the finest
+    level of the reduced-precision forms, against the CUDA-core operator: the FP32 smoothing step's
+    CUDA-event time (20 launches) and one complete mixed solve (CUDA events on the solver's stream)."""
+    import torch
+    import psfea
+    out = {}
+    for name in names:
+        m = make_model(name)
+        f = m.f if m.f.ndim == 1 else m.f[0]
+        row = {}
+        for label, env in (("cuda_core", None), ("tf32x1", "1"), ("tf32x3", "3")):
+            saved = {k: os.environ.get(k) for k in ("PSFEA_EBE", "PSFEA_EBE_SPLIT")}
+            if env:
+                os.environ["PSFEA_EBE"] = "1"
+                os.environ["PSFEA_EBE_SPLIT"] = env
+            try:
+                S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+            finally:
+                for k, v in saved.items():
+                    if v is None:
+                        os.environ.pop(k, None)
+                    else:
+                        os.environ[k] = v
+            dev = torch.device("cuda", torch.cuda.current_device())
+            stream = torch.cuda.Stream(device=dev)
+            S.set_stream(stream.cuda_stream)
+            f_dev = torch.from_numpy(np.ascontiguousarray(f)).to(dev)
+            u_dev = torch.zeros(m.n_dof, dtype=torch.float64, device=dev)
+            S.solve_dev(f_dev.data_ptr(), u_dev.data_ptr(), tol=TOL, max_iter=MAX_ITER, precision="mixed")
+            ms_step = S.time_kernel(0, 20)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            r = S.solve_dev(f_dev.data_ptr(), u_dev.data_ptr(), tol=TOL, max_iter=MAX_ITER, precision="mixed")
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            row[label] = {"smoothing_step_ms": ms_step, "solve_ms": ms, "MDOF_per_s": m.n_dof / (ms / 1e3) / 1e6, "iterations": r.iterations,
+                          "converged": r.converged, "residual": r.residual}
+            S.set_stream(0)
+            S.close()
+            del f_dev, u_dev
+        out[name] = row
+    return out
+
+
 def serving_leg(n):
     """The serving stream: `n` requests of the Poisson stream (200 requests/s; box grids 24-160
     voxels per axis with spherical voids, random material, face and traction; rtol 1e-8, mixed
@@ -481,6 +529,12 @@ def main():
     lbr = l_bracket_leg(args.lbracket_steps) if args.lbracket_steps > 0 and world == 1 else None
     batched = batched_leg(args.batch_rhs) if args.batch_rhs > 0 and world == 1 else None
     serving = serving_leg(args.serve_requests) if args.serve_requests > 0 and world == 1 else None
+    tensor = None
+    if args.tensor_trial and world == 1:
+        try:
+            tensor = tensor_leg()
+        except Exception as e:  # reported, not hidden: the trial's outcome is part of the record
+            tensor = {"error": repr(e)}
     cb = None
     if world == 1 and not args.no_cpu_baseline:
         try:
@@ -507,6 +561,7 @@ def main():
         "l_bracket": lbr,
         "batched": batched,
         "serving": serving,
+        "tensor_trial": tensor,
         "cpu_baseline": cb,
         "gpu_launches": int(kmx),
         "clocks": clk.summary(),

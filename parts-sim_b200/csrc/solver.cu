@@ -1186,6 +1186,7 @@ __global__ void k_reactions(long long nNodes, const uint8_t* __restrict__ nmask,
 }  // namespace psfea
 
 #include "block_kernels.cuh"  // the multi-RHS kernels (they use the control helpers above)
+#include "ebe_kernels.cuh"    // the tensor-core element-block operator
 
 namespace psfea {
 
@@ -1341,8 +1342,12 @@ struct DevLevel {
     float cf0 = 0, cf1 = 0, cf2 = 0, omega = 0.5f;
     std::vector<float> chebC1, chebC2;  // steps 1 .. degree-1 of the Chebyshev smoother: d = c1 d + c2 D^-1 (r - K z)
     bool hasOwn = false;
+    // the tensor-core element-block operator (levels without Galerkin matrices): its 8 x 8 x 4 tiles
+    DevMem ebeTiles;
+    int nEbeTiles = 0;
+    bool ebe = false;
     void release() {
-        for (DevMem* b : {&word, &nmask, &own, &own16, &invD, &dadd, &dadd32, &bc, &tiles, &blist}) b->release();
+        for (DevMem* b : {&word, &nmask, &own, &own16, &invD, &dadd, &dadd32, &bc, &tiles, &blist, &ebeTiles}) b->release();
     }
 };
 
@@ -1376,6 +1381,11 @@ struct SharedModel {
     bool mixedOwn16 = true;
     bool ownDedup = true;  // one device copy per class of equal own matrices (PSFEA_OWN_DEDUP=0: one per voxel)
     double foldFactor = 0.1;  // fold when the FP32 residual is this fraction of its peak
+    // reduced-precision forms: levels (bit l) whose FP32 operator runs on the tensor cores
+    // (element-block form, levels without Galerkin matrices only), and its TF32 split (1 or 3 terms).
+    // PSFEA_EBE, PSFEA_EBE_SPLIT
+    int64_t ebeLevels = 0;
+    int ebeSplit = 3;
     cudaStream_t ms = nullptr;     // allocation / upload stream of the shared data
     cudaEvent_t readyEv = nullptr; // recorded when the uploads are done; contexts wait on it
 
@@ -1415,6 +1425,8 @@ void SharedModel::adopt(Hierarchy&& h) {
     if (const char* e = std::getenv("PSFEA_FOLD")) foldFactor = std::atof(e);
     if (const char* e = std::getenv("PSFEA_MIXED_OWN32")) mixedOwn16 = std::atoi(e) == 0;
     if (const char* e = std::getenv("PSFEA_OWN_DEDUP")) ownDedup = std::atoi(e) != 0;
+    if (const char* e = std::getenv("PSFEA_EBE")) ebeLevels = std::atoll(e);
+    if (const char* e = std::getenv("PSFEA_EBE_SPLIT")) ebeSplit = std::atoi(e) == 1 ? 1 : 3;
     check(cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking), "stream");
     check(cudaEventCreateWithFlags(&readyEv, cudaEventDisableTiming), "event");
     static std::once_flag attrOnce;
@@ -1440,6 +1452,12 @@ void SharedModel::adopt(Hierarchy&& h) {
         set(dev::k_tile<float, dev::TOP_RESID, false, false, false>, dev::tileSmemBytes<float, dev::TOP_RESID, false>());
         set(dev::k_tile<float, dev::TOP_RESID, true, false, false>, dev::tileSmemBytes<float, dev::TOP_RESID, false>());
         set(dev::k_tile<float, dev::TOP_RESID, true, true, false>, dev::tileSmemBytes<float, dev::TOP_RESID, false>());
+        set(dev::k_ebe<dev::TOP_APPLY, 1>, dev::ebeSmemBytes<1>());
+        set(dev::k_ebe<dev::TOP_CHEB, 1>, dev::ebeSmemBytes<1>());
+        set(dev::k_ebe<dev::TOP_RESID, 1>, dev::ebeSmemBytes<1>());
+        set(dev::k_ebe<dev::TOP_APPLY, 3>, dev::ebeSmemBytes<3>());
+        set(dev::k_ebe<dev::TOP_CHEB, 3>, dev::ebeSmemBytes<3>());
+        set(dev::k_ebe<dev::TOP_RESID, 3>, dev::ebeSmemBytes<3>());
     });
     L.resize(H.levels.size());
     for (int l = 0; l < int(H.levels.size()); l++) uploadLevel(l);
@@ -1531,6 +1549,25 @@ void SharedModel::uploadLevel(int l) {
                     if (act[size_t(tx + ntx * (ty + size_t(nty) * tz))]) list.push_back(dev::packTile(tx, ty, tz));
         D.nTiles = int(list.size());
         upload(D.tiles, list, bytes, ms);
+        if (h.nOwn == 0 && l < 63 && ((ebeLevels >> l) & 1)) {
+            // the element-block tiles (8 x 8 x 4 nodes) with an active node
+            const int ex = (h.NX + dev::EX - 1) / dev::EX, ey = (h.NY + dev::EY - 1) / dev::EY, ez = (h.NZ + dev::EZ - 1) / dev::EZ;
+            std::vector<uint8_t> ea(size_t(ex) * ey * ez, 0);
+            for (int k = 0; k < h.NZ; k++)
+                for (int j = 0; j < h.NY; j++) {
+                    const uint8_t* row = h.nmask.data() + h.node(0, j, k);
+                    for (int i = 0; i < h.NX; i++)
+                        if (row[i] & NM_ACTIVE) ea[size_t((i / dev::EX) + ex * ((j / dev::EY) + size_t(ey) * (k / dev::EZ)))] = 1;
+                }
+            std::vector<uint32_t> el;
+            for (int tz = 0; tz < ez; tz++)
+                for (int ty = 0; ty < ey; ty++)
+                    for (int tx = 0; tx < ex; tx++)
+                        if (ea[size_t(tx + ex * (ty + size_t(ey) * tz))]) el.push_back(dev::packTile(tx, ty, tz));
+            D.nEbeTiles = int(el.size());
+            upload(D.ebeTiles, el, bytes, ms);
+            D.ebe = D.nEbeTiles > 0;
+        }
         // small levels have too few tiles to fill the GPU: one thread per node instead, or eight
         // lanes per node on the smallest ones
         int64_t minNodes = 400000;
@@ -1834,6 +1871,18 @@ void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev
     if (!D.nTiles) return;
     float* rr = W[size_t(l)].r.as<float>();
     float* dd = W[size_t(l)].d.as<float>();
+    if (own16 && D.ebe) {
+        // the reduced-precision forms: the element-block product on the tensor cores
+        constexpr int EM = MODE == dev::OP_CHEB ? dev::TOP_CHEB : (MODE == dev::OP_RESID ? dev::TOP_RESID : dev::TOP_APPLY);
+        const uint32_t* et = D.ebeTiles.as<uint32_t>();
+        if (M->ebeSplit == 1)
+            launch(dev::k_ebe<EM, 1>, D.nEbeTiles, dev::EBE_THREADS, dev::ebeSmemBytes<1>(), stream, D.view, static_cast<const dev::Coefs<float>&>(D.c32),
+                   et, xin, y, rr, dd, c1, c2, 0, st(), ctl);
+        else
+            launch(dev::k_ebe<EM, 3>, D.nEbeTiles, dev::EBE_THREADS, dev::ebeSmemBytes<3>(), stream, D.view, static_cast<const dev::Coefs<float>&>(D.c32),
+                   et, xin, y, rr, dd, c1, c2, 0, st(), ctl);
+        return;
+    }
     const bool o16 = own16 && D.hasOwn, diff = o16 && M->ownDiff;
     if (D.use8) {
         const int g = gridFor(D.view.nNodes * 8, 256, smCount * 32);
