@@ -486,6 +486,7 @@ def main():
     t64, per64, it64, k64, res64 = timed("fp64", args.steps, args.warmup)
     with Clocks(local) as clk:
         tmx, permx, itmx, kmx, resmx = timed("mixed", args.steps, args.warmup)
+    t32, per32, it32, k32, res32 = timed("fp32", 1, 1)  # the FP32-Krylov form, one solve for reference
     tmx_max = reduce_max(pg, tmx, dev)
     t64_max = reduce_max(pg, t64, dev)
     value = job_rate(world, n, args.steps, tmx_max / 1e3)
@@ -552,6 +553,8 @@ def main():
         "iterations": {"mixed": itmx, "plain_fp64": it64},
         "residual": {"mixed": max(resmx), "plain_fp64": max(res64)},
         "plain_fp64": {"value": plain, "unit": "MDOF/s", "ms_per_solve": t64_max / args.steps},
+        "fp32_krylov": {"value": job_rate(world, n, 1, t32 / 1e3), "unit": "MDOF/s", "ms_per_solve": t32, "iterations": it32[0],
+                        "residual": res32[0]},
         "mixed_over_plain": value / plain,
         "setup_s": setup_s,  # model creation (outside the timed solves): the setup path
         "e2e": {"value": e2e_value, "unit": "MDOF/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
