@@ -486,7 +486,10 @@ def main():
     t64, per64, it64, k64, res64 = timed("fp64", args.steps, args.warmup)
     with Clocks(local) as clk:
         tmx, permx, itmx, kmx, resmx = timed("mixed", args.steps, args.warmup)
-    t32, per32, it32, k32, res32 = timed("fp32", 1, 1)  # the FP32-Krylov form, one solve for reference
+    try:  # the FP32-Krylov form, one solve for reference
+        t32, per32, it32, k32, res32 = timed("fp32", 1, 1)
+    except RuntimeError:
+        t32, it32, res32 = float("nan"), [None], [None]
     tmx_max = reduce_max(pg, tmx, dev)
     t64_max = reduce_max(pg, t64, dev)
     value = job_rate(world, n, args.steps, tmx_max / 1e3)
