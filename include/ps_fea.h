@@ -293,6 +293,15 @@ ps_status ps_break_test(const int32_t dims[3], const float* density, double nu, 
                         double strength, int32_t principal, int32_t max_steps, ps_break_step* steps, int32_t* n_steps, int32_t* cracked,
                         int64_t cracked_cap, float* density_out, double* peak, int32_t* reason);
 
+/* pruneFloating (voxel_fea.cpp:1086-1119) on device arrays, for callers that keep their voxel grid
+ * on the GPU (the break test prunes this way after every step): out_dev = density_dev where the
+ * voxel's face-connected solid component touches a held node (held_dev: NX NY NZ bytes), else 0;
+ * *removed = solid voxels dropped. Components by lock-free union-find; the kept set is unique, so
+ * the result equals the reference's breadth-first search. Stream-ordered on cuda_stream (NULL = the
+ * legacy default stream); returns once the result is written. */
+ps_status ps_prune_floating_dev(const int32_t dims[3], const float* density_dev, const uint8_t* held_dev, float* out_dev, int32_t* removed,
+                                void* cuda_stream);
+
 /* ---- Serving: many independent solves on one GPU with continuous batching (no counterpart in the
  * reference, which runs one job at a time behind a GPU lock, native/src/gpu/gpu.hpp:43).
  * Requests are submitted at any time; host threads build their hierarchies; a scheduler admits

@@ -172,6 +172,17 @@ ps_status ps_topology_run(const int32_t dims[3], const float* fill, const uint8_
     });
 }
 
+ps_status ps_prune_floating_dev(const int32_t dims[3], const float* density_dev, const uint8_t* held_dev, float* out_dev, int32_t* removed,
+                                void* cuda_stream) {
+    return guarded([&] {
+        if (!dims || !density_dev || !held_dev || !out_dev) return fail(PS_EINVAL, "NULL argument");
+        if (!psfea::deviceAvailable()) return fail(PS_ENODEV, "no CUDA device is available");
+        const int r = psfea::pruneFloatingDevice(dims, density_dev, held_dev, out_dev, cuda_stream);
+        if (removed) *removed = r;
+        return PS_OK;
+    });
+}
+
 ps_status ps_break_test(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, const double* f, double E, double h,
                         double strength, int32_t principal, int32_t max_steps, ps_break_step* steps, int32_t* n_steps, int32_t* cracked,
                         int64_t cracked_cap, float* density_out, double* peak, int32_t* reason) {

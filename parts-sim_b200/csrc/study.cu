@@ -247,44 +247,119 @@ int smCountNow() {
     return sm;
 }
 
-// voxels face-connected to a voxel touching a held node survive (voxel_fea.cpp:1086-1119)
-int pruneHost(const int32_t dims[3], std::vector<float>& density, const std::vector<uint8_t>& heldNode) {
-    const int nx = dims[0], ny = dims[1], nz = dims[2];
-    const int64_t NX = nx + 1, NY = ny + 1, nVox = int64_t(nx) * ny * nz;
-    std::vector<uint8_t> seen(size_t(nVox), 0);
-    std::vector<int64_t> queue;
-    for (int64_t e = 0; e < nVox; e++) {
-        if (!(density[size_t(e)] > 0)) continue;
-        const int64_t i = e % nx, j = (e / nx) % ny, k = e / (int64_t(nx) * ny);
-        bool touch = false;
-        for (int a = 0; a < 8 && !touch; a++)
-            touch = heldNode[size_t((i + CORNER_XYZ[a][0]) + NX * ((j + CORNER_XYZ[a][1]) + NY * (k + CORNER_XYZ[a][2])))] != 0;
-        if (touch) {
-            seen[size_t(e)] = 1;
-            queue.push_back(e);
+// ---- pruneFloating on the device (voxel_fea.cpp:1086-1119): the voxels face-connected to a voxel
+// touching a held node survive. The reference walks them breadth-first; here the solid voxels'
+// 6-connected components are found by a lock-free union-find (roots hooked under the smaller index
+// by compare-and-swap, paths halved on the way), and a voxel survives when its component holds a
+// voxel with a held corner. The surviving set is unique, so the result equals the reference's.
+
+constexpr int UF_MAX_STEPS = 1 << 24;  // bound on any find / hook loop (a bad state ends the kernel)
+
+__device__ __forceinline__ int ufFind(int* p, int x, int* err) {
+    for (int s = 0; s < UF_MAX_STEPS; s++) {
+        const int px = p[x];
+        if (px == x) return x;
+        const int gp = p[px];
+        if (gp != px) p[x] = gp;  // path halving; any value written is an ancestor, so it is safe
+        x = gp;
+    }
+    atomicExch(err, 1);
+    return x;
+}
+
+__global__ void k_uf_init(long long nVox, const float* __restrict__ density, int* __restrict__ parent) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nVox; e += (long long)gridDim.x * blockDim.x)
+        parent[e] = density[e] > 0 ? int(e) : -1;
+}
+
+__global__ void k_uf_hook(long long nVox, int nx, int ny, int* __restrict__ parent, int* err) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nVox; e += (long long)gridDim.x * blockDim.x) {
+        if (parent[e] < 0) continue;
+        const long long i = e % nx, j = (e / nx) % ny;
+        const long long nb[3] = {i + 1 < nx ? e + 1 : -1, j + 1 < ny ? e + nx : -1, e + (long long)nx * ny < nVox ? e + (long long)nx * ny : -1};
+        for (int q = 0; q < 3; q++) {
+            if (nb[q] < 0 || parent[nb[q]] < 0) continue;
+            int a = int(e), b = int(nb[q]);
+            for (int s = 0; s < UF_MAX_STEPS; s++) {
+                a = ufFind(parent, a, err);
+                b = ufFind(parent, b, err);
+                if (a == b) break;
+                if (a < b) {
+                    const int t = a;
+                    a = b;
+                    b = t;
+                }
+                const int old = atomicCAS(parent + a, a, b);  // the larger root under the smaller
+                if (old == a) break;
+                a = old;
+                if (s + 1 == UF_MAX_STEPS) atomicExch(err, 1);
+            }
         }
     }
-    for (size_t h = 0; h < queue.size(); h++) {
-        const int64_t e = queue[h], i = e % nx, j = (e / nx) % ny, k = e / (int64_t(nx) * ny);
-        const int64_t nb[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
-        for (const auto& p : nb) {
-            if (p[0] < 0 || p[1] < 0 || p[2] < 0 || p[0] >= nx || p[1] >= ny || p[2] >= nz) continue;
-            const int64_t v = p[0] + nx * (p[1] + int64_t(ny) * p[2]);
-            if (seen[size_t(v)] || !(density[size_t(v)] > 0)) continue;
-            seen[size_t(v)] = 1;
-            queue.push_back(v);
+}
+
+// roots of the components with a voxel touching a held node: flag[root] = 1
+__global__ void k_uf_touch(long long nVox, int nx, int ny, const uint8_t* __restrict__ held, int* __restrict__ parent, int* __restrict__ flag,
+                           int* err) {
+    const long long NX = nx + 1, NY = ny + 1;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nVox; e += (long long)gridDim.x * blockDim.x) {
+        if (parent[e] < 0) continue;
+        const long long i = e % nx, j = (e / nx) % ny, k = e / ((long long)nx * ny);
+        bool t = false;
+#pragma unroll
+        for (int a = 0; a < 8; a++) {
+            const int bx = (a == 1 || a == 2 || a == 5 || a == 6), by = (a == 2 || a == 3 || a == 6 || a == 7), bz = a >> 2;
+            t = t || held[(i + bx) + NX * ((j + by) + NY * (k + bz))] != 0;
         }
+        if (t) flag[ufFind(parent, int(e), err)] = 1;
     }
-    int removed = 0;
-    for (int64_t e = 0; e < nVox; e++)
-        if (density[size_t(e)] > 0 && !seen[size_t(e)]) {
-            density[size_t(e)] = 0.f;
-            removed++;
+}
+
+__global__ void k_uf_keep(long long nVox, const float* __restrict__ density, int* __restrict__ parent, const int* __restrict__ flag,
+                          float* __restrict__ out, int* __restrict__ removed, int* err) {
+    int rem = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nVox; e += (long long)gridDim.x * blockDim.x) {
+        float v = 0.f;
+        if (parent[e] >= 0) {
+            if (flag[ufFind(parent, int(e), err)]) v = density[e];
+            else rem++;
         }
-    return removed;
+        out[e] = v;
+    }
+    if (rem) atomicAdd(removed, rem);
 }
 
 }  // namespace
+
+int pruneFloatingDevice(const int32_t dims[3], const float* densityDev, const uint8_t* heldDev, float* outDev, void* streamPtr) {
+    cudaStream_t stream = static_cast<cudaStream_t>(streamPtr);
+    const int nx = dims[0], ny = dims[1], nz = dims[2];
+    if (nx < 1 || ny < 1 || nz < 1) throw Error(PS_EINVAL, "The structural grid must have three positive dimensions.");
+    const long long nVox = (long long)nx * ny * nz;
+    if (nVox > (long long)INT32_MAX) throw Error(PS_EINVAL, "grid too large for 32-bit voxel labels");
+    int* parent = nullptr;
+    int* flag = nullptr;
+    int* cnt = nullptr;  // removed, error
+    ck(cudaMallocAsync(&parent, size_t(nVox) * 4, stream), "cudaMallocAsync");
+    ck(cudaMallocAsync(&flag, size_t(nVox) * 4, stream), "cudaMallocAsync");
+    ck(cudaMallocAsync(&cnt, 8, stream), "cudaMallocAsync");
+    ck(cudaMemsetAsync(flag, 0, size_t(nVox) * 4, stream), "memset");
+    ck(cudaMemsetAsync(cnt, 0, 8, stream), "memset");
+    const int sm = smCountNow();
+    const int g = gridOf(nVox, sm);
+    k_uf_init<<<g, 256, 0, stream>>>(nVox, densityDev, parent);
+    k_uf_hook<<<g, 256, 0, stream>>>(nVox, nx, ny, parent, cnt + 1);
+    k_uf_touch<<<g, 256, 0, stream>>>(nVox, nx, ny, heldDev, parent, flag, cnt + 1);
+    k_uf_keep<<<g, 256, 0, stream>>>(nVox, densityDev, parent, flag, outDev, cnt, cnt + 1);
+    int h[2] = {0, 0};
+    ck(cudaMemcpyAsync(h, cnt, 8, cudaMemcpyDeviceToHost, stream), "download");
+    cudaFreeAsync(parent, stream);
+    cudaFreeAsync(flag, stream);
+    cudaFreeAsync(cnt, stream);
+    ck(cudaStreamSynchronize(stream), "prune");
+    if (h[1]) throw Error(PS_ECUDA, "the component labelling did not settle");
+    return h[0];
+}
 
 bool deviceAvailable() {
     int count = 0;
@@ -433,7 +508,15 @@ BreakReason breakTest(const int32_t dims[3], const float* density0, double nu, c
     std::vector<uint8_t> held(size_t(nNodes), 0);
     for (int64_t n = 0; n < nNodes; n++) held[size_t(n)] = (bc[3 * n] | bc[3 * n + 1] | bc[3 * n + 2]) ? 1 : 0;
     std::vector<float> density(density0, density0 + nVox);
-    pruneHost(dims, density, held);
+    Dev<uint8_t> dHeld(static_cast<size_t>(nNodes));
+    dHeld.upload(held.data(), size_t(nNodes));
+    Dev<float> dIn(static_cast<size_t>(nVox)), dOut(static_cast<size_t>(nVox));
+    auto prune = [&](std::vector<float>& d) {
+        dIn.upload(d.data(), size_t(nVox));
+        pruneFloatingDevice(dims, dIn.p, dHeld.p, dOut.p, nullptr);
+        dOut.download(d.data(), size_t(nVox));
+    };
+    prune(density);
     // the load on each node, for the lost-load fraction (static_study.cpp:23-32)
     std::vector<double> fmag(static_cast<size_t>(nNodes));
     double ftotal = 0;
@@ -530,7 +613,7 @@ BreakReason breakTest(const int32_t dims[3], const float* density0, double nu, c
         std::vector<float> next = density;
         for (int e : bs.cracked) next[size_t(e)] = 0;
         std::vector<float> pruned = next;
-        pruneHost(dims, pruned, held);
+        prune(pruned);
         for (int64_t e = 0; e < nVox; e++)
             if (next[size_t(e)] > 0 && !(pruned[size_t(e)] > 0)) bs.detached.push_back(int(e));
         density = std::move(pruned);

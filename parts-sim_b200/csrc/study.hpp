@@ -12,6 +12,11 @@ namespace psfea {
 // a usable CUDA device is present
 bool deviceAvailable();
 
+// pruneFloating (voxel_fea.cpp:1086-1119) on device arrays: outDev = densityDev where the voxel's
+// 6-connected solid component has a voxel with a held corner node (heldDev: per node), else 0;
+// returns the number of solid voxels removed. Stream-ordered; waits for its result.
+int pruneFloatingDevice(const int32_t dims[3], const float* densityDev, const uint8_t* heldDev, float* outDev, void* stream);
+
 // native/src/fea/topology.hpp:38-48 and the solve of native/src/fea/study_runner.cpp:403-419
 struct TopologyOptions {
     double volFrac = 0.4, penal = 3, rmin = 1.5, move = 0.2, tol = 0.01;

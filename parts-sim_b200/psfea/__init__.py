@@ -132,6 +132,7 @@ _topo_run = _sig("ps_topology_run", C.c_int, _I32P, _F32P, C.c_void_p, C.c_doubl
 _break_test = _sig("ps_break_test", C.c_int, _I32P, _F32P, C.c_double, _U8P, _F64P, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32,
                    C.c_void_p, C.POINTER(C.c_int32), C.c_void_p, C.c_int64, _F32P, C.POINTER(C.c_double), C.POINTER(C.c_int32))
 _prune = _sig("ps_prune_floating", C.c_int, _I32P, _F32P, _U8P, _F32P, C.POINTER(C.c_int32))
+_prune_dev = _sig("ps_prune_floating_dev", C.c_int, _I32P, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.c_void_p)
 _last_error = _sig("ps_last_error", C.c_char_p)
 _opts_default = _sig("ps_solve_opts_default", None, C.POINTER(SolveOpts))
 _h_create = _sig("ps_hierarchy_create", C.c_int, _I32P, _F32P, C.c_double, _U8P, C.c_int64, C.c_void_p, C.POINTER(C.c_void_p))
@@ -150,6 +151,7 @@ EXPORTS = ("ps_solve_opts_default", "ps_fea_create", "ps_fea_solve", "ps_fea_sol
            "ps_hierarchy_level_fixed", "ps_hierarchy_level_own", "ps_hierarchy_level_kb", "ps_hierarchy_destroy",
            "ps_fea_set_stream", "ps_fea_time_kernel", "ps_fea_kernel_launches", "ps_fea_apply_dot_noalloc", "ps_fea_precondition_block",
            "ps_topology_opts_default", "ps_topology_run", "ps_break_test", "ps_fea_autotune", "ps_fea_create_tuned",
+           "ps_prune_floating_dev",
            "ps_server_create", "ps_server_submit", "ps_server_poll", "ps_server_wait", "ps_server_release", "ps_server_get_stats",
            "ps_server_destroy")
 
@@ -506,6 +508,16 @@ def prune_floating(dims, density, held_node):
     if st != PS_OK:
         _raise(st)
     return out, int(removed.value)
+
+
+def prune_floating_dev(dims, density_ptr, held_ptr, out_ptr, stream_ptr=None):
+    """pruneFloating on device arrays (pointers); returns the number of voxels removed."""
+    removed = C.c_int32()
+    st = _prune_dev(np.ascontiguousarray(dims, np.int32), C.c_void_p(density_ptr), C.c_void_p(held_ptr), C.c_void_p(out_ptr),
+                    C.byref(removed), C.c_void_p(stream_ptr) if stream_ptr else None)
+    if st != PS_OK:
+        _raise(st)
+    return int(removed.value)
 
 
 def topology_run(dims, fill, nu, bc, f, keep=None, vol_frac=0.4, penal=3.0, rmin=1.5, move=0.2, tol=0.01, max_iter=40, solve_tol=1e-5,

@@ -120,3 +120,44 @@ def test_break_test_matches_reference(principal):
     assert rel(out["peak"], ref_peak) < 1e-4
     if all(r["candidates"] <= r["cap"] for r in ref_steps):
         assert np.array_equal(out["density"], ref_dens)
+
+
+def test_prune_floating_on_the_device_matches_the_library_and_reference():
+    """ps_prune_floating_dev (union-find components) keeps exactly the voxels of the host
+    breadth-first search and of the reference's prune fixture: random sparse grids, a gyroid sheet
+    with floating fragments, a grid with nothing held."""
+    import torch
+    from conftest import golden
+    dev = torch.device("cuda", 0)
+
+    def run(dims, d, held):
+        dd = torch.from_numpy(np.ascontiguousarray(d, np.float32)).to(dev)
+        hh = torch.from_numpy(np.ascontiguousarray(held, np.uint8)).to(dev)
+        out = torch.full_like(dd, float("nan"))
+        rem = psfea.prune_floating_dev(dims, dd.data_ptr(), hh.data_ptr(), out.data_ptr())
+        return out.cpu().numpy(), rem
+
+    g = golden("prune")
+    for d, h, dims in ((g["d1"], g["h1"], (4, 1, 1)), (g["d2"], g["h2"], tuple(g["dims2"]))):
+        o, r = run(dims, d, h)
+        o_ref, r_ref = oracle.prune("reference", dims, d, h)
+        assert np.array_equal(o, o_ref) and r == r_ref
+    rng = np.random.default_rng(8)
+    for dims in ((64, 48, 40), (17, 9, 13), (1, 1, 1), (200, 3, 2)):
+        nx, ny, nz = dims
+        for frac in (0.3, 0.55):
+            d = (rng.random(nx * ny * nz) < frac).astype(np.float32) * (0.5 + rng.random(nx * ny * nz).astype(np.float32))
+            held = (rng.random((nx + 1) * (ny + 1) * (nz + 1)) < 0.01).astype(np.uint8)
+            o, r = run(dims, d, held)
+            o_lib, r_lib = psfea.prune_floating(dims, d, held)
+            assert np.array_equal(o, o_lib) and r == r_lib, (dims, frac)
+    m = W.gyroid(96, 96, 48)
+    t = lambda n: 2 * np.pi * (np.arange(n) + 0.5) / 24
+    val = (np.sin(t(96))[None, None, :] * np.cos(t(96))[None, :, None] + np.sin(t(96))[None, :, None] * np.cos(t(48))[:, None, None]
+           + np.sin(t(48))[:, None, None] * np.cos(t(96))[None, None, :])
+    raw = (np.abs(val) < 0.3).astype(np.float32).ravel()
+    held = W.held_nodes((96, 96, 48), m.bc)
+    o, r = run((96, 96, 48), raw, held)
+    assert np.array_equal(o, m.density) and r == m.meta["removed"]
+    o, r = run((96, 96, 48), raw, np.zeros_like(held))
+    assert not o.any() and r == int((raw > 0).sum())
