@@ -87,6 +87,9 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=512, help="requests of the serving leg (0: skip the leg)")
     ap.add_argument("--lbracket-steps", type=int, default=3, help="solves per form of the L-bracket leg (0: skip the leg)")
     ap.add_argument("--tensor-trial", type=int, default=1, help="1: the tensor-core element-block trial leg, 0: skip it")
+    ap.add_argument("--leg", choices=["batched", "serving", "tensor", "l_bracket"], default=None,
+                    help="run only this extra leg and print its JSON (a short command for profilers and sweeps)")
+    ap.add_argument("--serve-max-active", type=int, default=0, help="active-solve slots of the serving leg (0: the server default)")
     return ap.parse_args()
 
 
@@ -364,7 +367,7 @@ def tensor_leg(names=("gyroid", "simp")):
     return out
 
 
-def serving_leg(n):
+def serving_leg(n, max_active=0):
     """The serving stream: `n` requests of the Poisson stream (200 requests/s; box grids 24-160
     voxels per axis with spherical voids, random material, face and traction; rtol 1e-8, mixed
     precision), submitted at their arrival times to the continuous-batching server; latency =
@@ -372,7 +375,7 @@ def serving_leg(n):
     import psfea
     import voxel_models as W
     reqs = list(W.serving_stream(n=n))
-    srv = psfea.Server()
+    srv = psfea.Server(max_active=max_active)
     t0 = time.perf_counter()
     ids = []
     for ta, m in reqs:
@@ -442,6 +445,11 @@ def main():
         return
     if args.kernel_only:
         kernel_only(args)
+        return
+    if args.leg:
+        fn = {"batched": lambda: batched_leg(args.batch_rhs), "serving": lambda: serving_leg(args.serve_requests, args.serve_max_active),
+              "tensor": tensor_leg, "l_bracket": lambda: l_bracket_leg(args.lbracket_steps)}[args.leg]
+        print(json.dumps({"leg": args.leg, "result": fn()}), flush=True)
         return
     rank, world, local, pg = dist_setup(args.gpus)
     import torch
@@ -532,7 +540,7 @@ def main():
     # the other workloads, on one GPU (rank 0 of a replica run skips them)
     lbr = l_bracket_leg(args.lbracket_steps) if args.lbracket_steps > 0 and world == 1 else None
     batched = batched_leg(args.batch_rhs) if args.batch_rhs > 0 and world == 1 else None
-    serving = serving_leg(args.serve_requests) if args.serve_requests > 0 and world == 1 else None
+    serving = serving_leg(args.serve_requests, args.serve_max_active) if args.serve_requests > 0 and world == 1 else None
     tensor = None
     if args.tensor_trial and world == 1:
         try:

@@ -113,74 +113,88 @@ __device__ __forceinline__ void blockAllDone(BlockState* bs) {
 
 enum { BOP_APPLY = 0, BOP_CHEB = 1, BOP_RESID = 2, BOP_DOT = 3 };
 
-// (K x) at node (i, j, k) of a block vector (stride S, x at the lane's right-hand side) with the
-// node's 27 neighbours read once into registers: the same sums in the same order as applyAt (so
-// bitwise the same), with 81 loads instead of up to 192 on nodes that take the per-voxel gather.
-// Neighbours outside the grid read 0; they only ever meet empty voxels.
-template <bool OWN16, int S>
-__device__ __forceinline__ void applyNbr(const LevelView& L, const Coefs<float>& C, const float* __restrict__ x, int i, int j, int k,
-                                         long long n, uint8_t mask, float acc[3]) {
-    acc[0] = acc[1] = acc[2] = 0.f;
+// (K x) at node (i, j, k) of a block vector (stride S, x at the lane's right-hand side) with each of
+// the node's 27 neighbours read once, two z-planes of 9 nodes in registers at a time (planes -1 and
+// 0 for the voxels below the node, 0 and +1 for those above): the same sums in the same order as
+// applyAt (so bitwise the same), with 81 loads instead of up to 192 on nodes that take the per-voxel
+// gather. Neighbours outside the grid read 0; they only ever meet empty voxels.
+template <class T, bool OWN16, int S>
+__device__ __forceinline__ void applyNbr(const LevelView& L, const Coefs<T>& C, const T* __restrict__ x, int i, int j, int k, long long n,
+                                         uint8_t mask, T acc[3]) {
+    acc[0] = acc[1] = acc[2] = T(0);
     if (!(mask & NM_ACTIVE)) return;
     const long long NX = L.PX, NXY = (long long)L.PX * L.NY;
-    float v[27][3];
+    auto plane = [&](int oz, T (&P)[9][3]) {
 #pragma unroll
-    for (int m = 0; m < 27; m++) {
-        const int ox = m % 3 - 1, oy = (m / 3) % 3 - 1, oz = m / 9 - 1;
-        const bool in = i + ox >= 0 && j + oy >= 0 && k + oz >= 0 && i + ox < L.NX && j + oy < L.NY && k + oz < L.NZ;
-        const float* xp = x + 3 * S * (n + ox + oy * NX + oz * NXY);
-        v[m][0] = in ? __ldg(xp) : 0.f;
-        v[m][1] = in ? __ldg(xp + S) : 0.f;
-        v[m][2] = in ? __ldg(xp + 2 * S) : 0.f;
-    }
+        for (int b = 0; b < 9; b++) {
+            const int ox = b % 3 - 1, oy = b / 3 - 1;
+            const bool in = i + ox >= 0 && j + oy >= 0 && k + oz >= 0 && i + ox < L.NX && j + oy < L.NY && k + oz < L.NZ;
+            const T* xp = x + 3 * S * (n + ox + oy * NX + oz * NXY);
+            P[b][0] = in ? __ldg(xp) : T(0);
+            P[b][1] = in ? __ldg(xp + S) : T(0);
+            P[b][2] = in ? __ldg(xp + 2 * S) : T(0);
+        }
+    };
+    T A[9][3], B[9][3];  // A: planes -1 then +1; B: plane 0
+    plane(-1, A);
+    plane(0, B);
+    const T own[3] = {B[4][0], B[4][1], B[4][2]};
     if (mask & NM_UNIFORM) {
         const float s = __uint_as_float(__ldg(L.word + L.wi(i - 1, j - 1, k - 1)));
-        float a0 = 0, a1 = 0, a2 = 0;
+        T a0 = 0, a1 = 0, a2 = 0;
+        auto sweep = [&](int oz, const T (&P)[9][3]) {
 #pragma unroll
-        for (int m = 0; m < 27; m++) {
-            const int ox = m % 3 - 1, oy = (m / 3) % 3 - 1, oz = m / 9 - 1;
-            const float x0 = v[m][0], x1 = v[m][1], x2 = v[m][2];
-            a0 += C.S[m * 9 + 0] * x0;
-            a1 += C.S[m * 9 + 4] * x1;
-            a2 += C.S[m * 9 + 8] * x2;
-            if (ox && oy) { a0 += C.S[m * 9 + 1] * x1; a1 += C.S[m * 9 + 3] * x0; }
-            if (ox && oz) { a0 += C.S[m * 9 + 2] * x2; a2 += C.S[m * 9 + 6] * x0; }
-            if (oy && oz) { a1 += C.S[m * 9 + 5] * x2; a2 += C.S[m * 9 + 7] * x1; }
-        }
-        acc[0] = s * a0;
-        acc[1] = s * a1;
-        acc[2] = s * a2;
+            for (int b = 0; b < 9; b++) {
+                const int ox = b % 3 - 1, oy = b / 3 - 1, m = b + 9 * (oz + 1);
+                const T x0 = P[b][0], x1 = P[b][1], x2 = P[b][2];
+                a0 += C.S[m * 9 + 0] * x0;
+                a1 += C.S[m * 9 + 4] * x1;
+                a2 += C.S[m * 9 + 8] * x2;
+                if (ox && oy) { a0 += C.S[m * 9 + 1] * x1; a1 += C.S[m * 9 + 3] * x0; }
+                if (ox && oz) { a0 += C.S[m * 9 + 2] * x2; a2 += C.S[m * 9 + 6] * x0; }
+                if (oy && oz) { a1 += C.S[m * 9 + 5] * x2; a2 += C.S[m * 9 + 7] * x1; }
+            }
+        };
+        sweep(-1, A);
+        sweep(0, B);
+        plane(1, A);
+        sweep(1, A);
+        acc[0] = T(s) * a0;
+        acc[1] = T(s) * a1;
+        acc[2] = T(s) * a2;
     } else {
-#pragma unroll
-        for (int vv = 0; vv < 8; vv++) {
+        // voxel vv = di + 2 dj + 4 dk at offset (di - 1, dj - 1, dk - 1); its corner b sits in plane
+        // dk + bz - 1: lo = the plane below (dk - 1), hi = the plane above (dk)
+        auto voxel = [&](int vv, const T (&lo)[9][3], const T (&hi)[9][3]) {
             const int di = vv & 1, dj = (vv >> 1) & 1, dk = vv >> 2;
             const int ei = i - 1 + di, ej = j - 1 + dj, ek = k - 1 + dk;
-            if (ei < 0 || ej < 0 || ek < 0 || ei >= L.nx || ej >= L.ny || ek >= L.nz) continue;
+            if (ei < 0 || ej < 0 || ek < 0 || ei >= L.nx || ej >= L.ny || ek >= L.nz) return;
             const uint32_t w = __ldg(L.word + L.wi(ei, ej, ek));
-            if (w == 0) continue;
+            if (w == 0) return;
             const int a = cornerOf(1 - di, 1 - dj, 1 - dk);
-            float xe[24];
+            T xe[24];
 #pragma unroll
             for (int b = 0; b < 8; b++) {
                 const int bx = (b == 1 || b == 2 || b == 5 || b == 6), by = (b == 2 || b == 3 || b == 6 || b == 7), bz = b >> 2;
-                const int m = (di + bx) + 3 * (dj + by) + 9 * (dk + bz);
-                xe[3 * b] = v[m][0];
-                xe[3 * b + 1] = v[m][1];
-                xe[3 * b + 2] = v[m][2];
+                const int b9 = (di + bx) + 3 * (dj + by);
+                const T* src = bz ? hi[b9] : lo[b9];
+                xe[3 * b] = src[0];
+                xe[3 * b + 1] = src[1];
+                xe[3 * b + 2] = src[2];
             }
             if (!(w & OWN_BIT)) {
-                float t[3];
-                kbRows<float>(C.Kb, a, xe, t);
-                const float s = __uint_as_float(w);
-                acc[0] += s * t[0];
-                acc[1] += s * t[1];
-                acc[2] += s * t[2];
+                T t[3];
+                kbRows<T>(C.Kb, a, xe, t);
+                const T sc = T(__uint_as_float(w));
+                acc[0] += sc * t[0];
+                acc[1] += sc * t[1];
+                acc[2] += sc * t[2];
             } else if (OWN16) {
-                float t[3];
-                own16Rows<float>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a, xe, t);
-                acc[0] += L.hs * t[0];
-                acc[1] += L.hs * t[1];
-                acc[2] += L.hs * t[2];
+                T t[3];
+                own16Rows<T>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a, xe, t);
+                acc[0] += T(L.hs) * t[0];
+                acc[1] += T(L.hs) * t[1];
+                acc[2] += T(L.hs) * t[2];
             } else {
                 const float4* K4 = reinterpret_cast<const float4*>(L.own + (long long)(w & ~OWN_BIT) * 576 + 72 * a);
 #pragma unroll
@@ -188,14 +202,19 @@ __device__ __forceinline__ void applyNbr(const LevelView& L, const Coefs<float>&
 #pragma unroll
                     for (int q = 0; q < 6; q++) {
                         const float4 kv = __ldg(K4 + d * 6 + q);
-                        acc[d] += kv.x * xe[4 * q] + kv.y * xe[4 * q + 1] + kv.z * xe[4 * q + 2] + kv.w * xe[4 * q + 3];
+                        acc[d] += T(kv.x) * xe[4 * q] + T(kv.y) * xe[4 * q + 1] + T(kv.z) * xe[4 * q + 2] + T(kv.w) * xe[4 * q + 3];
                     }
             }
-        }
+        };
+#pragma unroll
+        for (int vv = 0; vv < 4; vv++) voxel(vv, A, B);
+        plane(1, A);
+#pragma unroll
+        for (int vv = 4; vv < 8; vv++) voxel(vv, B, A);
     }
     if (L.dadd) {
 #pragma unroll
-        for (int d = 0; d < 3; d++) acc[d] += L.dadd32[3 * n + d] * v[13][d];
+        for (int d = 0; d < 3; d++) acc[d] += (sizeof(T) == 8 ? T(L.dadd[3 * n + d]) : T(L.dadd32[3 * n + d])) * own[d];
     }
 }
 
@@ -222,8 +241,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 2) kb_op(LevelView L, Coefs<T> 
         int i, j, k;
         nodeCoords(L, n, i, j, k);
         T acc[3];
-        if constexpr (sizeof(T) == 4) applyNbr<OWN16, RB>(L, C, x + q, i, j, k, n, mask, acc);
-        else applyAt<T, OWN16, false, RB>(L, C, x + q, i, j, k, n, mask, acc, L.PX, n);
+        applyNbr<T, OWN16, RB>(L, C, x + q, i, j, k, n, mask, acc);
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const long long id = (3 * n + c) * RB + q;

@@ -81,7 +81,11 @@ def test_precondition_close_to_oracle_and_linear():
     r = P.apply(g["apply_x"])
     z = S.precondition(r)
     zo = P.precondition(r)
-    assert rel(z, zo) < 1e-2  # one FP32 V-cycle, different summation order
+    # one FP32 V-cycle, different summation order: measured on a B200 6.8e-6 against the reference's
+    # own V-cycle and 1.9e-5 against the restatement on this model (the golden models: 2e-6 - 9.5e-5)
+    assert rel(z, zo) < 1e-4
+    R = oracle.OracleModel("reference", tuple(g["dims"]), g["density"], float(g["nu"]), g["bc"], int(g["coarsest"]))
+    assert rel(z, R.precondition(r)) < 1e-4
     # r is scaled by 1 / max|r| before the FP32 cycle: scaling by 2 is exact
     assert np.array_equal(S.precondition(2 * r), 2 * z)
     assert np.allclose([S.lmax(l) for l in range(S.n_levels - 1)], g["lmax"], rtol=1e-9)
