@@ -1187,6 +1187,7 @@ __global__ void k_reactions(long long nNodes, const uint8_t* __restrict__ nmask,
 
 #include "block_kernels.cuh"  // the multi-RHS kernels (they use the control helpers above)
 #include "ebe_kernels.cuh"    // the tensor-core element-block operator
+#include "block_tc.cuh"       // the block operator on the tensor cores
 
 namespace psfea {
 
@@ -1391,6 +1392,7 @@ struct SharedModel {
 
     ~SharedModel() {
         for (auto& a : act) a.release();
+        btTiles.release();
         for (auto& D : L) D.release();
         cDof.release();
         cInv.release();
@@ -1405,6 +1407,12 @@ struct SharedModel {
     // them); built on the first block solve
     std::vector<DevMem> act;
     std::vector<int> nAct;
+    // the finest level's 8 x 4 x 4 node tiles with an active node, for the block tensor-core
+    // operator (built with the active lists); PSFEA_BLOCK_TC=0 keeps the mixed block form on the
+    // CUDA cores
+    DevMem btTiles;
+    int nBtTiles = 0;
+    bool blockTc = true;
 
     void build(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsest, const double* diagAdd);
     void adopt(Hierarchy&& h);  // upload a hierarchy built on the host beforehand
@@ -1458,6 +1466,9 @@ void SharedModel::adopt(Hierarchy&& h) {
         set(dev::k_ebe<dev::TOP_APPLY, 3>, dev::ebeSmemBytes<3>());
         set(dev::k_ebe<dev::TOP_CHEB, 3>, dev::ebeSmemBytes<3>());
         set(dev::k_ebe<dev::TOP_RESID, 3>, dev::ebeSmemBytes<3>());
+        set(dev::kb_tc<dev::BOP_APPLY>, dev::btSmemBytes());
+        set(dev::kb_tc<dev::BOP_CHEB>, dev::btSmemBytes());
+        set(dev::kb_tc<dev::BOP_RESID>, dev::btSmemBytes());
     });
     L.resize(H.levels.size());
     for (int l = 0; l < int(H.levels.size()); l++) uploadLevel(l);
@@ -1644,6 +1655,27 @@ void SharedModel::ensureActiveLists() {
         act.emplace_back();
         nAct[l] = int(list.size());
         upload(act.back(), list, bytes, ms);
+    }
+    if (const char* e = std::getenv("PSFEA_BLOCK_TC")) blockTc = std::atoi(e) != 0;
+    const HostLevel& h0 = H.levels[0];
+    if (h0.nOwn == 0) {
+        const int ex = (h0.NX + dev::BT_X - 1) / dev::BT_X, ey = (h0.NY + dev::BT_Y - 1) / dev::BT_Y, ez = (h0.NZ + dev::BT_Z - 1) / dev::BT_Z;
+        if (ex <= 2047 && ey <= 2047 && ez <= 1023) {
+            std::vector<uint8_t> ea(size_t(ex) * ey * ez, 0);
+            for (int k = 0; k < h0.NZ; k++)
+                for (int j = 0; j < h0.NY; j++) {
+                    const uint8_t* row = h0.nmask.data() + h0.node(0, j, k);
+                    for (int i = 0; i < h0.NX; i++)
+                        if (row[i] & NM_ACTIVE) ea[size_t((i / dev::BT_X) + ex * ((j / dev::BT_Y) + size_t(ey) * (k / dev::BT_Z)))] = 1;
+                }
+            std::vector<uint32_t> tl;
+            for (int tz = 0; tz < ez; tz++)
+                for (int ty = 0; ty < ey; ty++)
+                    for (int tx = 0; tx < ex; tx++)
+                        if (ea[size_t(tx + ex * (ty + size_t(ey) * tz))]) tl.push_back(dev::packTile(tx, ty, tz));
+            nBtTiles = int(tl.size());
+            upload(btTiles, tl, bytes, ms);
+        }
     }
     check(cudaEventRecord(readyEv, ms), "event");
 }
@@ -2462,6 +2494,14 @@ struct BlockImpl final : BlockBase {
         if (!nAct(l)) return;
         float* rr = W[size_t(l)].r.template as<float>();
         float* dd = W[size_t(l)].d.template as<float>();
+        if constexpr (sizeof(T) == 4 && RB == 32 && MODE != dev::BOP_DOT) {
+            if (own16 && l == 0 && M->blockTc && M->nBtTiles > 0) {
+                // the mixed form's finest level on the tensor cores (TF32)
+                launch(dev::kb_tc<MODE>, M->nBtTiles, dev::BT_THREADS, dev::btSmemBytes(), D.view, static_cast<const dev::Coefs<float>&>(D.c32),
+                       M->btTiles.template as<uint32_t>(), xin, y, rr, dd, c1, c2, raw ? 1 : 0, ctl);
+                return;
+            }
+        }
         const auto& C = [&]() -> const dev::Coefs<T>& {
             if constexpr (sizeof(T) == 8) return D.c64;
             else return D.c32;

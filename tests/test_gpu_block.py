@@ -120,3 +120,22 @@ def test_precondition_block_matches_single():
     r_dev[1] *= 4.0
     S.precondition_block(6, r_dev.data_ptr(), z_dev.data_ptr(), torch.cuda.current_stream(dev).cuda_stream)
     assert rel(z_dev[1].cpu().numpy(), 4 * Z[1]) < 1e-12
+
+
+def test_mixed_block_on_the_tensor_cores_matches_the_oracle(monkeypatch):
+    """A 32-wide mixed block runs its finest-level V-cycle operator on the tensor cores (TF32 with
+    the translation removed per voxel): every right-hand side must still match the oracle's solve to
+    1e-6, with the iteration count of its CUDA-core block (PSFEA_BLOCK_TC=0) within 15 %."""
+    m = W.simp(24, 12, 12, nrhs=20, seed=11)
+    P = oracle.OracleModel("port", m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    tc = S.solve_batch(m.f, tol=1e-8, max_iter=3000, precision="mixed")
+    monkeypatch.setenv("PSFEA_BLOCK_TC", "0")
+    S0 = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    cc = S0.solve_batch(m.f, tol=1e-8, max_iter=3000, precision="mixed")
+    for q in range(20):
+        assert tc[q].converged and tc[q].residual <= 1e-7, (q, tc[q].iterations, tc[q].residual)
+        if q % 5 == 0:
+            uo, _, _, _ = P.solve(m.f[q], 1e-8, 3000)
+            assert rel(tc[q].u, uo) < 1e-6, q
+        assert abs(tc[q].iterations - cc[q].iterations) <= max(2, 0.15 * cc[q].iterations), (q, tc[q].iterations, cc[q].iterations)
