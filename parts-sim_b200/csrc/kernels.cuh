@@ -82,7 +82,8 @@ __device__ __forceinline__ void kbRows(const T* Kb, int a, const T xe[24], T t[3
         t[2] = t2;
     }
 }
-template <class T>
+// SMEM: M is in shared memory (plain loads; the read-only global path otherwise)
+template <class T, bool SMEM = false>
 __device__ __forceinline__ void own16Rows(const __half* M, const T xe[24], T t[3]) {
     const uint4* K16 = reinterpret_cast<const uint4*>(M);  // 72 halves: rows d at [24 d, 24 d + 24)
 #pragma unroll
@@ -90,7 +91,7 @@ __device__ __forceinline__ void own16Rows(const __half* M, const T xe[24], T t[3
         T acc = 0;
 #pragma unroll
         for (int g = 0; g < 3; g++) {
-            const uint4 u = __ldg(K16 + 3 * d + g);
+            const uint4 u = SMEM ? K16[3 * d + g] : __ldg(K16 + 3 * d + g);
             const uint32_t w[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
             for (int e = 0; e < 4; e++) {
@@ -117,8 +118,8 @@ __device__ __forceinline__ void own16Rows(const __half* M, const T xe[24], T t[3
 // x is read at node index n with row pitch XP (L.PX for the level's own vectors); the diagonal
 // shift at the level's node index nm. S: the stride between consecutive DOFs of x (1 for one
 // vector; the block width for the RHS-minor layout of a multi-RHS block, x then pointing at the
-// lane's right-hand side).
-template <class T, bool OWN16, bool DIFF = false, int S = 1>
+// lane's right-hand side). SMEM: L.own / L.own16 point at a copy in shared memory.
+template <class T, bool OWN16, bool DIFF = false, int S = 1, bool SMEM = false>
 __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, const T* __restrict__ x, int i, int j, int k,
                                         long long n, uint8_t mask, T acc[3], long long XP, long long nm) {
     acc[0] = acc[1] = acc[2] = T(0);
@@ -177,7 +178,7 @@ __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, c
                 acc[2] += s * t[2];
             } else if (OWN16) {
                 T t[3];
-                own16Rows<T>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a, xe, t);
+                own16Rows<T, SMEM>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a, xe, t);
                 acc[0] += T(L.hs) * t[0];
                 acc[1] += T(L.hs) * t[1];
                 acc[2] += T(L.hs) * t[2];
@@ -187,7 +188,7 @@ __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, c
                 for (int d = 0; d < 3; d++)
 #pragma unroll
                     for (int q = 0; q < 6; q++) {
-                        const float4 kv = __ldg(K4 + d * 6 + q);
+                        const float4 kv = SMEM ? K4[d * 6 + q] : __ldg(K4 + d * 6 + q);
                         acc[d] += T(kv.x) * xe[4 * q] + T(kv.y) * xe[4 * q + 1] + T(kv.z) * xe[4 * q + 2] + T(kv.w) * xe[4 * q + 3];
                     }
             }

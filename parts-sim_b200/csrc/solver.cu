@@ -549,6 +549,54 @@ __global__ void __launch_bounds__(NODE_THREADS) k_bnd(LevelView L, Coefs<T> C, c
     }
 }
 
+// The same list-driven boundary-node pass (FP32 modes) for levels whose Galerkin matrices come in
+// few classes: each CTA (persistent, one per SM) first copies every class matrix into shared
+// memory, then gathers the rows from there. The class matrices are shared by thousands of voxels,
+// so the per-thread row loads, scattered over the matrices, hit a shared-memory copy instead of
+// queueing in the L1 (the global-load form of this pass is bound by L1 wavefronts). Sums as in k_bnd.
+template <int MODE, bool OWN16>
+__global__ void __launch_bounds__(512) k_bnd_cls(LevelView L, Coefs<float> C, const int* __restrict__ list, int count, int nClass,
+                                                  const float* __restrict__ x, float* __restrict__ y, const float* __restrict__ r,
+                                                  float* __restrict__ d, float c1, float c2, int raw, Ctl ctl) {
+    if (skipped(ctl)) return;
+    extern __shared__ __align__(16) unsigned char clsRaw[];
+    const size_t bytes = size_t(nClass) * 576 * (OWN16 ? 2 : 4);
+    const uint4* src = reinterpret_cast<const uint4*>(OWN16 ? static_cast<const void*>(L.own16) : static_cast<const void*>(L.own));
+    uint4* dst = reinterpret_cast<uint4*>(clsRaw);
+    for (size_t e = threadIdx.x; e < bytes / 16; e += blockDim.x) dst[e] = __ldg(src + e);
+    __syncthreads();
+    LevelView Ls = L;
+    if (OWN16) Ls.own16 = reinterpret_cast<const __half*>(clsRaw);
+    else Ls.own = reinterpret_cast<const float*>(clsRaw);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count; t += (long long)gridDim.x * blockDim.x) {
+        const long long n = list[t];
+        const uint8_t mask = __ldg(L.nmask + n);
+        int i, j, k;
+        nodeCoords(L, n, i, j, k);
+        float acc[3];
+        applyAt<float, OWN16, false, 1, true>(Ls, C, x, i, j, k, n, mask, acc, L.PX, n);
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const long long id = 3 * n + q;
+            const bool fx = fixedDof(mask, q);
+            if (MODE == TOP_APPLY) {
+                y[id] = (!raw && fx) ? 0.f : acc[q];
+            } else if (MODE == TOP_RESID) {
+                y[id] = fx ? 0.f : r[id] - acc[q];
+            } else {
+                if (fx) {
+                    d[id] = 0.f;
+                    y[id] = 0.f;
+                } else {
+                    const float dn = c1 * d[id] + c2 * L.invD[id] * (r[id] - acc[q]);
+                    d[id] = dn;
+                    y[id] = x[id] + dn;
+                }
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------- V-cycle pieces (32-bit)
 
 // z = d = c0 D^-1 r (the first Chebyshev step from zero)
@@ -1343,6 +1391,7 @@ struct DevLevel {
     float cf0 = 0, cf1 = 0, cf2 = 0, omega = 0.5f;
     std::vector<float> chebC1, chebC2;  // steps 1 .. degree-1 of the Chebyshev smoother: d = c1 d + c2 D^-1 (r - K z)
     bool hasOwn = false;
+    int nOwnDev = 0;  // own matrices on the device (classes when they are shared)
     // the tensor-core element-block operator (levels without Galerkin matrices): its 8 x 8 x 4 tiles
     DevMem ebeTiles;
     int nEbeTiles = 0;
@@ -1387,6 +1436,9 @@ struct SharedModel {
     // PSFEA_EBE, PSFEA_EBE_SPLIT
     int64_t ebeLevels = 0;
     int ebeSplit = 3;
+    // boundary passes gather Galerkin classes from shared memory when they fit in this many bytes
+    // (PSFEA_CLS_SMEM; 0 = never)
+    size_t clsSmemMax = 200 * 1024;
     cudaStream_t ms = nullptr;     // allocation / upload stream of the shared data
     cudaEvent_t readyEv = nullptr; // recorded when the uploads are done; contexts wait on it
 
@@ -1434,6 +1486,7 @@ void SharedModel::adopt(Hierarchy&& h) {
     if (const char* e = std::getenv("PSFEA_MIXED_OWN32")) mixedOwn16 = std::atoi(e) == 0;
     if (const char* e = std::getenv("PSFEA_OWN_DEDUP")) ownDedup = std::atoi(e) != 0;
     if (const char* e = std::getenv("PSFEA_EBE")) ebeLevels = std::atoll(e);
+    if (const char* e = std::getenv("PSFEA_CLS_SMEM")) clsSmemMax = size_t(std::atoll(e));
     if (const char* e = std::getenv("PSFEA_EBE_SPLIT")) ebeSplit = std::atoi(e) == 1 ? 1 : 3;
     check(cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking), "stream");
     check(cudaEventCreateWithFlags(&readyEv, cudaEventDisableTiming), "event");
@@ -1466,6 +1519,12 @@ void SharedModel::adopt(Hierarchy&& h) {
         set(dev::k_ebe<dev::TOP_APPLY, 3>, dev::ebeSmemBytes<3>());
         set(dev::k_ebe<dev::TOP_CHEB, 3>, dev::ebeSmemBytes<3>());
         set(dev::k_ebe<dev::TOP_RESID, 3>, dev::ebeSmemBytes<3>());
+        set(dev::k_bnd_cls<dev::TOP_CHEB, true>, 200 * 1024);
+        set(dev::k_bnd_cls<dev::TOP_CHEB, false>, 200 * 1024);
+        set(dev::k_bnd_cls<dev::TOP_RESID, true>, 200 * 1024);
+        set(dev::k_bnd_cls<dev::TOP_RESID, false>, 200 * 1024);
+        set(dev::k_bnd_cls<dev::TOP_APPLY, true>, 200 * 1024);
+        set(dev::k_bnd_cls<dev::TOP_APPLY, false>, 200 * 1024);
         set(dev::kb_tc<dev::BOP_APPLY>, dev::btSmemBytes());
         set(dev::kb_tc<dev::BOP_CHEB>, dev::btSmemBytes());
         set(dev::kb_tc<dev::BOP_RESID>, dev::btSmemBytes());
@@ -1518,6 +1577,7 @@ void SharedModel::uploadLevel(int l) {
         }
     }
     const auto& own = *ownSrc;
+    D.nOwnDev = int(own.size() / 576);
     upload(D.word, words, bytes, ms);
     upload(D.nmask, pitched<uint8_t>(h.nmask, 1, h, PX, uint8_t(7)), bytes, ms);  // padding: inactive, all held
     D.hasOwn = h.nOwn > 0;
@@ -1949,8 +2009,18 @@ void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev
         else if (o16) launch(dev::k_tile<float, TM, true, false, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
         else launch(dev::k_tile<float, TM, false, false, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
         if (!D.nBnd) return;
-        const int g = gridFor(D.nBnd, dev::NODE_THREADS, smCount * 16);
         const int* bl = D.blist.as<int>();
+        if (!diff && D.hasOwn) {
+            // few Galerkin classes: the boundary pass gathers from a shared-memory copy of them
+            const size_t cls = size_t(D.nOwnDev) * 576 * (o16 ? 2 : 4);
+            if (cls <= M->clsSmemMax) {
+                const int gc = std::min(smCount, (D.nBnd + 511) / 512);
+                if (o16) launch(dev::k_bnd_cls<TM, true>, gc, 512, cls, stream, D.view, c, bl, D.nBnd, D.nOwnDev, xin, y, rr, dd, c1, c2, 0, ctl);
+                else launch(dev::k_bnd_cls<TM, false>, gc, 512, cls, stream, D.view, c, bl, D.nBnd, D.nOwnDev, xin, y, rr, dd, c1, c2, 0, ctl);
+                return;
+            }
+        }
+        const int g = gridFor(D.nBnd, dev::NODE_THREADS, smCount * 16);
         if (diff) launch(dev::k_bnd<float, TM, true, true>, g, dev::NODE_THREADS, 0, stream, D.view, c, bl, D.nBnd, xin, y, rr, dd, c1, c2, 0, st(), part(), tick(), ctl);
         else if (o16) launch(dev::k_bnd<float, TM, true, false>, g, dev::NODE_THREADS, 0, stream, D.view, c, bl, D.nBnd, xin, y, rr, dd, c1, c2, 0, st(), part(), tick(), ctl);
         else launch(dev::k_bnd<float, TM, false, false>, g, dev::NODE_THREADS, 0, stream, D.view, c, bl, D.nBnd, xin, y, rr, dd, c1, c2, 0, st(), part(), tick(), ctl);
