@@ -1460,11 +1460,11 @@ struct SharedModel {
     std::vector<DevMem> act;
     std::vector<int> nAct;
     // the finest level's 8 x 4 x 4 node tiles with an active node, for the block tensor-core
-    // operator (built with the active lists); PSFEA_BLOCK_TC=0 keeps the mixed block form on the
-    // CUDA cores
+    // operator (built with the active lists); PSFEA_BLOCK_TC=1 runs the mixed block form's finest
+    // level on it (measured slower than the CUDA-core block kernel, so off by default)
     DevMem btTiles;
     int nBtTiles = 0;
-    bool blockTc = true;
+    bool blockTc = false;
 
     void build(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsest, const double* diagAdd);
     void adopt(Hierarchy&& h);  // upload a hierarchy built on the host beforehand

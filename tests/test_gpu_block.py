@@ -123,11 +123,12 @@ def test_precondition_block_matches_single():
 
 
 def test_mixed_block_on_the_tensor_cores_matches_the_oracle(monkeypatch):
-    """A 32-wide mixed block runs its finest-level V-cycle operator on the tensor cores (TF32 with
+    """A 32-wide mixed block with PSFEA_BLOCK_TC=1 runs its finest-level V-cycle operator on the tensor cores (TF32 with
     the translation removed per voxel): every right-hand side must still match the oracle's solve to
     1e-6, with the iteration count of its CUDA-core block (PSFEA_BLOCK_TC=0) within 15 %."""
     m = W.simp(24, 12, 12, nrhs=20, seed=11)
     P = oracle.OracleModel("port", m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    monkeypatch.setenv("PSFEA_BLOCK_TC", "1")
     S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
     tc = S.solve_batch(m.f, tol=1e-8, max_iter=3000, precision="mixed")
     monkeypatch.setenv("PSFEA_BLOCK_TC", "0")
