@@ -118,7 +118,7 @@ enum { BOP_APPLY = 0, BOP_CHEB = 1, BOP_RESID = 2, BOP_DOT = 3 };
 // 0 for the voxels below the node, 0 and +1 for those above): the same sums in the same order as
 // applyAt (so bitwise the same), with 81 loads instead of up to 192 on nodes that take the per-voxel
 // gather. Neighbours outside the grid read 0; they only ever meet empty voxels.
-template <class T, bool OWN16, int S>
+template <class T, bool OWN16, int S, bool SMEM = false>
 __device__ __forceinline__ void applyNbr(const LevelView& L, const Coefs<T>& C, const T* __restrict__ x, int i, int j, int k, long long n,
                                          uint8_t mask, T acc[3]) {
     acc[0] = acc[1] = acc[2] = T(0);
@@ -191,7 +191,7 @@ __device__ __forceinline__ void applyNbr(const LevelView& L, const Coefs<T>& C, 
                 acc[2] += sc * t[2];
             } else if (OWN16) {
                 T t[3];
-                own16Rows<T>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a, xe, t);
+                own16Rows<T, SMEM>(L.own16 + (long long)(w & ~OWN_BIT) * 576 + 72 * a, xe, t);
                 acc[0] += T(L.hs) * t[0];
                 acc[1] += T(L.hs) * t[1];
                 acc[2] += T(L.hs) * t[2];
@@ -201,7 +201,7 @@ __device__ __forceinline__ void applyNbr(const LevelView& L, const Coefs<T>& C, 
                 for (int d = 0; d < 3; d++)
 #pragma unroll
                     for (int q = 0; q < 6; q++) {
-                        const float4 kv = __ldg(K4 + d * 6 + q);
+                        const float4 kv = SMEM ? K4[d * 6 + q] : __ldg(K4 + d * 6 + q);
                         acc[d] += T(kv.x) * xe[4 * q] + T(kv.y) * xe[4 * q + 1] + T(kv.z) * xe[4 * q + 2] + T(kv.w) * xe[4 * q + 3];
                     }
             }

@@ -549,54 +549,6 @@ __global__ void __launch_bounds__(NODE_THREADS) k_bnd(LevelView L, Coefs<T> C, c
     }
 }
 
-// The same list-driven boundary-node pass (FP32 modes) for levels whose Galerkin matrices come in
-// few classes: each CTA (persistent, one per SM) first copies every class matrix into shared
-// memory, then gathers the rows from there. The class matrices are shared by thousands of voxels,
-// so the per-thread row loads, scattered over the matrices, hit a shared-memory copy instead of
-// queueing in the L1 (the global-load form of this pass is bound by L1 wavefronts). Sums as in k_bnd.
-template <int MODE, bool OWN16>
-__global__ void __launch_bounds__(512) k_bnd_cls(LevelView L, Coefs<float> C, const int* __restrict__ list, int count, int nClass,
-                                                  const float* __restrict__ x, float* __restrict__ y, const float* __restrict__ r,
-                                                  float* __restrict__ d, float c1, float c2, int raw, Ctl ctl) {
-    if (skipped(ctl)) return;
-    extern __shared__ __align__(16) unsigned char clsRaw[];
-    const size_t bytes = size_t(nClass) * 576 * (OWN16 ? 2 : 4);
-    const uint4* src = reinterpret_cast<const uint4*>(OWN16 ? static_cast<const void*>(L.own16) : static_cast<const void*>(L.own));
-    uint4* dst = reinterpret_cast<uint4*>(clsRaw);
-    for (size_t e = threadIdx.x; e < bytes / 16; e += blockDim.x) dst[e] = __ldg(src + e);
-    __syncthreads();
-    LevelView Ls = L;
-    if (OWN16) Ls.own16 = reinterpret_cast<const __half*>(clsRaw);
-    else Ls.own = reinterpret_cast<const float*>(clsRaw);
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count; t += (long long)gridDim.x * blockDim.x) {
-        const long long n = list[t];
-        const uint8_t mask = __ldg(L.nmask + n);
-        int i, j, k;
-        nodeCoords(L, n, i, j, k);
-        float acc[3];
-        applyAt<float, OWN16, false, 1, true>(Ls, C, x, i, j, k, n, mask, acc, L.PX, n);
-#pragma unroll
-        for (int q = 0; q < 3; q++) {
-            const long long id = 3 * n + q;
-            const bool fx = fixedDof(mask, q);
-            if (MODE == TOP_APPLY) {
-                y[id] = (!raw && fx) ? 0.f : acc[q];
-            } else if (MODE == TOP_RESID) {
-                y[id] = fx ? 0.f : r[id] - acc[q];
-            } else {
-                if (fx) {
-                    d[id] = 0.f;
-                    y[id] = 0.f;
-                } else {
-                    const float dn = c1 * d[id] + c2 * L.invD[id] * (r[id] - acc[q]);
-                    d[id] = dn;
-                    y[id] = x[id] + dn;
-                }
-            }
-        }
-    }
-}
-
 // ---------------------------------------------------------------- V-cycle pieces (32-bit)
 
 // z = d = c0 D^-1 r (the first Chebyshev step from zero)
@@ -1236,6 +1188,60 @@ __global__ void k_reactions(long long nNodes, const uint8_t* __restrict__ nmask,
 #include "block_kernels.cuh"  // the multi-RHS kernels (they use the control helpers above)
 #include "ebe_kernels.cuh"    // the tensor-core element-block operator
 #include "block_tc.cuh"       // the block operator on the tensor cores
+
+namespace psfea {
+namespace dev {
+
+// The same list-driven boundary-node pass (FP32 modes) for levels whose Galerkin matrices come in
+// few classes: each CTA (persistent, one per SM) first copies every class matrix into shared
+// memory and gathers the rows from there, and each node's 27 neighbours are read once, two z-planes
+// at a time (81 loads instead of up to 192): the global-load form of this pass is bound by L1
+// wavefronts. The same sums in the same order as k_bnd (bitwise).
+template <int MODE, bool OWN16>
+__global__ void __launch_bounds__(512) k_bnd_cls(LevelView L, Coefs<float> C, const int* __restrict__ list, int count, int nClass,
+                                                  const float* __restrict__ x, float* __restrict__ y, const float* __restrict__ r,
+                                                  float* __restrict__ d, float c1, float c2, int raw, Ctl ctl) {
+    if (skipped(ctl)) return;
+    extern __shared__ __align__(16) unsigned char clsRaw[];
+    const size_t bytes = size_t(nClass) * 576 * (OWN16 ? 2 : 4);
+    const uint4* src = reinterpret_cast<const uint4*>(OWN16 ? static_cast<const void*>(L.own16) : static_cast<const void*>(L.own));
+    uint4* dst = reinterpret_cast<uint4*>(clsRaw);
+    for (size_t e = threadIdx.x; e < bytes / 16; e += blockDim.x) dst[e] = __ldg(src + e);
+    __syncthreads();
+    LevelView Ls = L;
+    if (OWN16) Ls.own16 = reinterpret_cast<const __half*>(clsRaw);
+    else Ls.own = reinterpret_cast<const float*>(clsRaw);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count; t += (long long)gridDim.x * blockDim.x) {
+        const long long n = list[t];
+        const uint8_t mask = __ldg(L.nmask + n);
+        int i, j, k;
+        nodeCoords(L, n, i, j, k);
+        float acc[3];
+        applyNbr<float, OWN16, 1, true>(Ls, C, x, i, j, k, n, mask, acc);
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const long long id = 3 * n + q;
+            const bool fx = fixedDof(mask, q);
+            if (MODE == TOP_APPLY) {
+                y[id] = (!raw && fx) ? 0.f : acc[q];
+            } else if (MODE == TOP_RESID) {
+                y[id] = fx ? 0.f : r[id] - acc[q];
+            } else {
+                if (fx) {
+                    d[id] = 0.f;
+                    y[id] = 0.f;
+                } else {
+                    const float dn = c1 * d[id] + c2 * L.invD[id] * (r[id] - acc[q]);
+                    d[id] = dn;
+                    y[id] = x[id] + dn;
+                }
+            }
+        }
+    }
+}
+
+}  // namespace dev
+}  // namespace psfea
 
 namespace psfea {
 
