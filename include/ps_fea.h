@@ -61,7 +61,18 @@ typedef enum ps_precision {
      * updates: whenever the FP32 residual has dropped tenfold the FP32 iterate is folded into the
      * FP64 solution and the FP64 defect f - K u replaces the FP32 residual. On ill-conditioned
      * models the FP32 recurrence needs markedly more iterations than the FP64 one. */
-    PS_PREC_FP32 = 2
+    PS_PREC_FP32 = 2,
+    /* FP64 iterative refinement around an FP32 flexible PCG whose V-cycle keeps every level below
+     * the finest in FP16 vectors: the outer FP64 step forms the defect f - K u, rescales it to
+     * max |r| = 1 and restarts the inner FP32 recurrence on it, which runs until its residual has
+     * fallen by the refinement factor (0.1; PSFEA_REFINE_ETA), when its iterate is added to u in
+     * FP64. Levels >= 1 store residuals r * 8^-l and iterates x * 8^-l * delta_l (delta_l a
+     * power of two near the level's median diagonal over 16), so that both sit near order one in
+     * FP16 with headroom; every scale is a power of two and the operator sums run in FP32.
+     * FP16 element matrices as in PS_PREC_MIXED. One scale per level cannot hold graded
+     * stiffness: where a level's diagonal spans more than a factor 256 (SIMP densities), the
+     * coarse vectors stay FP32 and only the refinement remains. */
+    PS_PREC_HALF = 3
 } ps_precision;
 
 typedef struct ps_fea ps_fea_t;

@@ -118,8 +118,9 @@ enum { BOP_APPLY = 0, BOP_CHEB = 1, BOP_RESID = 2, BOP_DOT = 3 };
 // 0 for the voxels below the node, 0 and +1 for those above): the same sums in the same order as
 // applyAt (so bitwise the same), with 81 loads instead of up to 192 on nodes that take the per-voxel
 // gather. Neighbours outside the grid read 0; they only ever meet empty voxels.
-template <class T, bool OWN16, int S, bool SMEM = false>
-__device__ __forceinline__ void applyNbr(const LevelView& L, const Coefs<T>& C, const T* __restrict__ x, int i, int j, int k, long long n,
+// V: the storage type of x (T, or __half for the FP16 coarse-level vectors; converted on load).
+template <class T, bool OWN16, int S, bool SMEM = false, class V = T>
+__device__ __forceinline__ void applyNbr(const LevelView& L, const Coefs<T>& C, const V* __restrict__ x, int i, int j, int k, long long n,
                                          uint8_t mask, T acc[3]) {
     acc[0] = acc[1] = acc[2] = T(0);
     if (!(mask & NM_ACTIVE)) return;
@@ -129,10 +130,10 @@ __device__ __forceinline__ void applyNbr(const LevelView& L, const Coefs<T>& C, 
         for (int b = 0; b < 9; b++) {
             const int ox = b % 3 - 1, oy = b / 3 - 1;
             const bool in = i + ox >= 0 && j + oy >= 0 && k + oz >= 0 && i + ox < L.NX && j + oy < L.NY && k + oz < L.NZ;
-            const T* xp = x + 3 * S * (n + ox + oy * NX + oz * NXY);
-            P[b][0] = in ? __ldg(xp) : T(0);
-            P[b][1] = in ? __ldg(xp + S) : T(0);
-            P[b][2] = in ? __ldg(xp + 2 * S) : T(0);
+            const V* xp = x + 3 * S * (n + ox + oy * NX + oz * NXY);
+            P[b][0] = in ? ldv<T>(xp) : T(0);
+            P[b][1] = in ? ldv<T>(xp + S) : T(0);
+            P[b][2] = in ? ldv<T>(xp + 2 * S) : T(0);
         }
     };
     T A[9][3], B[9][3];  // A: planes -1 then +1; B: plane 0

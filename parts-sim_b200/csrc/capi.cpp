@@ -82,7 +82,7 @@ ps_status ps_fea_solve(ps_fea_t* h, const double* f, const ps_solve_opts* opts, 
     return guarded([&] {
         if (!h || !f || !u_out) return fail(PS_EINVAL, "Force or displacement vector has the wrong size.");
         const ps_solve_opts o = resolve(opts);
-        if (!(o.tol >= 0) || o.max_iter < 0 || (o.precision < PS_PREC_FP64 || o.precision > PS_PREC_FP32) || o.smoother_degree < 0 ||
+        if (!(o.tol >= 0) || o.max_iter < 0 || (o.precision < PS_PREC_FP64 || o.precision > PS_PREC_HALF) || o.smoother_degree < 0 ||
             o.smoother_degree > 8)
             return fail(PS_EINVAL, "invalid solve options");
         ps_solve_result r{};
@@ -96,7 +96,7 @@ ps_status ps_fea_solve_dev(ps_fea_t* h, const double* f_dev, const ps_solve_opts
     return guarded([&] {
         if (!h || !f_dev || !u_dev) return fail(PS_EINVAL, "Force or displacement vector has the wrong size.");
         const ps_solve_opts o = resolve(opts);
-        if (!(o.tol >= 0) || o.max_iter < 0 || (o.precision < PS_PREC_FP64 || o.precision > PS_PREC_FP32) || o.smoother_degree < 0 ||
+        if (!(o.tol >= 0) || o.max_iter < 0 || (o.precision < PS_PREC_FP64 || o.precision > PS_PREC_HALF) || o.smoother_degree < 0 ||
             o.smoother_degree > 8)
             return fail(PS_EINVAL, "invalid solve options");
         ps_solve_result r{};
@@ -110,7 +110,7 @@ ps_status ps_fea_solve_batch(ps_fea_t* h, int32_t nrhs, const double* f, const p
     return guarded([&] {
         if (!h || !f || !u_out || nrhs < 0) return fail(PS_EINVAL, "Force or displacement vector has the wrong size.");
         const ps_solve_opts base = resolve(opts);
-        if (!(base.tol >= 0) || base.max_iter < 0 || (base.precision < PS_PREC_FP64 || base.precision > PS_PREC_FP32) ||
+        if (!(base.tol >= 0) || base.max_iter < 0 || (base.precision < PS_PREC_FP64 || base.precision > PS_PREC_HALF) ||
             base.smoother_degree < 0 || base.smoother_degree > 8)
             return fail(PS_EINVAL, "invalid solve options");
         if (nrhs == 0) return PS_OK;
@@ -149,7 +149,7 @@ ps_status ps_topology_run(const int32_t dims[3], const float* fill, const uint8_
         ps_topology_opts_default(&o);
         if (opts) o = *opts;
         if (!(o.vol_frac > 0 && o.vol_frac <= 1) || !(o.penal >= 1) || !(o.rmin > 0) || !(o.move > 0) || o.max_iter < 0 || !(o.solve_tol > 0) ||
-            o.precision < PS_PREC_FP64 || o.precision > PS_PREC_FP32)
+            o.precision < PS_PREC_FP64 || o.precision > PS_PREC_HALF)
             return fail(PS_EINVAL, "invalid topology options");
         if (!psfea::deviceAvailable()) return fail(PS_ENODEV, "no CUDA device is available");
         psfea::TopologyOptions to;
@@ -223,7 +223,7 @@ void toC(const psfea::TuneResult& t, int64_t coarsest, ps_tune_result* out) {
     out->default_seconds = t.defaultSeconds;
 }
 bool validOpts(const ps_solve_opts& o) {
-    return o.tol >= 0 && o.max_iter >= 0 && o.precision >= PS_PREC_FP64 && o.precision <= PS_PREC_FP32 && o.smoother_degree >= 0 &&
+    return o.tol >= 0 && o.max_iter >= 0 && o.precision >= PS_PREC_FP64 && o.precision <= PS_PREC_HALF && o.smoother_degree >= 0 &&
            o.smoother_degree <= 8;
 }
 }  // namespace

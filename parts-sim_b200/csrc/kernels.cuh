@@ -200,6 +200,18 @@ __device__ __forceinline__ void applyAt(const LevelView& L, const Coefs<T>& C, c
     }
 }
 
+// a read-only vector entry as T: FP32 / FP64 storage as is, FP16 storage converted
+template <class T>
+__device__ __forceinline__ T ldv(const float* p) { return T(__ldg(p)); }
+template <class T>
+__device__ __forceinline__ T ldv(const double* p) { return T(__ldg(p)); }
+template <class T>
+__device__ __forceinline__ T ldv(const __half* p) { return T(__half2float(__ldg(p))); }
+__device__ __forceinline__ void stv(float* p, float v) { *p = v; }
+__device__ __forceinline__ void stv(__half* p, float v) { *p = __float2half_rn(v); }
+__device__ __forceinline__ float ldf(const float* p) { return *p; }
+__device__ __forceinline__ float ldf(const __half* p) { return __half2float(*p); }
+
 __device__ __forceinline__ void nodeCoords(const LevelView& L, long long n, int& i, int& j, int& k) {
     if (n <= 0xffffffffLL) {  // two 32-bit divisions: a 64-bit one is a long software sequence
         const unsigned u = unsigned(n), px = unsigned(L.PX), ny = unsigned(L.NY);

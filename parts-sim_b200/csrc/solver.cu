@@ -26,6 +26,7 @@
 #include <map>
 #include <memory>
 #include <tuple>
+#include <type_traits>
 #include <mutex>
 #include <thread>
 #include <cmath>
@@ -50,6 +51,10 @@ struct SolveState {
     double vscale;  // the scale the current FP32 right-hand side r32 was made with (r32 = r * vscale)
     int it, maxIter, done, status, fold, folds, first, mixed;
     int err;  // a device-side failure (ST_ERR_*): the solve is ended and reported as a CUDA error
+    // iterative refinement (PS_PREC_HALF): each fold rescales the FP32 residual to max |r| = 1
+    // (r32 *= rescale, due while restart is set) and restarts the FP32 recurrence (beta = 0)
+    int refine, restart;
+    double rescale;
 };
 enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_BREAKDOWN = 3 };
 
@@ -551,21 +556,25 @@ __global__ void __launch_bounds__(NODE_THREADS) k_bnd(LevelView L, Coefs<T> C, c
 
 // ---------------------------------------------------------------- V-cycle pieces (32-bit)
 
-// z = d = c0 D^-1 r (the first Chebyshev step from zero)
-__global__ void k_cheb_first(long long nDof, const float* __restrict__ r, const float* __restrict__ invD, float* __restrict__ d,
-                             float* __restrict__ z, float c0, Ctl ctl) {
+// z = d = c0 D^-1 r (the first Chebyshev step from zero); V = __half: the FP16 coarse-level
+// vectors, c0 carrying the level's iterate-to-residual scale
+template <class V = float>
+__global__ void k_cheb_first(long long nDof, const V* __restrict__ r, const float* __restrict__ invD, V* __restrict__ d, V* __restrict__ z,
+                             float c0, Ctl ctl) {
     if (skipped(ctl)) return;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x) {
-        const float v = c0 * invD[i] * r[i];
-        d[i] = v;
-        z[i] = v;
+        const float v = c0 * invD[i] * ldf(r + i);
+        stv(d + i, v);
+        stv(z + i, v);
     }
 }
 
 // rc = P^T rf gathered per coarse node: fine 2I (weight 1) and 2I +- 1 (weight 1/2) per axis;
-// held / inactive coarse DOFs 0
-__global__ void k_restrict(LevelView F, LevelView C, const float* __restrict__ rf, float* __restrict__ rc, float* __restrict__ dc,
-                           float* __restrict__ zc, float c0, Ctl ctl) {
+// held / inactive coarse DOFs 0. VF / VC: the fine / coarse storage (float, or __half for the FP16
+// coarse-level vectors, whose residual scales differ by the power of two sr: rc = sr P^T rf).
+template <class VF = float, class VC = float>
+__global__ void k_restrict(LevelView F, LevelView C, const VF* __restrict__ rf, VC* __restrict__ rc, VC* __restrict__ dc,
+                           VC* __restrict__ zc, float c0, float sr, Ctl ctl) {
     if (skipped(ctl)) return;
     const int FNX = F.NX, FNY = F.NY, FNZ = F.NZ;
     const long long FPX = F.PX, FPXY = (long long)F.PX * F.NY;
@@ -587,30 +596,33 @@ __global__ void k_restrict(LevelView F, LevelView C, const float* __restrict__ r
                         const int i = 2 * I + di;
                         if (i < 0 || i >= FNX) continue;
                         const float w = (di ? 0.5f : 1.f) * wj;
-                        const float* p = rf + 3 * (i + j * FPX + k * FPXY);
-                        s0 += w * p[0];
-                        s1 += w * p[1];
-                        s2 += w * p[2];
+                        const VF* p = rf + 3 * (i + j * FPX + k * FPXY);
+                        s0 += w * ldf(p);
+                        s1 += w * ldf(p + 1);
+                        s2 += w * ldf(p + 2);
                     }
                 }
             }
         }
         const float sv[3] = {s0, s1, s2};
+        constexpr bool SCALED = !std::is_same<VC, float>::value;
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-            const float v = fixedDof(mask, q) ? 0.f : sv[q];
-            rc[3 * cn + q] = v;
+            const float v = fixedDof(mask, q) ? 0.f : (SCALED ? sr * sv[q] : sv[q]);
+            stv(rc + 3 * cn + q, v);
             if (dc) {  // the coarse level's first smoothing step, d = z = c0 D^-1 r
                 const float dv = c0 * C.invD[3 * cn + q] * v;
-                dc[3 * cn + q] = dv;
-                zc[3 * cn + q] = dv;
+                stv(dc + 3 * cn + q, dv);
+                stv(zc + 3 * cn + q, dv);
             }
         }
     }
 }
 
-// zf += P zc at free fine DOFs (trilinear: coarse i/2 and, when odd, (i+1)/2, weight 1/2 each)
-__global__ void k_prolong(LevelView F, int CPX, int CNY, const float* __restrict__ zc, float* __restrict__ zf, Ctl ctl) {
+// zf += P zc at free fine DOFs (trilinear: coarse i/2 and, when odd, (i+1)/2, weight 1/2 each);
+// VC / VF as in k_restrict, the iterate scales differing by the power of two sp: zf += sp P zc
+template <class VC = float, class VF = float>
+__global__ void k_prolong(LevelView F, int CPX, int CNY, const VC* __restrict__ zc, VF* __restrict__ zf, float sp, Ctl ctl) {
     if (skipped(ctl)) return;
     const long long CNX = CPX, CNXY = (long long)CPX * CNY;
     for (long long fn = blockIdx.x * (long long)blockDim.x + threadIdx.x; fn < F.nNodes; fn += (long long)gridDim.x * blockDim.x) {
@@ -625,25 +637,32 @@ __global__ void k_prolong(LevelView F, int CPX, int CNY, const float* __restrict
         for (int c = 0; c < nk; c++)
             for (int b = 0; b < nj; b++)
                 for (int a = 0; a < ni; a++) {
-                    const float* p = zc + 3 * ((i0 + a) + (j0 + b) * CNX + (k0 + c) * CNXY);
-                    s0 += w * p[0];
-                    s1 += w * p[1];
-                    s2 += w * p[2];
+                    const VC* p = zc + 3 * ((i0 + a) + (j0 + b) * CNX + (k0 + c) * CNXY);
+                    s0 += w * ldf(p);
+                    s1 += w * ldf(p + 1);
+                    s2 += w * ldf(p + 2);
                 }
-        if (!fixedDof(mask, 0)) zf[3 * fn] += s0;
-        if (!fixedDof(mask, 1)) zf[3 * fn + 1] += s1;
-        if (!fixedDof(mask, 2)) zf[3 * fn + 2] += s2;
+        constexpr bool SCALED = !std::is_same<VC, float>::value;
+        if (SCALED) {
+            s0 *= sp;
+            s1 *= sp;
+            s2 *= sp;
+        }
+        if (!fixedDof(mask, 0)) stv(zf + 3 * fn, ldf(zf + 3 * fn) + s0);
+        if (!fixedDof(mask, 1)) stv(zf + 3 * fn + 1, ldf(zf + 3 * fn + 1) + s1);
+        if (!fixedDof(mask, 2)) stv(zf + 3 * fn + 2, ldf(zf + 3 * fn + 2) + s2);
     }
 }
 
 // coarsest level: z = A^-1 r over the m free DOFs (FP64 dense inverse, one warp per row);
 // r, z are the level's vectors (float or double), held DOFs of z are never written (stay 0)
+// (zs: the FP16 coarse-level vectors' iterate-to-residual scale, a power of two; 1 otherwise)
 template <class TI, class TO>
 __global__ void k_coarse(int m, const int* __restrict__ dof, const double* __restrict__ Ainv, const TI* __restrict__ r, TO* __restrict__ z,
-                         Ctl ctl) {
+                         double zs, Ctl ctl) {
     if (skipped(ctl)) return;
     extern __shared__ double rs[];
-    for (int q = threadIdx.x; q < m; q += blockDim.x) rs[q] = double(r[dof[q]]);
+    for (int q = threadIdx.x; q < m; q += blockDim.x) rs[q] = ldv<double>(r + dof[q]);
     __syncthreads();
     const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
     for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < m; row += gridDim.x * warps) {
@@ -652,7 +671,10 @@ __global__ void k_coarse(int m, const int* __restrict__ dof, const double* __res
         for (int c = lane; c < m; c += 32) s += a[c] * rs[c];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (lane == 0) z[dof[row]] = TO(s);
+        if (lane == 0) {
+            if constexpr (std::is_same<TO, __half>::value) z[dof[row]] = __double2half(s * zs);
+            else z[dof[row]] = TO(s);
+        }
     }
 }
 
@@ -891,7 +913,7 @@ __global__ void k_mx_fold2(long long nNodes, const uint8_t* __restrict__ nmask, 
                            float* __restrict__ r32, SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
     if (skipped(ctl)) return;
     const double s = st->scale;
-    double v[1] = {0};
+    double v[2] = {0, 0};
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
         const uint8_t mask = nmask[n];
 #pragma unroll
@@ -900,11 +922,18 @@ __global__ void k_mx_fold2(long long nNodes, const uint8_t* __restrict__ nmask, 
             double rv = 0;
             if (!fixedDof(mask, c)) rv = f[id] - q[id];
             v[0] += rv * rv;
+            v[1] = fmax(v[1], fabs(rv));
             r32[id] = float(rv * s);
         }
     }
-    double tot[1];
-    if (gridReduce<1>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) {
+    double tot[2];
+    if (gridReduce<2>(v, 2u, partials, ticket, tot) && threadIdx.x == 0) {
+        if (st->refine && tot[1] > 0) {
+            // the next inner solve starts from the defect scaled to max |r| = 1
+            st->rescale = (1.0 / tot[1]) / s;
+            st->scale = 1.0 / tot[1];
+            st->restart = 1;
+        }
         st->rel = sqrt(tot[0]) / st->bnorm;
         st->peak = st->rel;
         st->folds += 1;
@@ -932,9 +961,17 @@ __global__ void k_mx_dots(long long nDof, const float* __restrict__ r, const flo
     }
     double tot[2];
     if (gridReduce<2>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) {
-        st->beta = first ? 0.0 : fmax(0.0, -st->alpha * tot[1] / st->rz);
+        st->beta = (first || st->restart) ? 0.0 : fmax(0.0, -st->alpha * tot[1] / st->rz);
         st->rz = tot[0];
+        st->restart = 0;
     }
+}
+
+// after a refinement fold: r32 *= rescale (runs while st->restart is set)
+__global__ void k_mx_rescale(long long nDof, float* __restrict__ r32, const SolveState* st, Ctl ctl) {
+    if (skipped(ctl)) return;
+    const float f = float(st->rescale);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x) r32[i] *= f;
 }
 
 __global__ void k_mx_p(long long nDof, const float* __restrict__ z, float* __restrict__ p, const SolveState* st, Ctl ctl) {
@@ -1188,52 +1225,62 @@ __global__ void k_reactions(long long nNodes, const uint8_t* __restrict__ nmask,
 #include "block_kernels.cuh"  // the multi-RHS kernels (they use the control helpers above)
 #include "ebe_kernels.cuh"    // the tensor-core element-block operator
 #include "block_tc.cuh"       // the block operator on the tensor cores
+#include "stencil_kernels.cuh"  // assembled stencils of the Galerkin levels
 
 namespace psfea {
 namespace dev {
 
-// The same list-driven boundary-node pass (FP32 modes) for levels whose Galerkin matrices come in
-// few classes: each CTA (persistent, one per SM) first copies every class matrix into shared
-// memory and gathers the rows from there, and each node's 27 neighbours are read once, two z-planes
-// at a time (81 loads instead of up to 192): the global-load form of this pass is bound by L1
-// wavefronts. The same sums in the same order as k_bnd (bitwise).
-template <int MODE, bool OWN16>
-__global__ void __launch_bounds__(512) k_bnd_cls(LevelView L, Coefs<float> C, const int* __restrict__ list, int count, int nClass,
-                                                  const float* __restrict__ x, float* __restrict__ y, const float* __restrict__ r,
-                                                  float* __restrict__ d, float c1, float c2, int raw, Ctl ctl) {
+// A list-driven FP32 pass (APPLY / CHEB / RESID) over a level's nodes: the boundary nodes of a split
+// level, or every active node of a sparse level (a thin-walled lattice leaves two thirds of a
+// tile's node slots inactive, and the tiles still stage and store them). Each node's 27 neighbours
+// are read once, two z-planes at a time (81 loads instead of up to 192 in the per-voxel gather).
+// CLS: the level's Galerkin matrices come in few classes; each CTA (persistent, one per SM) first
+// copies them all into shared memory and gathers the rows from there. The sums are those of k_bnd
+// in the same order (bitwise the same results); nodes off the list are not written.
+// V = __half: the FP16 coarse-level vectors, iterates (x, d, y of CHEB) stored as x * sx and
+// residuals (r, y of RESID) as r * sr with powers of two sx, sr; rho = sr / sx brings K x to the
+// residual's scale and the caller passes c2 / rho (exact: powers of two). V = float: rho = 1.
+template <int MODE, bool OWN16, bool CLS, class V = float>
+__global__ void __launch_bounds__(512) k_list(LevelView L, Coefs<float> C, const int* __restrict__ list, int count, int nClass,
+                                               const V* __restrict__ x, V* __restrict__ y, const V* __restrict__ r, V* __restrict__ d,
+                                               float c1, float c2, float rho, int raw, Ctl ctl) {
     if (skipped(ctl)) return;
     extern __shared__ __align__(16) unsigned char clsRaw[];
-    const size_t bytes = size_t(nClass) * 576 * (OWN16 ? 2 : 4);
-    const uint4* src = reinterpret_cast<const uint4*>(OWN16 ? static_cast<const void*>(L.own16) : static_cast<const void*>(L.own));
-    uint4* dst = reinterpret_cast<uint4*>(clsRaw);
-    for (size_t e = threadIdx.x; e < bytes / 16; e += blockDim.x) dst[e] = __ldg(src + e);
-    __syncthreads();
     LevelView Ls = L;
-    if (OWN16) Ls.own16 = reinterpret_cast<const __half*>(clsRaw);
-    else Ls.own = reinterpret_cast<const float*>(clsRaw);
+    if constexpr (CLS) {
+        const size_t bytes = size_t(nClass) * 576 * (OWN16 ? 2 : 4);
+        const uint4* src = reinterpret_cast<const uint4*>(OWN16 ? static_cast<const void*>(L.own16) : static_cast<const void*>(L.own));
+        uint4* dst = reinterpret_cast<uint4*>(clsRaw);
+        for (size_t e = threadIdx.x; e < bytes / 16; e += blockDim.x) dst[e] = __ldg(src + e);
+        __syncthreads();
+        if (OWN16) Ls.own16 = reinterpret_cast<const __half*>(clsRaw);
+        else Ls.own = reinterpret_cast<const float*>(clsRaw);
+    }
+    constexpr bool H = !std::is_same<V, float>::value;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count; t += (long long)gridDim.x * blockDim.x) {
         const long long n = list[t];
         const uint8_t mask = __ldg(L.nmask + n);
         int i, j, k;
         nodeCoords(L, n, i, j, k);
         float acc[3];
-        applyNbr<float, OWN16, 1, true>(Ls, C, x, i, j, k, n, mask, acc);
+        applyNbr<float, OWN16, 1, CLS, V>(Ls, C, x, i, j, k, n, mask, acc);
 #pragma unroll
         for (int q = 0; q < 3; q++) {
             const long long id = 3 * n + q;
             const bool fx = fixedDof(mask, q);
+            const float kx = H ? rho * acc[q] : acc[q];
             if (MODE == TOP_APPLY) {
-                y[id] = (!raw && fx) ? 0.f : acc[q];
+                stv(y + id, (!raw && fx) ? 0.f : kx);
             } else if (MODE == TOP_RESID) {
-                y[id] = fx ? 0.f : r[id] - acc[q];
+                stv(y + id, fx ? 0.f : ldf(r + id) - kx);
             } else {
                 if (fx) {
-                    d[id] = 0.f;
-                    y[id] = 0.f;
+                    stv(d + id, 0.f);
+                    stv(y + id, 0.f);
                 } else {
-                    const float dn = c1 * d[id] + c2 * L.invD[id] * (r[id] - acc[q]);
-                    d[id] = dn;
-                    y[id] = x[id] + dn;
+                    const float dn = c1 * ldf(d + id) + c2 * L.invD[id] * (ldf(r + id) - kx);
+                    stv(d + id, dn);
+                    stv(y + id, ldf(x + id) + dn);
                 }
             }
         }
@@ -1402,8 +1449,15 @@ struct DevLevel {
     DevMem ebeTiles;
     int nEbeTiles = 0;
     bool ebe = false;
+    // assembled stencils (levels >= 1): of the boundary nodes of a split tiled level, or of every
+    // active node of an untiled one (stnNodes: those nodes, in order); FP32 and the FP16 copy
+    // over the power-of-two scale stnScale, each made on first use
+    const int* stnNodes = nullptr;
+    int nStn = 0;
+    DevMem stn32, stn16;
+    float stnScale = 1.f;
     void release() {
-        for (DevMem* b : {&word, &nmask, &own, &own16, &invD, &dadd, &dadd32, &bc, &tiles, &blist, &ebeTiles}) b->release();
+        for (DevMem* b : {&word, &nmask, &own, &own16, &invD, &dadd, &dadd32, &bc, &tiles, &blist, &ebeTiles, &stn32, &stn16}) b->release();
     }
 };
 
@@ -1445,6 +1499,15 @@ struct SharedModel {
     // boundary passes gather Galerkin classes from shared memory when they fit in this many bytes
     // (PSFEA_CLS_SMEM; 0 = never)
     size_t clsSmemMax = 200 * 1024;
+    // levels (bit l) whose FP32 passes run over their active-node list instead of tiles or one
+    // thread per pitched node (PSFEA_LIST_LEVELS)
+    int64_t listLevels = 0;
+    // PS_PREC_HALF: per level the power of two delta_l (iterates stored as x * 8^-l * delta_l,
+    // residuals as r * 8^-l) and the inner solve's refinement factor
+    std::vector<float> halfDelta;
+    bool halfOk = false;  // every level >= 1 fits FP16 with its scale
+    double refineEta = 0.1;
+    std::mutex listMu;
     cudaStream_t ms = nullptr;     // allocation / upload stream of the shared data
     cudaEvent_t readyEv = nullptr; // recorded when the uploads are done; contexts wait on it
 
@@ -1476,6 +1539,11 @@ struct SharedModel {
     void adopt(Hierarchy&& h);  // upload a hierarchy built on the host beforehand
     void uploadLevel(int l);
     void ensureActiveLists();
+    // the assembled stencils of the levels in stencilLevels (FP16 copies too when half); the
+    // callers' streams wait on readyEv
+    void ensureStencils(bool half);
+    int64_t stencilLevels = ~int64_t(1);  // PSFEA_STENCIL_LEVELS: bit l = level l (never level 0)
+    int64_t stencilMinNodes = 65536;      // PSFEA_STENCIL_MIN_NODES: smaller node lists keep the gather
     bool exactOneLevel() const { return L.size() == 1 && H.hasFactor(); }
 };
 
@@ -1493,6 +1561,10 @@ void SharedModel::adopt(Hierarchy&& h) {
     if (const char* e = std::getenv("PSFEA_OWN_DEDUP")) ownDedup = std::atoi(e) != 0;
     if (const char* e = std::getenv("PSFEA_EBE")) ebeLevels = std::atoll(e);
     if (const char* e = std::getenv("PSFEA_CLS_SMEM")) clsSmemMax = size_t(std::atoll(e));
+    if (const char* e = std::getenv("PSFEA_LIST_LEVELS")) listLevels = std::atoll(e);
+    if (const char* e = std::getenv("PSFEA_REFINE_ETA")) refineEta = std::atof(e);
+    if (const char* e = std::getenv("PSFEA_STENCIL_LEVELS")) stencilLevels = std::atoll(e) & ~int64_t(1);
+    if (const char* e = std::getenv("PSFEA_STENCIL_MIN_NODES")) stencilMinNodes = std::atoll(e);
     if (const char* e = std::getenv("PSFEA_EBE_SPLIT")) ebeSplit = std::atoi(e) == 1 ? 1 : 3;
     check(cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking), "stream");
     check(cudaEventCreateWithFlags(&readyEv, cudaEventDisableTiming), "event");
@@ -1525,12 +1597,16 @@ void SharedModel::adopt(Hierarchy&& h) {
         set(dev::k_ebe<dev::TOP_APPLY, 3>, dev::ebeSmemBytes<3>());
         set(dev::k_ebe<dev::TOP_CHEB, 3>, dev::ebeSmemBytes<3>());
         set(dev::k_ebe<dev::TOP_RESID, 3>, dev::ebeSmemBytes<3>());
-        set(dev::k_bnd_cls<dev::TOP_CHEB, true>, 200 * 1024);
-        set(dev::k_bnd_cls<dev::TOP_CHEB, false>, 200 * 1024);
-        set(dev::k_bnd_cls<dev::TOP_RESID, true>, 200 * 1024);
-        set(dev::k_bnd_cls<dev::TOP_RESID, false>, 200 * 1024);
-        set(dev::k_bnd_cls<dev::TOP_APPLY, true>, 200 * 1024);
-        set(dev::k_bnd_cls<dev::TOP_APPLY, false>, 200 * 1024);
+        set(dev::k_list<dev::TOP_CHEB, true, true>, 200 * 1024);
+        set(dev::k_list<dev::TOP_CHEB, false, true>, 200 * 1024);
+        set(dev::k_list<dev::TOP_RESID, true, true>, 200 * 1024);
+        set(dev::k_list<dev::TOP_RESID, false, true>, 200 * 1024);
+        set(dev::k_list<dev::TOP_APPLY, true, true>, 200 * 1024);
+        set(dev::k_list<dev::TOP_APPLY, false, true>, 200 * 1024);
+        set(dev::k_list<dev::TOP_CHEB, true, true, __half>, 200 * 1024);
+        set(dev::k_list<dev::TOP_CHEB, false, true, __half>, 200 * 1024);
+        set(dev::k_list<dev::TOP_RESID, true, true, __half>, 200 * 1024);
+        set(dev::k_list<dev::TOP_RESID, false, true, __half>, 200 * 1024);
         set(dev::kb_tc<dev::BOP_APPLY>, dev::btSmemBytes());
         set(dev::kb_tc<dev::BOP_CHEB>, dev::btSmemBytes());
         set(dev::kb_tc<dev::BOP_RESID>, dev::btSmemBytes());
@@ -1551,6 +1627,31 @@ void SharedModel::adopt(Hierarchy&& h) {
         upload(cInv, H.coarseInv, bytes, ms);
     }
     for (auto& D : L) maxTiles = std::max(maxTiles, D.nTiles);
+    // delta_l = 2^(round(log2(median diagonal of level l)) - 4): the FP16 iterates then sit near
+    // 1/16 of the residuals' order one, leaving room for the coarse corrections' growth
+    // (one scale per level cannot hold graded stiffness in FP16: when a level's diagonal spans more
+    // than 2^8, e.g. SIMP densities down to 1e-3 with p = 3, the form keeps FP32 coarse vectors)
+    halfDelta.assign(L.size(), 1.f);
+    halfOk = L.size() > 1;
+    for (size_t l = 1; l < L.size(); l++) {
+        const auto& inv = H.levels[l].invDiag;
+        double lo = 0, hi = 0;
+        std::vector<double> dg;
+        const size_t stride = std::max<size_t>(1, inv.size() / 65536);
+        for (size_t q = 0; q < inv.size(); q++)
+            if (inv[q] > 0) {
+                const double v = 1.0 / inv[q];
+                lo = lo > 0 ? std::min(lo, v) : v;
+                hi = std::max(hi, v);
+                if (q % stride == 0) dg.push_back(v);
+            }
+        if (dg.empty()) continue;
+        if (hi > 256.0 * lo) halfOk = false;
+        std::nth_element(dg.begin(), dg.begin() + dg.size() / 2, dg.end());
+        const int e = int(std::lround(std::log2(dg[dg.size() / 2]))) - 4;
+        halfDelta[l] = std::ldexp(1.f, std::max(-120, std::min(120, e)));
+    }
+    if (listLevels) ensureActiveLists();
     check(cudaEventRecord(readyEv, ms), "event");
 }
 
@@ -1704,7 +1805,63 @@ void SharedModel::uploadLevel(int l) {
         }
 }
 
+void SharedModel::ensureStencils(bool half) {
+    if (!stencilLevels) return;
+    ensureActiveLists();
+    std::lock_guard<std::mutex> g(listMu);
+    bool need = false;
+    for (size_t l = 1; l < L.size() && l < 63; l++) {
+        const DevLevel& D = L[l];
+        const int cnt = D.useTiles ? (D.split32 ? D.nBnd : 0) : nAct[l];
+        const bool on = ((stencilLevels >> l) & 1) && cnt > 0 && cnt >= stencilMinNodes;
+        if (on && (!D.stn32.p || (half && !D.stn16.p))) need = true;
+    }
+    if (!need) return;
+    unsigned* mx = nullptr;
+    unsigned* mxHost = nullptr;
+    for (size_t l = 1; l < L.size() && l < 63; l++) {
+        DevLevel& D = L[l];
+        const int cnt = D.useTiles ? (D.split32 ? D.nBnd : 0) : nAct[l];
+        if (!((stencilLevels >> l) & 1) || cnt <= 0 || cnt < stencilMinNodes) continue;
+        if (!D.stn32.p) {
+            D.stnNodes = D.useTiles ? D.blist.as<int>() : act[l].as<int>();
+            D.nStn = D.useTiles ? D.nBnd : nAct[l];
+            if (!D.nStn) continue;
+            D.stn32.alloc(size_t(D.nStn) * dev::stnChunks<4>() * 4 * sizeof(float), bytes, ms);
+            dev::k_stn_build<<<gridFor(int64_t(D.nStn) * 27, 256, smCount * 32), 256, 0, ms>>>(D.view, D.c32, D.stnNodes, D.nStn,
+                                                                                             D.stn32.as<float>());
+            check(cudaGetLastError(), "stencil build");
+        }
+        if (half && !D.stn16.p && D.nStn) {
+            if (!mx) {
+                check(cudaMalloc(&mx, sizeof(unsigned)), "cudaMalloc");
+                check(cudaMallocHost(&mxHost, sizeof(unsigned)), "cudaMallocHost");
+            }
+            const int64_t ne = int64_t(D.nStn) * dev::stnChunks<4>() * 4;
+            check(cudaMemsetAsync(mx, 0, sizeof(unsigned), ms), "memset");
+            dev::k_stn_max<<<gridFor(ne, 256, smCount * 8), 256, 0, ms>>>(ne, D.stn32.as<float>(), mx);
+            check(cudaMemcpyAsync(mxHost, mx, sizeof(unsigned), cudaMemcpyDeviceToHost, ms), "copy");
+            check(cudaStreamSynchronize(ms), "stencil scale");
+            float kmax;
+            std::memcpy(&kmax, mxHost, sizeof kmax);
+            // the largest coefficient near 2^14, as for the FP16 element matrices
+            D.stnScale = kmax > 0 ? float(std::exp2(std::ceil(std::log2(double(kmax) / 16384.0)))) : 1.f;
+            D.stn16.alloc(size_t(D.nStn) * dev::stnChunks<8>() * 8 * sizeof(__half), bytes, ms);
+            dev::k_stn_half<<<gridFor(int64_t(D.nStn) * 243, 256, smCount * 8), 256, 0, ms>>>(D.nStn, D.stn32.as<float>(), 1.f / D.stnScale,
+                                                                                              D.stn16.as<__half>());
+            check(cudaGetLastError(), "stencil halves");
+        }
+    }
+    if (mx) {
+        check(cudaStreamSynchronize(ms), "stencils");
+        cudaFree(mx);
+        cudaFreeHost(mxHost);
+    }
+    check(cudaEventRecord(readyEv, ms), "event");
+}
+
 void SharedModel::ensureActiveLists() {
+    std::lock_guard<std::mutex> g(listMu);
     if (!act.empty()) return;
     act.reserve(L.size());
     nAct.resize(L.size());
@@ -1769,9 +1926,9 @@ struct SolverImpl {
     int64_t launches = 0;     // kernels launched by this context (graph replays add their kernel count)
     // graphs of one iteration, per precision, and the coefficient version they were recorded with
     // (by ps_precision: FP64 Krylov with the FP32 or the FP16-matrix V-cycle, FP32 Krylov)
-    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
-    int64_t graphKernels[3] = {0, 0, 0};
-    int64_t graphVersion[3] = {-1, -1, -1};
+    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+    int64_t graphKernels[4] = {0, 0, 0, 0};
+    int64_t graphVersion[4] = {-1, -1, -1, -1};
 
     // smoother estimation in flight: its scratch (stream-ordered, freed as soon as the kernels
     // have run) and the Lanczos scalars of every level, copied to pinned host memory
@@ -1780,7 +1937,7 @@ struct SolverImpl {
 
     // the solve in progress (a resumable state machine, so one host thread can drive many)
     struct Pending {
-        bool active = false, finishing = false, mixed = false, lanczos = false;
+        bool active = false, finishing = false, mixed = false, lanczos = false, half = false;
         int graph = 0;  // the iteration graph in use
         const double* fDev = nullptr;
         const double* x0Dev = nullptr;
@@ -1860,10 +2017,19 @@ struct SolverImpl {
     // V-cycle on level l from W[l].r; returns the buffer holding the result
     // firstDone: W[l].d and W[l].z already hold the first smoothing step (fused upstream)
     float* vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone = false);
+    // PS_PREC_HALF: level l >= 1 over its active-node list on FP16 vectors; the V-cycle with FP16
+    // vectors below the finest level (vcycleHalf: level 0, FP32; vcycle16: levels >= 1)
+    template <int MODE>
+    void op16(int l, const __half* x, __half* y, float c1, float c2, dev::Ctl ctl, bool own16);
+    float* vcycleHalf(dev::Ctl ctl, bool own16, bool firstDone);
+    __half* vcycle16(int l, dev::Ctl ctl, bool own16, bool firstDone);
+    float* vcycleFor(bool half, dev::Ctl ctl, bool own16, bool firstDone = false) {
+        return half ? vcycleHalf(ctl, own16, firstDone) : vcycle(0, ctl, own16, firstDone);
+    }
     bool exactOneLevel() const { return M->exactOneLevel(); }
 
     void recordPlainIteration(dev::Ctl ctl, bool own16);
-    void recordMixedIteration(dev::Ctl ctl);
+    void recordMixedIteration(dev::Ctl ctl, bool refine, bool half);
     // enqueue a solve (f, x0, u in device memory; uHost, if set, receives u as well)
     void startSolve(const double* fDev, const double* x0Dev, const ps_solve_opts& o, double* uDev, double* uHost);
     // move the solve on; returns true (and fills res) once it has finished. block: wait for the
@@ -1982,6 +2148,39 @@ void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev
         return;
     }
     const bool o16 = own16 && D.hasOwn, diff = o16 && M->ownDiff;
+    constexpr int SM_ = MODE == dev::OP_CHEB ? dev::TOP_CHEB : (MODE == dev::OP_RESID ? dev::TOP_RESID : dev::TOP_APPLY);
+    // the assembled stencils of the listed nodes (FP16 in the reduced-precision forms)
+    auto stencilPass = [&]() {
+        const int g = gridFor(D.nStn, 256, smCount * 16);
+        if (o16)
+            launch(dev::k_stn<SM_, __half, float>, g, 256, 0, stream, D.view, D.stnNodes, D.nStn, D.stn16.as<__half>(), D.stnScale, xin, y, rr, dd,
+                   c1, c2, 1.f, 0, ctl);
+        else
+            launch(dev::k_stn<SM_, float, float>, g, 256, 0, stream, D.view, D.stnNodes, D.nStn, D.stn32.as<float>(), 1.f, xin, y, rr, dd, c1, c2,
+                   1.f, 0, ctl);
+    };
+    const bool stn = l > 0 && !diff && D.nStn > 0 && (o16 ? D.stn16.p != nullptr : D.stn32.p != nullptr);
+    if (stn && !D.useTiles) {
+        stencilPass();
+        return;
+    }
+    if (l < 63 && ((M->listLevels >> l) & 1) && !diff && !M->act.empty()) {
+        // the whole level over its active-node list
+        constexpr int LM = MODE == dev::OP_CHEB ? dev::TOP_CHEB : (MODE == dev::OP_RESID ? dev::TOP_RESID : dev::TOP_APPLY);
+        const int* al = M->act[size_t(l)].as<int>();
+        const int na = M->nAct[size_t(l)];
+        const size_t cls = D.hasOwn ? size_t(D.nOwnDev) * 576 * (o16 ? 2 : 4) : 0;
+        if (D.hasOwn && cls <= M->clsSmemMax) {
+            const int gc = std::min(smCount, (na + 511) / 512);
+            if (o16) launch(dev::k_list<LM, true, true>, gc, 512, cls, stream, D.view, static_cast<const dev::Coefs<float>&>(D.c32), al, na, D.nOwnDev, xin, y, rr, dd, c1, c2, 1.f, 0, ctl);
+            else launch(dev::k_list<LM, false, true>, gc, 512, cls, stream, D.view, static_cast<const dev::Coefs<float>&>(D.c32), al, na, D.nOwnDev, xin, y, rr, dd, c1, c2, 1.f, 0, ctl);
+        } else {
+            const int gl = gridFor(na, 512, smCount * 2);
+            if (o16) launch(dev::k_list<LM, true, false>, gl, 512, 0, stream, D.view, static_cast<const dev::Coefs<float>&>(D.c32), al, na, 0, xin, y, rr, dd, c1, c2, 1.f, 0, ctl);
+            else launch(dev::k_list<LM, false, false>, gl, 512, 0, stream, D.view, static_cast<const dev::Coefs<float>&>(D.c32), al, na, 0, xin, y, rr, dd, c1, c2, 1.f, 0, ctl);
+        }
+        return;
+    }
     if (D.use8) {
         const int g = gridFor(D.view.nNodes * 8, 256, smCount * 32);
         if (diff) launch(dev::k_op8<float, MODE, true, true>, g, 256, 0, stream, D.view, D.c32, xin, y, rr, dd, c1, c2, 0, ctl);
@@ -2015,14 +2214,18 @@ void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev
         else if (o16) launch(dev::k_tile<float, TM, true, false, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
         else launch(dev::k_tile<float, TM, false, false, false>, D.nTiles, dev::TILE_THREADS, sm, stream, D.view, D.c32, tl, mp, io, st(), part(), tick(), ctl);
         if (!D.nBnd) return;
+        if (stn) {
+            stencilPass();
+            return;
+        }
         const int* bl = D.blist.as<int>();
         if (!diff && D.hasOwn) {
             // few Galerkin classes: the boundary pass gathers from a shared-memory copy of them
             const size_t cls = size_t(D.nOwnDev) * 576 * (o16 ? 2 : 4);
             if (cls <= M->clsSmemMax) {
                 const int gc = std::min(smCount, (D.nBnd + 511) / 512);
-                if (o16) launch(dev::k_bnd_cls<TM, true>, gc, 512, cls, stream, D.view, c, bl, D.nBnd, D.nOwnDev, xin, y, rr, dd, c1, c2, 0, ctl);
-                else launch(dev::k_bnd_cls<TM, false>, gc, 512, cls, stream, D.view, c, bl, D.nBnd, D.nOwnDev, xin, y, rr, dd, c1, c2, 0, ctl);
+                if (o16) launch(dev::k_list<TM, true, true>, gc, 512, cls, stream, D.view, c, bl, D.nBnd, D.nOwnDev, xin, y, rr, dd, c1, c2, 1.f, 0, ctl);
+                else launch(dev::k_list<TM, false, true>, gc, 512, cls, stream, D.view, c, bl, D.nBnd, D.nOwnDev, xin, y, rr, dd, c1, c2, 1.f, 0, ctl);
                 return;
             }
         }
@@ -2050,12 +2253,12 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
         if (H.hasFactor()) {
             const int threads = 256, warps = threads / 32;
             const int grid = std::max(1, std::min(smCount * 2, (m + warps - 1) / warps));
-            launch(dev::k_coarse<float, float>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(), r, z, ctl);
+            launch(dev::k_coarse<float, float>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(), r, z, 1.0, ctl);
             return z;
         }
         // no factor: 40 damped Jacobi sweeps with the default weight (voxel_fea.cpp:676-678)
         if (!firstDone)
-            launch(dev::k_cheb_first, vecGrid(pd(l)), dev::VEC_THREADS, 0, stream, pd(l), r, D.invD.as<float>(), d, z, D.omega, ctl);
+            launch(dev::k_cheb_first<float>, vecGrid(pd(l)), dev::VEC_THREADS, 0, stream, pd(l), r, D.invD.as<float>(), d, z, D.omega, ctl);
         float* a = z;
         float* b = t;
         for (int s = 1; s < 40; s++) {
@@ -2068,7 +2271,7 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
     LevelWork& Wc = W[size_t(l + 1)];
     const HostLevel& hc = H.levels[size_t(l + 1)];
     if (!firstDone)
-        launch(dev::k_cheb_first, vecGrid(pd(l)), dev::VEC_THREADS, 0, stream, pd(l), r, D.invD.as<float>(), d, z, D.cf0, ctl);
+        launch(dev::k_cheb_first<float>, vecGrid(pd(l)), dev::VEC_THREADS, 0, stream, pd(l), r, D.invD.as<float>(), d, z, D.cf0, ctl);
     float* a = z;  // the current iterate
     float* b = t;
     for (size_t k = 0; k < D.chebC1.size(); k++) {  // pre-smoothing from zero
@@ -2079,14 +2282,130 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
     // restriction, with the coarse level's first smoothing step fused in (unless it is the dense solve)
     const bool fuse = !(l + 1 == last && H.hasFactor());
     const float c0c = (l + 1 == last) ? C.omega : C.cf0;
-    launch(dev::k_restrict, gridFor(pn(l + 1), 256, smCount * 16), 256, 0, stream, D.view, C.view, b, Wc.r.as<float>(),
-           fuse ? Wc.d.as<float>() : nullptr, fuse ? Wc.z.as<float>() : nullptr, c0c, ctl);
+    launch(dev::k_restrict<float, float>, gridFor(pn(l + 1), 256, smCount * 16), 256, 0, stream, D.view, C.view, b, Wc.r.as<float>(),
+           fuse ? Wc.d.as<float>() : nullptr, fuse ? Wc.z.as<float>() : nullptr, c0c, 1.f, ctl);
     float* zc = vcycle(l + 1, ctl, own16, fuse);
-    launch(dev::k_prolong, gridFor(pn(l), 256, smCount * 16), 256, 0, stream, D.view, C.view.PX, hc.NY, zc, a, ctl);
+    launch(dev::k_prolong<float, float>, gridFor(pn(l), 256, smCount * 16), 256, 0, stream, D.view, C.view.PX, hc.NY, zc, a, 1.f, ctl);
     op32<dev::OP_CHEB>(l, a, b, 0.f, D.cf0, ctl, own16);  // post-smoothing: d = c0 D^-1 (r - K a); b = a + d
     std::swap(a, b);
     for (size_t k = 0; k < D.chebC1.size(); k++) {
         op32<dev::OP_CHEB>(l, a, b, D.chebC1[k], D.chebC2[k], ctl, own16);
+        std::swap(a, b);
+    }
+    return a;
+}
+
+template <int MODE>
+void SolverImpl::op16(int l, const __half* xin, __half* y, float c1, float c2, dev::Ctl ctl, bool own16) {
+    DevLevel& D = L[size_t(l)];
+    const int na = M->nAct[size_t(l)];
+    if (!na) return;
+    constexpr int LM = MODE == dev::OP_CHEB ? dev::TOP_CHEB : (MODE == dev::OP_RESID ? dev::TOP_RESID : dev::TOP_APPLY);
+    const float delta = M->halfDelta[size_t(l)], rho = 1.f / delta;
+    const __half* rr = W[size_t(l)].r.as<__half>();
+    __half* dd = W[size_t(l)].d.as<__half>();
+    const int* al = M->act[size_t(l)].as<int>();
+    const bool o16 = own16 && D.hasOwn;
+    const dev::Coefs<float>& c = D.c32;
+    const size_t cls = D.hasOwn ? size_t(D.nOwnDev) * 576 * (o16 ? 2 : 4) : 0;
+    if (D.hasOwn && cls <= M->clsSmemMax) {
+        const int gc = std::min(smCount, (na + 511) / 512);
+        if (o16) launch(dev::k_list<LM, true, true, __half>, gc, 512, cls, stream, D.view, c, al, na, D.nOwnDev, xin, y, rr, dd, c1, c2 * delta, rho, 0, ctl);
+        else launch(dev::k_list<LM, false, true, __half>, gc, 512, cls, stream, D.view, c, al, na, D.nOwnDev, xin, y, rr, dd, c1, c2 * delta, rho, 0, ctl);
+    } else {
+        const int g = gridFor(na, 512, smCount * 2);
+        if (o16) launch(dev::k_list<LM, true, false, __half>, g, 512, 0, stream, D.view, c, al, na, 0, xin, y, rr, dd, c1, c2 * delta, rho, 0, ctl);
+        else launch(dev::k_list<LM, false, false, __half>, g, 512, 0, stream, D.view, c, al, na, 0, xin, y, rr, dd, c1, c2 * delta, rho, 0, ctl);
+    }
+}
+
+// The finest level of the FP16 V-cycle: vcycle's level 0 (FP32 vectors), restricting into and
+// prolongating from level 1's FP16 vectors (residual scale 1/8 there; iterate scale delta_1 / 8)
+float* SolverImpl::vcycleHalf(dev::Ctl ctl, bool own16, bool firstDone) {
+    DevLevel& D = L[0];
+    LevelWork& W0 = W[0];
+    float *z = W0.z.as<float>(), *t = W0.t.as<float>(), *r = W0.r.as<float>(), *d = W0.d.as<float>();
+    DevLevel& C = L[1];
+    LevelWork& Wc = W[1];
+    const HostLevel& hc = H.levels[1];
+    const int last = int(L.size()) - 1;
+    const float dc = M->halfDelta[1];
+    if (!firstDone)
+        launch(dev::k_cheb_first<float>, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), r, D.invD.as<float>(), d, z, D.cf0, ctl);
+    float* a = z;
+    float* b = t;
+    for (size_t k = 0; k < D.chebC1.size(); k++) {
+        op32<dev::OP_CHEB>(0, a, b, D.chebC1[k], D.chebC2[k], ctl, own16);
+        std::swap(a, b);
+    }
+    op32<dev::OP_RESID>(0, a, b, 0.f, 0.f, ctl, own16);
+    const bool fuse = !(1 == last && H.hasFactor());
+    const float c0c = (1 == last) ? C.omega : C.cf0;
+    launch(dev::k_restrict<float, __half>, gridFor(pn(1), 256, smCount * 16), 256, 0, stream, D.view, C.view, b, Wc.r.as<__half>(),
+           fuse ? Wc.d.as<__half>() : nullptr, fuse ? Wc.z.as<__half>() : nullptr, c0c * dc, 0.125f, ctl);
+    const __half* zc = vcycle16(1, ctl, own16, fuse);
+    launch(dev::k_prolong<__half, float>, gridFor(pn(0), 256, smCount * 16), 256, 0, stream, D.view, C.view.PX, hc.NY, zc, a, 8.f / dc, ctl);
+    op32<dev::OP_CHEB>(0, a, b, 0.f, D.cf0, ctl, own16);
+    std::swap(a, b);
+    for (size_t k = 0; k < D.chebC1.size(); k++) {
+        op32<dev::OP_CHEB>(0, a, b, D.chebC1[k], D.chebC2[k], ctl, own16);
+        std::swap(a, b);
+    }
+    return a;
+}
+
+// vcycle on level l >= 1 with FP16 vectors (residuals r * 8^-l, iterates x * 8^-l * delta_l)
+__half* SolverImpl::vcycle16(int l, dev::Ctl ctl, bool own16, bool firstDone) {
+    DevLevel& D = L[size_t(l)];
+    LevelWork& Wl = W[size_t(l)];
+    __half *z = Wl.z.as<__half>(), *t = Wl.t.as<__half>(), *r = Wl.r.as<__half>(), *d = Wl.d.as<__half>();
+    const float dl = M->halfDelta[size_t(l)];
+    const int last = int(L.size()) - 1;
+    if (l == last) {
+        if (H.hasFactor()) {
+            const int threads = 256, warps = threads / 32;
+            const int grid = std::max(1, std::min(smCount * 2, (m + warps - 1) / warps));
+            // held DOFs are not written by the solve and must read 0 (the buffer is shared with
+            // the FP32 forms' vectors, laid out differently)
+            check(cudaMemsetAsync(z, 0, size_t(pd(l)) * sizeof(__half), stream), "memset");
+            launch(dev::k_coarse<__half, __half>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(), r, z,
+                   double(dl), ctl);
+            return z;
+        }
+        if (!firstDone)
+            launch(dev::k_cheb_first<__half>, vecGrid(pd(l)), dev::VEC_THREADS, 0, stream, pd(l), r, D.invD.as<float>(), d, z, D.omega * dl, ctl);
+        __half* a = z;
+        __half* b = t;
+        for (int s = 1; s < 40; s++) {
+            op16<dev::OP_CHEB>(l, a, b, 0.f, D.omega, ctl, own16);
+            std::swap(a, b);
+        }
+        return a;
+    }
+    DevLevel& C = L[size_t(l + 1)];
+    LevelWork& Wc = W[size_t(l + 1)];
+    const HostLevel& hc = H.levels[size_t(l + 1)];
+    const float dc = M->halfDelta[size_t(l + 1)];
+    if (!firstDone)
+        launch(dev::k_cheb_first<__half>, vecGrid(pd(l)), dev::VEC_THREADS, 0, stream, pd(l), r, D.invD.as<float>(), d, z, D.cf0 * dl, ctl);
+    __half* a = z;
+    __half* b = t;
+    for (size_t k = 0; k < D.chebC1.size(); k++) {
+        op16<dev::OP_CHEB>(l, a, b, D.chebC1[k], D.chebC2[k], ctl, own16);
+        std::swap(a, b);
+    }
+    op16<dev::OP_RESID>(l, a, b, 0.f, 0.f, ctl, own16);
+    const bool fuse = !(l + 1 == last && H.hasFactor());
+    const float c0c = (l + 1 == last) ? C.omega : C.cf0;
+    launch(dev::k_restrict<__half, __half>, gridFor(pn(l + 1), 256, smCount * 16), 256, 0, stream, D.view, C.view, b, Wc.r.as<__half>(),
+           fuse ? Wc.d.as<__half>() : nullptr, fuse ? Wc.z.as<__half>() : nullptr, c0c * dc, 0.125f, ctl);
+    const __half* zc = vcycle16(l + 1, ctl, own16, fuse);
+    launch(dev::k_prolong<__half, __half>, gridFor(pn(l), 256, smCount * 16), 256, 0, stream, D.view, C.view.PX, hc.NY, zc, a, 8.f * dl / dc,
+           ctl);
+    op16<dev::OP_CHEB>(l, a, b, 0.f, D.cf0, ctl, own16);
+    std::swap(a, b);
+    for (size_t k = 0; k < D.chebC1.size(); k++) {
+        op16<dev::OP_CHEB>(l, a, b, D.chebC1[k], D.chebC2[k], ctl, own16);
         std::swap(a, b);
     }
     return a;
@@ -2226,7 +2545,7 @@ void SolverImpl::recordPlainIteration(dev::Ctl ctl, bool own16) {
         const int threads = 256, warps = threads / 32;
         const int grid = std::max(1, std::min(smCount * 2, (m + warps - 1) / warps));
         launch(dev::k_coarse<double, double>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(), r.as<double>(),
-               z64.as<double>(), ctl);
+               z64.as<double>(), 1.0, ctl);
     } else {
         z32 = vcycle(0, ctl, own16, true);  // r32 and the first smoothing step came with the update
     }
@@ -2236,7 +2555,7 @@ void SolverImpl::recordPlainIteration(dev::Ctl ctl, bool own16) {
 }
 
 // one FP32 CG iteration with the FP64 fold (runs only when due)
-void SolverImpl::recordMixedIteration(dev::Ctl ctl) {
+void SolverImpl::recordMixedIteration(dev::Ctl ctl, bool refine, bool half) {
     const HostLevel& h = H.levels[0];
     DevLevel& D = L[0];
     LevelWork& W0 = W[0];
@@ -2261,7 +2580,10 @@ void SolverImpl::recordMixedIteration(dev::Ctl ctl) {
     op64(0, x.as<double>(), q.as<double>(), false, foldCtl);
     launch(dev::k_mx_fold2, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, f.as<double>(), q.as<double>(),
            W0.r.as<float>(), st(), part(), tick(), foldCtl);
-    float* z32 = vcycle(0, ctl, M->mixedOwn16);
+    if (refine)
+        launch(dev::k_mx_rescale, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), W0.r.as<float>(), st(),
+               dev::Ctl{ctl.skipIf, &st()->restart});
+    float* z32 = vcycleFor(half, ctl, M->mixedOwn16);
     launch(dev::k_mx_dots, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), W0.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
     launch(dev::k_mx_p, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), z32, p32.as<float>(), st(), ctl);
 }
@@ -2296,9 +2618,23 @@ void SolverImpl::startIterations() {
     DevLevel& D = L[0];
     LevelWork& W0 = W[0];
     // FP32 Krylov (PS_PREC_FP32); the FP64 Krylov forms differ only in the V-cycle's matrices
-    const bool mixed = o.precision == PS_PREC_FP32 && !exactOneLevel();
+    const bool refine = o.precision == PS_PREC_HALF && !exactOneLevel();
+    const bool half = refine && M->halfOk;
+    const bool mixed = (o.precision == PS_PREC_FP32 || refine) && !exactOneLevel();
     const bool own16 = o.precision == PS_PREC_MIXED && M->mixedOwn16;
     pend.mixed = mixed;
+    pend.half = half;
+    if (!exactOneLevel()) {
+        M->ensureStencils(own16 || (mixed && M->mixedOwn16));
+        check(cudaStreamWaitEvent(stream, M->readyEv, 0), "wait");
+    }
+    if (half) {
+        M->ensureActiveLists();
+        check(cudaStreamWaitEvent(stream, M->readyEv, 0), "wait");
+        // the list kernels write active nodes only: the FP16 views of the levels' second iterate
+        // buffers (also the FP32 forms' storage) start from zeros, so that their inactive nodes read 0
+        for (size_t l = 1; l < W.size(); l++) check(cudaMemsetAsync(W[l].t.p, 0, size_t(pd(int(l))) * sizeof(__half), stream), "memset");
+    }
     const int64_t n = pd(0);
     // state
     dev::SolveState s{};
@@ -2306,7 +2642,9 @@ void SolverImpl::startIterations() {
     s.maxIter = o.max_iter;
     s.first = 1;
     s.mixed = mixed ? 1 : 0;
-    s.foldFactor = M->foldFactor;
+    s.foldFactor = refine ? M->refineEta : M->foldFactor;
+    s.refine = refine ? 1 : 0;
+    s.rescale = 1.0;
     *hostState = s;
     check(cudaMemcpyAsync(state.p, hostState, sizeof s, cudaMemcpyHostToDevice, stream), "state");
     if (fDev != f.p) pitch(fDev, f.as<double>(), 0, true);  // a caller's device vector (dense layout)
@@ -2324,7 +2662,7 @@ void SolverImpl::startIterations() {
         check(cudaMemsetAsync(x32.p, 0, size_t(n) * 4, stream), "memset");
         launch(dev::k_vc_load, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, r.as<double>(), W0.r.as<float>(),
                D.invD.as<float>(), W0.d.as<float>(), W0.z.as<float>(), D.cf0, st(), ctl);
-        float* z32 = vcycle(0, ctl, M->mixedOwn16, true);
+        float* z32 = vcycleFor(half, ctl, M->mixedOwn16, true);
         launch(dev::k_mx_dots, vecGrid(n), dev::VEC_THREADS, 0, stream, n, W0.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
         launch(dev::k_mx_p, vecGrid(n), dev::VEC_THREADS, 0, stream, n, z32, p32.as<float>(), st(), ctl);
     } else {
@@ -2334,7 +2672,7 @@ void SolverImpl::startIterations() {
             const int grid = std::max(1, std::min(smCount * 2, (m + warps - 1) / warps));
             check(cudaMemsetAsync(z64.p, 0, size_t(n) * 8, stream), "memset");
             launch(dev::k_coarse<double, double>, grid, threads, size_t(m) * sizeof(double), stream, m, cDof.as<int>(), cInv.as<double>(),
-                   r.as<double>(), z64.as<double>(), ctl);
+                   r.as<double>(), z64.as<double>(), 1.0, ctl);
         } else {
             launch(dev::k_vc_load, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, r.as<double>(), W0.r.as<float>(),
                    D.invD.as<float>(), W0.d.as<float>(), W0.z.as<float>(), D.cf0, st(), ctl);
@@ -2348,7 +2686,7 @@ void SolverImpl::startIterations() {
     launch(dev::k_clear_first, 1, 1, 0, stream, st());
     check(cudaGetLastError(), "solve setup");
     // the iteration graph (recorded once per precision and smoother version)
-    const int gi = mixed ? 2 : (own16 ? 1 : 0);
+    const int gi = refine ? 3 : (mixed ? 2 : (own16 ? 1 : 0));
     pend.graph = gi;
     if (graph[gi] && graphVersion[gi] != M->version) {
         cudaGraphExecDestroy(graph[gi]);
@@ -2357,7 +2695,7 @@ void SolverImpl::startIterations() {
     if (!graph[gi]) {
         cudaGraph_t gr;
         check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
-        if (mixed) recordMixedIteration(ctl);
+        if (mixed) recordMixedIteration(ctl, refine, half);
         else recordPlainIteration(ctl, own16);
         check(cudaStreamEndCapture(stream, &gr), "capture end");
         size_t nodes = 0;
@@ -3115,7 +3453,7 @@ void Solver::precondition(const double* rHost, double* zHost) {
         const int grid = std::max(1, std::min(I.smCount * 2, (I.m + warps - 1) / warps));
         check(cudaMemsetAsync(I.z64.p, 0, size_t(n) * 8, I.stream), "memset");
         I.launch(dev::k_coarse<double, double>, grid, threads, size_t(I.m) * sizeof(double), I.stream, I.m, I.cDof.as<int>(), I.cInv.as<double>(),
-                 I.r.as<double>(), I.z64.as<double>(), none);
+                 I.r.as<double>(), I.z64.as<double>(), 1.0, none);
         I.downloadPitched(I.z64.as<double>(), zHost, 0, I.q.as<double>());
     } else {
         I.launch(dev::k_rmax, I.vecGrid(nn), dev::VEC_THREADS, 0, I.stream, nn, D.view.nmask, I.r.as<double>(), I.st(), I.part(), I.tick());

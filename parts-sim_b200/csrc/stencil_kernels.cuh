@@ -1,0 +1,168 @@
+// Assembled stencils of the Galerkin levels. Included by solver.cu only.
+//
+// Below the finest level the operator's element matrices are Galerkin products (an own matrix per
+// voxel, shared by classes on lattices), and a node that is not uniform takes the per-voxel gather:
+// the rows of its corner in each of its up to 8 voxels, 576 multiply-adds against 24 corner values
+// each, through the class matrices (voxel_fea.cpp:451-486 computes the same sums). Here each such
+// node instead keeps its assembled row: the 27 3x3 blocks coupling it to its neighbours, summed once
+// at setup over the voxels the two nodes share. A pass then streams 243 coefficients per node
+// (coalesced: 16-byte chunks, chunk-major over the node list) and does 243 multiply-adds; the
+// gather of the 27 neighbours' values is unchanged. The sums run in another order than the per-voxel gather
+// (FP32 rounding differs; the stored blocks are the exact sums of the same FP32 matrices).
+#pragma once
+
+#include "kernels.cuh"
+
+#include <type_traits>
+
+namespace psfea {
+namespace dev {
+
+// Layout: coefficient c = 9 m + 3 p + q (m the neighbour (ox + 1) + 3 (oy + 1) + 9 (oz + 1), p the
+// row and q the column component) of listed node t sits in chunk c / CW of CW consecutive values
+// (16 bytes: CW = 4 floats or 8 halves), chunks stored chunk-major over the nodes, so that a warp
+// reads one chunk of 32 consecutive nodes as 512 contiguous bytes. The tail of the last chunk is 0.
+template <int CW>
+__host__ __device__ constexpr int stnChunks() { return (243 + CW - 1) / CW; }
+template <int CW>
+__host__ __device__ __forceinline__ long long stnAt(int c, long long t, long long count) { return ((c / CW) * count + t) * CW + c % CW; }
+
+// one thread per (listed node, neighbour o): block (n, n + o), rows of n's corner and columns of the
+// neighbour's corner in each voxel holding both (s Kb for a uniformly scaled voxel, its own matrix
+// otherwise); the diagonal shift joins the centre block. FP32, 4-value chunks.
+__global__ void k_stn_build(LevelView L, Coefs<float> C, const int* __restrict__ list, int count, float* __restrict__ stn) {
+    const long long total = (long long)count * 27;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int t = int(e % count), m = int(e / count);
+        const long long n = list[t];
+        int i, j, k;
+        nodeCoords(L, n, i, j, k);
+        const int ox = m % 3 - 1, oy = (m / 3) % 3 - 1, oz = m / 9 - 1;
+        float blk[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int v = 0; v < 8; v++) {
+            const int di = v & 1, dj = (v >> 1) & 1, dk = v >> 2;
+            // the voxel at offset (di - 1, dj - 1, dk - 1) holds the neighbour when o - d + 1 is 0 or 1 per axis
+            const int bx = ox - di + 1, by = oy - dj + 1, bz = oz - dk + 1;
+            if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+            const int ei = i - 1 + di, ej = j - 1 + dj, ek = k - 1 + dk;
+            if (ei < 0 || ej < 0 || ek < 0 || ei >= L.nx || ej >= L.ny || ek >= L.nz) continue;
+            const uint32_t w = L.word[L.wi(ei, ej, ek)];
+            if (!w) continue;
+            const int a = cornerOf(1 - di, 1 - dj, 1 - dk), b = cornerOf(bx, by, bz);
+            if (!(w & OWN_BIT)) {
+                const float s = __uint_as_float(w);
+                for (int p = 0; p < 3; p++)
+                    for (int q = 0; q < 3; q++) blk[3 * p + q] += s * C.Kb[(3 * a + p) * 24 + 3 * b + q];
+            } else {
+                const float* M = L.own + (long long)(w & ~OWN_BIT) * 576;
+                for (int p = 0; p < 3; p++)
+                    for (int q = 0; q < 3; q++) blk[3 * p + q] += M[(3 * a + p) * 24 + 3 * b + q];
+            }
+        }
+        if (m == 13 && L.dadd32)
+            for (int p = 0; p < 3; p++) blk[4 * p] += L.dadd32[3 * n + p];
+        for (int c = 0; c < 9; c++) stn[stnAt<4>(9 * m + c, t, count)] = blk[c];
+    }
+}
+
+// largest |coefficient| (as the bits of a non-negative float, which order like integers)
+__global__ void k_stn_max(long long n, const float* __restrict__ stn, unsigned* __restrict__ out) {
+    float v = 0.f;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) v = fmaxf(v, fabsf(stn[e]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(v));
+}
+
+// FP16 copy of the coefficients over a power-of-two scale (8-value chunks)
+__global__ void k_stn_half(int count, const float* __restrict__ stn, float inv, __half* __restrict__ out) {
+    const long long total = (long long)count * 243;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int c = int(e / count);
+        const long long t = e % count;
+        out[stnAt<8>(c, t, count)] = __float2half_rn(stn[stnAt<4>(c, t, count)] * inv);
+    }
+}
+
+// one 16-byte chunk of coefficients as floats
+__device__ __forceinline__ void ldChunk(const float* p, float (&v)[4]) {
+    const float4 u = __ldcs(reinterpret_cast<const float4*>(p));
+    v[0] = u.x;
+    v[1] = u.y;
+    v[2] = u.z;
+    v[3] = u.w;
+}
+__device__ __forceinline__ void ldChunk(const __half* p, float (&v)[8]) {
+    const uint4 u = __ldcs(reinterpret_cast<const uint4*>(p));
+    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[e]));
+        v[2 * e] = f.x;
+        v[2 * e + 1] = f.y;
+    }
+}
+
+// One FP32 pass (APPLY / CHEB / RESID, the epilogues of k_list) over the listed nodes of a level
+// with their assembled stencils: ST = float, or __half times the level's power-of-two scale ss.
+// V = __half: the FP16 coarse-level vectors (rho and c2 as in k_list). Nodes off the list are not
+// written.
+template <int MODE, class ST, class V = float>
+__global__ void __launch_bounds__(256) k_stn(LevelView L, const int* __restrict__ list, int count, const ST* __restrict__ stn, float ss,
+                                             const V* __restrict__ x, V* __restrict__ y, const V* __restrict__ r, V* __restrict__ d, float c1,
+                                             float c2, float rho, int raw, Ctl ctl) {
+    if (skipped(ctl)) return;
+    constexpr bool H = !std::is_same<V, float>::value;
+    constexpr int CW = std::is_same<ST, float>::value ? 4 : 8;
+    const long long NX = L.PX, NXY = (long long)L.PX * L.NY;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count; t += (long long)gridDim.x * blockDim.x) {
+        const long long n = list[t];
+        const uint8_t mask = __ldg(L.nmask + n);
+        int i, j, k;
+        nodeCoords(L, n, i, j, k);
+        float a[3] = {0.f, 0.f, 0.f};
+        float cf[CW];
+        int have = -1;  // the chunk in cf (known at compile time once the loops are unrolled)
+#pragma unroll
+        for (int m = 0; m < 27; m++) {
+            const int ox = m % 3 - 1, oy = (m / 3) % 3 - 1, oz = m / 9 - 1;
+            // no voxel couples the node to a neighbour outside the grid: its values read as 0
+            const bool in = i + ox >= 0 && j + oy >= 0 && k + oz >= 0 && i + ox < L.NX && j + oy < L.NY && k + oz < L.NZ;
+            const V* xp = x + 3 * (n + ox + oy * NX + oz * NXY);
+            const float xm[3] = {in ? ldv<float>(xp) : 0.f, in ? ldv<float>(xp + 1) : 0.f, in ? ldv<float>(xp + 2) : 0.f};
+#pragma unroll
+            for (int e = 0; e < 9; e++) {
+                const int c = 9 * m + e;
+                if (c / CW != have) {
+                    have = c / CW;
+                    ldChunk(stn + ((long long)have * count + t) * CW, cf);
+                }
+                a[e / 3] += cf[c % CW] * xm[e % 3];
+            }
+        }
+        const float sc = (std::is_same<ST, float>::value ? 1.f : ss) * (H ? rho : 1.f);
+        const float acc[3] = {a[0] * sc, a[1] * sc, a[2] * sc};
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const long long id = 3 * n + q;
+            const bool fx = fixedDof(mask, q);
+            if (MODE == TOP_APPLY) {
+                stv(y + id, (!raw && fx) ? 0.f : acc[q]);
+            } else if (MODE == TOP_RESID) {
+                stv(y + id, fx ? 0.f : ldf(r + id) - acc[q]);
+            } else {
+                if (fx) {
+                    stv(d + id, 0.f);
+                    stv(y + id, 0.f);
+                } else {
+                    const float dn = c1 * ldf(d + id) + c2 * L.invD[id] * (ldf(r + id) - acc[q]);
+                    stv(d + id, dn);
+                    stv(y + id, ldf(x + id) + dn);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace dev
+}  // namespace psfea

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "libpsfea.so")
 
 PS_OK, PS_NOT_CONVERGED, PS_BREAKDOWN, PS_CANCELLED, PS_TIMEOUT, PS_PENDING = 0, 1, 2, 3, 4, 5
 PS_EINVAL, PS_ENONFINITE, PS_EOOM, PS_ECUDA, PS_ENODEV = 10, 11, 12, 13, 14
-PREC = {"fp64": 0, "mixed": 1, "fp32": 2}
+PREC = {"fp64": 0, "mixed": 1, "fp32": 2, "half": 3}
 CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the legacy default stream (PyTorch's default stream, reported as 0)
 STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "CANCELLED", 4: "TIMEOUT", 5: "PENDING", 10: "EINVAL", 11: "ENONFINITE",
                 12: "EOOM", 13: "ECUDA", 14: "ENODEV"}

@@ -39,7 +39,7 @@ def test_apply_fp64_every_level(name):
 
 
 @pytest.mark.parametrize("name", MODELS)
-@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32", "half"])
 def test_solve_matches_reference(name, precision):
     g = golden(name)
     S = make(g)
@@ -91,7 +91,7 @@ def test_precondition_close_to_oracle_and_linear():
     assert np.allclose([S.lmax(l) for l in range(S.n_levels - 1)], g["lmax"], rtol=1e-9)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32", "half"])
 def test_solve_after_other_calls_on_the_handle(precision):
     """Calls made before a solve on the same handle (product, preconditioner, stresses, reactions,
     a warm-started solve) must leave nothing behind that changes the solve: same iterations and

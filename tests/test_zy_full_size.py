@@ -3,7 +3,8 @@
 The reference's CPU solver (``ps::VoxelFEA``, compiled from its sources into oracle/_ref) and the
 CUDA path get the same arrays; compared are the level-0 fixed-DOF mask (bit-exact), the
 displacements (relative L2 <= 1e-6), the nodal von Mises stress (relative L2 <= 1e-6) and the
-iteration count of the FP64-Krylov forms (within 15 %; the FP32 V-cycle rounds differently). The
+iteration count of the FP64-Krylov forms (within 15 %; the FP32 V-cycle rounds differently; the
+FP32-Krylov forms, PS_PREC_FP32 and PS_PREC_HALF, within 25 % of it on the gyroid and SIMP). The
 reference solves run on a background thread over all host cores while the GPU solves run, one
 model after another:
 
@@ -102,9 +103,11 @@ def check_against_reference(S, m, ref, r, prec, label):
     assert r.converged, (label, prec, r.iterations, r.residual)
     err = rel(r.u, ref["u"])
     assert err <= U_TOL, (label, prec, err)
+    it = ref["iterations"]
     if prec in ("fp64", "mixed"):
-        it = ref["iterations"]
         assert abs(r.iterations - it) <= max(2, 0.15 * it), (label, prec, r.iterations, it)
+    else:
+        assert r.iterations <= max(it + 2, 1.25 * it), (label, prec, r.iterations, it)
     if ref["vm"] is not None:
         vm = S.stresses(r.u / (m.E * m.h), m.E, m.h, principals=False)[0]
         assert rel(vm, ref["vm"]) <= VM_TOL, (label, prec, rel(vm, ref["vm"]))
@@ -114,7 +117,7 @@ def check_against_reference(S, m, ref, r, prec, label):
 def test_gyroid_384x384x192_matches_reference(refs):
     m = refs.models["gyroid"]
     S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
-    runs = {p: S.solve(m.f, tol=1e-8, max_iter=3000, precision=p) for p in ("fp64", "mixed")}
+    runs = {p: S.solve(m.f, tol=1e-8, max_iter=3000, precision=p) for p in ("fp64", "mixed", "fp32", "half")}
     ref = refs.get(("gyroid", 0))
     assert ref["converged"], ref["residual"]
     assert np.array_equal(S.fixed(0), ref["fixed"])
@@ -126,7 +129,7 @@ def test_gyroid_384x384x192_matches_reference(refs):
 def test_simp_192x96x96_load_cases_match_reference(refs):
     m = refs.models["simp"]
     S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
-    runs = {q: {p: S.solve(m.f[q], tol=1e-8, max_iter=3000, precision=p) for p in ("fp64", "mixed")} for q in SIMP_CASES}
+    runs = {q: {p: S.solve(m.f[q], tol=1e-8, max_iter=3000, precision=p) for p in ("fp64", "mixed", "fp32", "half")} for q in SIMP_CASES}
     first = refs.get(("simp", SIMP_CASES[0]))
     assert np.array_equal(S.fixed(0), first["fixed"])
     for q in SIMP_CASES:
