@@ -870,10 +870,17 @@ __global__ void k_final(long long nNodes, const uint8_t* __restrict__ nmask, con
 
 // x32 += alpha p32, r32 -= alpha q32; est = ||r32|| / (scale * bnorm); fold when est <= tol or it has
 // fallen tenfold since the last fold, or at the iteration cap
+// (foldIf: the graph condition of the fold's branch, set to the decision); with the V-cycle's first
+// smoothing step from zero fused in, d = z = c0 D^-1 r32 (a fold redoes it on its new r32)
 __global__ void k_mx_update(long long nNodes, const uint8_t* __restrict__ nmask, float* __restrict__ x, float* __restrict__ r,
-                            const float* __restrict__ p, const float* __restrict__ q, SolveState* st, double* partials, unsigned* ticket,
-                            Ctl ctl) {
-    if (skipped(ctl) || st->fold) return;
+                            const float* __restrict__ p, const float* __restrict__ q, const float* __restrict__ invD, float* __restrict__ d,
+                            float* __restrict__ z, float c0, SolveState* st, double* partials, unsigned* ticket,
+                            cudaGraphConditionalHandle foldIf, Ctl ctl) {
+    if (skipped(ctl)) return;
+    if (st->fold) {  // a breakdown in the product: fold what there is
+        if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(foldIf, 1u);
+        return;
+    }
     const float alpha = float(st->alpha);
     double v[1] = {0};
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
@@ -886,6 +893,9 @@ __global__ void k_mx_update(long long nNodes, const uint8_t* __restrict__ nmask,
             const float rv = r[id] - alpha * q[id];
             r[id] = rv;
             v[0] += double(rv) * rv;
+            const float dv = c0 * invD[id] * rv;
+            d[id] = dv;
+            z[id] = dv;
         }
     }
     double tot[1];
@@ -894,6 +904,7 @@ __global__ void k_mx_update(long long nNodes, const uint8_t* __restrict__ nmask,
         st->it += 1;
         st->peak = fmax(st->peak, st->est);
         if (st->est <= st->tol || st->est <= st->foldFactor * st->peak || st->it >= st->maxIter || !(st->est == st->est)) st->fold = 1;
+        cudaGraphSetConditional(foldIf, st->fold ? 1u : 0u);
     }
 }
 
@@ -910,7 +921,8 @@ __global__ void k_mx_fold1(long long nDof, double* __restrict__ u, float* __rest
 // fold part 2 (after q = K u in FP64): r64 = f - q, rel = ||r64|| / bnorm, r32 = float(r64 * scale);
 // stop when rel <= tol, at the cap or after a breakdown
 __global__ void k_mx_fold2(long long nNodes, const uint8_t* __restrict__ nmask, const double* __restrict__ f, const double* __restrict__ q,
-                           float* __restrict__ r32, SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
+                           float* __restrict__ r32, const float* __restrict__ invD, float* __restrict__ d, float* __restrict__ z, float c0,
+                           SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
     if (skipped(ctl)) return;
     const double s = st->scale;
     double v[2] = {0, 0};
@@ -923,7 +935,11 @@ __global__ void k_mx_fold2(long long nNodes, const uint8_t* __restrict__ nmask, 
             if (!fixedDof(mask, c)) rv = f[id] - q[id];
             v[0] += rv * rv;
             v[1] = fmax(v[1], fabs(rv));
-            r32[id] = float(rv * s);
+            const float rs = float(rv * s);
+            r32[id] = rs;
+            const float dv = c0 * invD[id] * rs;
+            d[id] = dv;
+            z[id] = dv;
         }
     }
     double tot[2];
@@ -967,11 +983,19 @@ __global__ void k_mx_dots(long long nDof, const float* __restrict__ r, const flo
     }
 }
 
-// after a refinement fold: r32 *= rescale (runs while st->restart is set)
-__global__ void k_mx_rescale(long long nDof, float* __restrict__ r32, const SolveState* st, Ctl ctl) {
+// after a refinement fold: r32 *= rescale and the first smoothing step again (runs while
+// st->restart is set)
+__global__ void k_mx_rescale(long long nDof, float* __restrict__ r32, const float* __restrict__ invD, float* __restrict__ d,
+                             float* __restrict__ z, float c0, const SolveState* st, Ctl ctl) {
     if (skipped(ctl)) return;
     const float f = float(st->rescale);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x) r32[i] *= f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x) {
+        const float rs = r32[i] * f;
+        r32[i] = rs;
+        const float dv = c0 * invD[i] * rs;
+        d[i] = dv;
+        z[i] = dv;
+    }
 }
 
 __global__ void k_mx_p(long long nDof, const float* __restrict__ z, float* __restrict__ p, const SolveState* st, Ctl ctl) {
@@ -1367,6 +1391,21 @@ void upload(DevMem& m, const std::vector<T, A>& v, int64_t& total, cudaStream_t 
         if (s) check(cudaMemcpyAsync(m.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
         else check(cudaMemcpy(m.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
     }
+}
+
+// the kernel nodes of a graph's top level (memset and conditional nodes are not launches)
+int64_t kernelNodes(cudaGraph_t g) {
+    size_t n = 0;
+    check(cudaGraphGetNodes(g, nullptr, &n), "graph nodes");
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n) check(cudaGraphGetNodes(g, nodes.data(), &n), "graph nodes");
+    int64_t k = 0;
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        check(cudaGraphNodeGetType(nd, &t), "node type");
+        k += t == cudaGraphNodeTypeKernel ? 1 : 0;
+    }
+    return k;
 }
 
 int gridFor(int64_t n, int threads, int cap) {
@@ -1809,55 +1848,42 @@ void SharedModel::ensureStencils(bool half) {
     if (!stencilLevels) return;
     ensureActiveLists();
     std::lock_guard<std::mutex> g(listMu);
-    bool need = false;
-    for (size_t l = 1; l < L.size() && l < 63; l++) {
-        const DevLevel& D = L[l];
-        const int cnt = D.useTiles ? (D.split32 ? D.nBnd : 0) : nAct[l];
-        const bool on = ((stencilLevels >> l) & 1) && cnt > 0 && cnt >= stencilMinNodes;
-        if (on && (!D.stn32.p || (half && !D.stn16.p))) need = true;
-    }
-    if (!need) return;
-    unsigned* mx = nullptr;
-    unsigned* mxHost = nullptr;
+    bool built = false;
     for (size_t l = 1; l < L.size() && l < 63; l++) {
         DevLevel& D = L[l];
         const int cnt = D.useTiles ? (D.split32 ? D.nBnd : 0) : nAct[l];
         if (!((stencilLevels >> l) & 1) || cnt <= 0 || cnt < stencilMinNodes) continue;
-        if (!D.stn32.p) {
-            D.stnNodes = D.useTiles ? D.blist.as<int>() : act[l].as<int>();
-            D.nStn = D.useTiles ? D.nBnd : nAct[l];
-            if (!D.nStn) continue;
-            D.stn32.alloc(size_t(D.nStn) * dev::stnChunks<4>() * 4 * sizeof(float), bytes, ms);
-            dev::k_stn_build<<<gridFor(int64_t(D.nStn) * 27, 256, smCount * 32), 256, 0, ms>>>(D.view, D.c32, D.stnNodes, D.nStn,
-                                                                                             D.stn32.as<float>());
+        D.stnNodes = D.useTiles ? D.blist.as<int>() : act[l].as<int>();
+        D.nStn = cnt;
+        const int grid = gridFor(int64_t(cnt) * 27, 256, smCount * 32);
+        if (!half && !D.stn32.p) {
+            D.stn32.alloc(size_t(cnt) * dev::stnChunks<4>() * 4 * sizeof(float), bytes, ms);
+            dev::k_stn_build<float><<<grid, 256, 0, ms>>>(D.view, D.c32, D.stnNodes, cnt, D.stn32.as<float>(), 1.f);
             check(cudaGetLastError(), "stencil build");
+            built = true;
         }
-        if (half && !D.stn16.p && D.nStn) {
-            if (!mx) {
-                check(cudaMalloc(&mx, sizeof(unsigned)), "cudaMalloc");
-                check(cudaMallocHost(&mxHost, sizeof(unsigned)), "cudaMallocHost");
-            }
-            const int64_t ne = int64_t(D.nStn) * dev::stnChunks<4>() * 4;
-            check(cudaMemsetAsync(mx, 0, sizeof(unsigned), ms), "memset");
-            dev::k_stn_max<<<gridFor(ne, 256, smCount * 8), 256, 0, ms>>>(ne, D.stn32.as<float>(), mx);
-            check(cudaMemcpyAsync(mxHost, mx, sizeof(unsigned), cudaMemcpyDeviceToHost, ms), "copy");
-            check(cudaStreamSynchronize(ms), "stencil scale");
-            float kmax;
-            std::memcpy(&kmax, mxHost, sizeof kmax);
-            // the largest coefficient near 2^14, as for the FP16 element matrices
-            D.stnScale = kmax > 0 ? float(std::exp2(std::ceil(std::log2(double(kmax) / 16384.0)))) : 1.f;
-            D.stn16.alloc(size_t(D.nStn) * dev::stnChunks<8>() * 8 * sizeof(__half), bytes, ms);
-            dev::k_stn_half<<<gridFor(int64_t(D.nStn) * 243, 256, smCount * 8), 256, 0, ms>>>(D.nStn, D.stn32.as<float>(), 1.f / D.stnScale,
-                                                                                              D.stn16.as<__half>());
-            check(cudaGetLastError(), "stencil halves");
+        if (half && !D.stn16.p) {
+            // a bound on every coefficient (at most 8 voxels add to one): 8 x the largest element
+            // entry (own matrices below 2^14 hs; s Kb; the diagonal shift), kept below 2^14
+            const HostLevel& h = H.levels[l];
+            double emax = D.hasOwn ? 16384.0 * double(D.view.hs) : 0.0, kb = 0.0, smax = 0.0, dmax = 0.0;
+            for (int e = 0; e < 576; e++) kb = std::max(kb, double(std::fabs(D.c32.Kb[e])));
+            for (uint32_t w : h.word)
+                if (w && !(w & OWN_BIT)) {
+                    float sv;
+                    std::memcpy(&sv, &w, sizeof sv);
+                    smax = std::max(smax, double(std::fabs(sv)));
+                }
+            for (double v : h.diagAdd) dmax = std::max(dmax, std::fabs(v));
+            const double bound = 8.0 * std::max(emax, smax * kb) + dmax;
+            D.stnScale = bound > 0 ? float(std::exp2(std::ceil(std::log2(bound / 16384.0)))) : 1.f;
+            D.stn16.alloc(size_t(cnt) * dev::stnChunks<8>() * 8 * sizeof(__half), bytes, ms);
+            dev::k_stn_build<__half><<<grid, 256, 0, ms>>>(D.view, D.c32, D.stnNodes, cnt, D.stn16.as<__half>(), 1.f / D.stnScale);
+            check(cudaGetLastError(), "stencil build");
+            built = true;
         }
     }
-    if (mx) {
-        check(cudaStreamSynchronize(ms), "stencils");
-        cudaFree(mx);
-        cudaFreeHost(mxHost);
-    }
-    check(cudaEventRecord(readyEv, ms), "event");
+    if (built) check(cudaEventRecord(readyEv, ms), "event");
 }
 
 void SharedModel::ensureActiveLists() {
@@ -1929,6 +1955,10 @@ struct SolverImpl {
     cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
     int64_t graphKernels[4] = {0, 0, 0, 0};
     int64_t graphVersion[4] = {-1, -1, -1, -1};
+    // the FP32-Krylov forms' fold runs in a conditional branch of the iteration graph (captured on
+    // the side stream): foldKernels of them per fold
+    cudaStream_t sideStream = nullptr;
+    int64_t foldKernels = 0;
 
     // smoother estimation in flight: its scratch (stream-ordered, freed as soon as the kernels
     // have run) and the Lanczos scalars of every level, copied to pinned host memory
@@ -2058,6 +2088,7 @@ struct SolverImpl {
         for (auto& w : W) w.release();
         for (DevMem* b : {&f, &x, &r, &p, &q, &z64, &x32, &p32, &q32, &state, &partials, &ticket}) b->release();
         if (ev) cudaEventDestroy(ev);
+        if (sideStream) cudaStreamDestroy(sideStream);
         if (hostState) cudaFreeHost(hostState);
         if (lzHost) cudaFreeHost(lzHost);
         if (ownStream) {
@@ -2573,17 +2604,49 @@ void SolverImpl::recordMixedIteration(dev::Ctl ctl, bool refine, bool half) {
         launch(dev::k_tile<float, dev::TOP_DOT, false, true>, D.nTiles, dev::TILE_THREADS, dev::tileSmemBytes<float, dev::TOP_DOT, true>(), stream, D.view,
                D.c32, D.tiles.as<uint32_t>(), mp, io, st(), part(), tick(), dev::Ctl{ctl.skipIf, nullptr});
     }
+    // the fold (u += x32, the FP64 defect as the new r32) is due every few iterations only: it sits
+    // in a conditional branch that the update kernel opens, so that iterations without it launch
+    // none of its kernels (a skipped tiled launch still dispatches all its CTAs)
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    check(cudaStreamGetCaptureInfo_v3(stream, &cs, nullptr, &cg, nullptr, nullptr, nullptr), "capture info");
+    cudaGraphConditionalHandle foldIf;
+    check(cudaGraphConditionalHandleCreate(&foldIf, cg, 0, cudaGraphCondAssignDefault), "conditional handle");
+    float* invD0 = D.invD.as<float>();
+    float *d0 = W0.d.as<float>(), *z0 = W0.z.as<float>();
     launch(dev::k_mx_update, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, x32.as<float>(), W0.r.as<float>(),
-           p32.as<float>(), q32.as<float>(), st(), part(), tick(), ctl);
+           p32.as<float>(), q32.as<float>(), invD0, d0, z0, D.cf0, st(), part(), tick(), foldIf, ctl);
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nDeps = 0;
+    check(cudaStreamGetCaptureInfo_v3(stream, &cs, nullptr, &cg, &deps, nullptr, &nDeps), "capture info");
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = foldIf;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t foldNode;
+    check(cudaGraphAddNode(&foldNode, cg, deps, nDeps, &cp), "conditional node");
+    check(cudaStreamUpdateCaptureDependencies(stream, &foldNode, 1, cudaStreamSetCaptureDependencies), "capture dependencies");
+    if (!sideStream) check(cudaStreamCreateWithFlags(&sideStream, cudaStreamNonBlocking), "stream");
+    cudaStream_t mainStream = stream;
+    stream = sideStream;
+    check(cudaStreamBeginCaptureToGraph(stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+          "capture the fold");
+    const int64_t before = launches;
     const dev::Ctl foldCtl{ctl.skipIf, foldFlag};
     launch(dev::k_mx_fold1, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), x.as<double>(), x32.as<float>(), st(), foldCtl);
     op64(0, x.as<double>(), q.as<double>(), false, foldCtl);
     launch(dev::k_mx_fold2, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, f.as<double>(), q.as<double>(),
-           W0.r.as<float>(), st(), part(), tick(), foldCtl);
+           W0.r.as<float>(), invD0, d0, z0, D.cf0, st(), part(), tick(), foldCtl);
     if (refine)
-        launch(dev::k_mx_rescale, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), W0.r.as<float>(), st(),
+        launch(dev::k_mx_rescale, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), W0.r.as<float>(), invD0, d0, z0, D.cf0, st(),
                dev::Ctl{ctl.skipIf, &st()->restart});
-    float* z32 = vcycleFor(half, ctl, M->mixedOwn16);
+    foldKernels = launches - before;
+    launches = before;  // counted per fold when the solve reports its kernels
+    cudaGraph_t body = nullptr;
+    check(cudaStreamEndCapture(stream, &body), "capture the fold");
+    stream = mainStream;
+    float* z32 = vcycleFor(half, ctl, M->mixedOwn16, true);  // the first smoothing step came with the update or the fold
     launch(dev::k_mx_dots, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), W0.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
     launch(dev::k_mx_p, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), z32, p32.as<float>(), st(), ctl);
 }
@@ -2698,10 +2761,9 @@ void SolverImpl::startIterations() {
         if (mixed) recordMixedIteration(ctl, refine, half);
         else recordPlainIteration(ctl, own16);
         check(cudaStreamEndCapture(stream, &gr), "capture end");
-        size_t nodes = 0;
-        check(cudaGraphGetNodes(gr, nullptr, &nodes), "graph nodes");
-        graphKernels[gi] = int64_t(nodes);
-        launches -= int64_t(nodes);  // captured, not run
+        const int64_t kn = kernelNodes(gr);
+        graphKernels[gi] = kn;
+        launches -= kn;  // captured, not run
         check(cudaGraphInstantiate(&graph[gi], gr, 0), "instantiate");
         cudaGraphDestroy(gr);
         graphVersion[gi] = M->version;
@@ -2797,7 +2859,7 @@ bool SolverImpl::advance(bool block, ps_solve_result& res) {
         else if (!res.converged) outcome = PS_NOT_CONVERGED;
     }
     res.status = outcome;
-    res.kernels = launches - pend.launches0;
+    res.kernels = launches - pend.launches0 + (pend.mixed ? int64_t(hs.folds) * foldKernels : 0);
     res.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - pend.t0).count();
     pend.active = false;
     return true;

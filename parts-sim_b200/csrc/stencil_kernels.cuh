@@ -27,10 +27,16 @@ __host__ __device__ constexpr int stnChunks() { return (243 + CW - 1) / CW; }
 template <int CW>
 __host__ __device__ __forceinline__ long long stnAt(int c, long long t, long long count) { return ((c / CW) * count + t) * CW + c % CW; }
 
+__device__ __forceinline__ void stStn(float* p, float v, float) { *p = v; }
+__device__ __forceinline__ void stStn(__half* p, float v, float inv) { *p = __float2half_rn(v * inv); }
+
 // one thread per (listed node, neighbour o): block (n, n + o), rows of n's corner and columns of the
 // neighbour's corner in each voxel holding both (s Kb for a uniformly scaled voxel, its own matrix
-// otherwise); the diagonal shift joins the centre block. FP32, 4-value chunks.
-__global__ void k_stn_build(LevelView L, Coefs<float> C, const int* __restrict__ list, int count, float* __restrict__ stn) {
+// otherwise); the diagonal shift joins the centre block. FP32 sums, stored as floats (4-value
+// chunks) or as halves times inv (8-value chunks).
+template <class ST>
+__global__ void k_stn_build(LevelView L, Coefs<float> C, const int* __restrict__ list, int count, ST* __restrict__ stn, float inv) {
+    constexpr int CW = 16 / int(sizeof(ST));
     const long long total = (long long)count * 27;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
         const int t = int(e % count), m = int(e / count);
@@ -61,26 +67,7 @@ __global__ void k_stn_build(LevelView L, Coefs<float> C, const int* __restrict__
         }
         if (m == 13 && L.dadd32)
             for (int p = 0; p < 3; p++) blk[4 * p] += L.dadd32[3 * n + p];
-        for (int c = 0; c < 9; c++) stn[stnAt<4>(9 * m + c, t, count)] = blk[c];
-    }
-}
-
-// largest |coefficient| (as the bits of a non-negative float, which order like integers)
-__global__ void k_stn_max(long long n, const float* __restrict__ stn, unsigned* __restrict__ out) {
-    float v = 0.f;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) v = fmaxf(v, fabsf(stn[e]));
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(v));
-}
-
-// FP16 copy of the coefficients over a power-of-two scale (8-value chunks)
-__global__ void k_stn_half(int count, const float* __restrict__ stn, float inv, __half* __restrict__ out) {
-    const long long total = (long long)count * 243;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
-        const int c = int(e / count);
-        const long long t = e % count;
-        out[stnAt<8>(c, t, count)] = __float2half_rn(stn[stnAt<4>(c, t, count)] * inv);
+        for (int c = 0; c < 9; c++) stStn(stn + stnAt<CW>(9 * m + c, t, count), blk[c], inv);
     }
 }
 

@@ -4,7 +4,8 @@ The reference's CPU solver (``ps::VoxelFEA``, compiled from its sources into ora
 CUDA path get the same arrays; compared are the level-0 fixed-DOF mask (bit-exact), the
 displacements (relative L2 <= 1e-6), the nodal von Mises stress (relative L2 <= 1e-6) and the
 iteration count of the FP64-Krylov forms (within 15 %; the FP32 V-cycle rounds differently; the
-FP32-Krylov forms, PS_PREC_FP32 and PS_PREC_HALF, within 25 % of it on the gyroid and SIMP). The
+FP32-Krylov forms within 25 % (PS_PREC_FP32, reliable updates) and 35 % (PS_PREC_HALF, whose
+refinement restarts the recurrence) of it on the gyroid and SIMP). The
 reference solves run on a background thread over all host cores while the GPU solves run, one
 model after another:
 
@@ -107,7 +108,7 @@ def check_against_reference(S, m, ref, r, prec, label):
     if prec in ("fp64", "mixed"):
         assert abs(r.iterations - it) <= max(2, 0.15 * it), (label, prec, r.iterations, it)
     else:
-        assert r.iterations <= max(it + 2, 1.25 * it), (label, prec, r.iterations, it)
+        assert r.iterations <= max(it + 2, (1.25 if prec == "fp32" else 1.35) * it), (label, prec, r.iterations, it)
     if ref["vm"] is not None:
         vm = S.stresses(r.u / (m.E * m.h), m.E, m.h, principals=False)[0]
         assert rel(vm, ref["vm"]) <= VM_TOL, (label, prec, rel(vm, ref["vm"]))
