@@ -875,10 +875,10 @@ __global__ void k_final(long long nNodes, const uint8_t* __restrict__ nmask, con
 __global__ void k_mx_update(long long nNodes, const uint8_t* __restrict__ nmask, float* __restrict__ x, float* __restrict__ r,
                             const float* __restrict__ p, const float* __restrict__ q, const float* __restrict__ invD, float* __restrict__ d,
                             float* __restrict__ z, float c0, SolveState* st, double* partials, unsigned* ticket,
-                            cudaGraphConditionalHandle foldIf, Ctl ctl) {
+                            cudaGraphConditionalHandle foldIf, int useIf, Ctl ctl) {
     if (skipped(ctl)) return;
     if (st->fold) {  // a breakdown in the product: fold what there is
-        if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(foldIf, 1u);
+        if (useIf && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(foldIf, 1u);
         return;
     }
     const float alpha = float(st->alpha);
@@ -904,7 +904,7 @@ __global__ void k_mx_update(long long nNodes, const uint8_t* __restrict__ nmask,
         st->it += 1;
         st->peak = fmax(st->peak, st->est);
         if (st->est <= st->tol || st->est <= st->foldFactor * st->peak || st->it >= st->maxIter || !(st->est == st->est)) st->fold = 1;
-        cudaGraphSetConditional(foldIf, st->fold ? 1u : 0u);
+        if (useIf) cudaGraphSetConditional(foldIf, st->fold ? 1u : 0u);
     }
 }
 
@@ -1393,21 +1393,6 @@ void upload(DevMem& m, const std::vector<T, A>& v, int64_t& total, cudaStream_t 
     }
 }
 
-// the kernel nodes of a graph's top level (memset and conditional nodes are not launches)
-int64_t kernelNodes(cudaGraph_t g) {
-    size_t n = 0;
-    check(cudaGraphGetNodes(g, nullptr, &n), "graph nodes");
-    std::vector<cudaGraphNode_t> nodes(n);
-    if (n) check(cudaGraphGetNodes(g, nodes.data(), &n), "graph nodes");
-    int64_t k = 0;
-    for (cudaGraphNode_t nd : nodes) {
-        cudaGraphNodeType t;
-        check(cudaGraphNodeGetType(nd, &t), "node type");
-        k += t == cudaGraphNodeTypeKernel ? 1 : 0;
-    }
-    return k;
-}
-
 int gridFor(int64_t n, int threads, int cap) {
     const int64_t b = (n + threads - 1) / threads;
     return int(std::max<int64_t>(1, std::min<int64_t>(b, cap)));
@@ -1583,6 +1568,7 @@ struct SharedModel {
     void ensureStencils(bool half);
     int64_t stencilLevels = ~int64_t(1);  // PSFEA_STENCIL_LEVELS: bit l = level l (never level 0)
     int64_t stencilMinNodes = 65536;      // PSFEA_STENCIL_MIN_NODES: smaller node lists keep the gather
+    bool foldBranch = true;               // PSFEA_FOLD_BRANCH: the FP32-Krylov fold as a conditional graph branch
     bool exactOneLevel() const { return L.size() == 1 && H.hasFactor(); }
 };
 
@@ -1604,6 +1590,7 @@ void SharedModel::adopt(Hierarchy&& h) {
     if (const char* e = std::getenv("PSFEA_REFINE_ETA")) refineEta = std::atof(e);
     if (const char* e = std::getenv("PSFEA_STENCIL_LEVELS")) stencilLevels = std::atoll(e) & ~int64_t(1);
     if (const char* e = std::getenv("PSFEA_STENCIL_MIN_NODES")) stencilMinNodes = std::atoll(e);
+    if (const char* e = std::getenv("PSFEA_FOLD_BRANCH")) foldBranch = std::atoi(e) != 0;
     if (const char* e = std::getenv("PSFEA_EBE_SPLIT")) ebeSplit = std::atoi(e) == 1 ? 1 : 3;
     check(cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking), "stream");
     check(cudaEventCreateWithFlags(&readyEv, cudaEventDisableTiming), "event");
@@ -2607,15 +2594,36 @@ void SolverImpl::recordMixedIteration(dev::Ctl ctl, bool refine, bool half) {
     // the fold (u += x32, the FP64 defect as the new r32) is due every few iterations only: it sits
     // in a conditional branch that the update kernel opens, so that iterations without it launch
     // none of its kernels (a skipped tiled launch still dispatches all its CTAs)
+    // (PSFEA_FOLD_BRANCH=0: the fold's kernels inline, each skipping itself unless due; ncu cannot
+    // profile the kernels of a graph with a conditional node)
+    const bool branch = M->foldBranch;
     cudaStreamCaptureStatus cs;
     cudaGraph_t cg = nullptr;
-    check(cudaStreamGetCaptureInfo_v3(stream, &cs, nullptr, &cg, nullptr, nullptr, nullptr), "capture info");
-    cudaGraphConditionalHandle foldIf;
-    check(cudaGraphConditionalHandleCreate(&foldIf, cg, 0, cudaGraphCondAssignDefault), "conditional handle");
+    cudaGraphConditionalHandle foldIf = 0;
+    if (branch) {
+        check(cudaStreamGetCaptureInfo_v3(stream, &cs, nullptr, &cg, nullptr, nullptr, nullptr), "capture info");
+        check(cudaGraphConditionalHandleCreate(&foldIf, cg, 0, cudaGraphCondAssignDefault), "conditional handle");
+    }
     float* invD0 = D.invD.as<float>();
     float *d0 = W0.d.as<float>(), *z0 = W0.z.as<float>();
     launch(dev::k_mx_update, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, x32.as<float>(), W0.r.as<float>(),
-           p32.as<float>(), q32.as<float>(), invD0, d0, z0, D.cf0, st(), part(), tick(), foldIf, ctl);
+           p32.as<float>(), q32.as<float>(), invD0, d0, z0, D.cf0, st(), part(), tick(), foldIf, branch ? 1 : 0, ctl);
+    const dev::Ctl foldCtl{ctl.skipIf, foldFlag};
+    if (!branch) {
+        launch(dev::k_mx_fold1, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), x.as<double>(), x32.as<float>(), st(), foldCtl);
+        op64(0, x.as<double>(), q.as<double>(), false, foldCtl);
+        launch(dev::k_mx_fold2, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, f.as<double>(), q.as<double>(),
+               W0.r.as<float>(), invD0, d0, z0, D.cf0, st(), part(), tick(), foldCtl);
+        if (refine)
+            launch(dev::k_mx_rescale, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), W0.r.as<float>(), invD0, d0, z0, D.cf0, st(),
+                   dev::Ctl{ctl.skipIf, &st()->restart});
+        foldKernels = 0;
+        float* z32 = vcycleFor(half, ctl, M->mixedOwn16, true);
+        launch(dev::k_mx_dots, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), W0.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(),
+               ctl);
+        launch(dev::k_mx_p, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), z32, p32.as<float>(), st(), ctl);
+        return;
+    }
     const cudaGraphNode_t* deps = nullptr;
     size_t nDeps = 0;
     check(cudaStreamGetCaptureInfo_v3(stream, &cs, nullptr, &cg, &deps, nullptr, &nDeps), "capture info");
@@ -2633,7 +2641,6 @@ void SolverImpl::recordMixedIteration(dev::Ctl ctl, bool refine, bool half) {
     check(cudaStreamBeginCaptureToGraph(stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
           "capture the fold");
     const int64_t before = launches;
-    const dev::Ctl foldCtl{ctl.skipIf, foldFlag};
     launch(dev::k_mx_fold1, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), x.as<double>(), x32.as<float>(), st(), foldCtl);
     op64(0, x.as<double>(), q.as<double>(), false, foldCtl);
     launch(dev::k_mx_fold2, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, f.as<double>(), q.as<double>(),
@@ -2757,13 +2764,16 @@ void SolverImpl::startIterations() {
     }
     if (!graph[gi]) {
         cudaGraph_t gr;
+        // the kernels of one replay: the launches made while recording (the fold branch's are
+        // counted per fold; a graph's node types are not queried, the driver does not report the
+        // conditional node's)
+        const int64_t l0 = launches;
         check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
         if (mixed) recordMixedIteration(ctl, refine, half);
         else recordPlainIteration(ctl, own16);
         check(cudaStreamEndCapture(stream, &gr), "capture end");
-        const int64_t kn = kernelNodes(gr);
-        graphKernels[gi] = kn;
-        launches -= kn;  // captured, not run
+        graphKernels[gi] = launches - l0;
+        launches = l0;  // captured, not run
         check(cudaGraphInstantiate(&graph[gi], gr, 0), "instantiate");
         cudaGraphDestroy(gr);
         graphVersion[gi] = M->version;
@@ -3143,13 +3153,12 @@ struct BlockImpl final : BlockBase {
         }
         if (!graph[gi]) {
             cudaGraph_t gr;
+            const int64_t l0 = launches;
             check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
             recordIteration(ctl, own16);
             check(cudaStreamEndCapture(stream, &gr), "capture end");
-            size_t nodes = 0;
-            check(cudaGraphGetNodes(gr, nullptr, &nodes), "graph nodes");
-            graphKernels[gi] = int64_t(nodes);
-            launches -= int64_t(nodes);
+            graphKernels[gi] = launches - l0;
+            launches = l0;
             check(cudaGraphInstantiate(&graph[gi], gr, 0), "instantiate");
             cudaGraphDestroy(gr);
             graphVersion[gi] = M->version;
