@@ -36,10 +36,10 @@ MAX_ITER = 5000
 # mask byte, r, d, 1/diag read and d written: 4x12 B) and per solid voxel (its 4-byte word)
 BYTES_PER_NODE_CHEB32 = 12 + 12 + 1 + 4 * 12
 BYTES_PER_VOXEL = 4
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of that kernel on the
-# headline model, from an ncu capture of `bench.py --kernel-only cheb32 --kernel-workload gyroid`
-# (None until captured)
-TRAFFIC_BYTES_CHEB32 = None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of that kernel per active node, from an
+# ncu capture of one launch on the 256x256x128 gyroid (same period and wall thickness as the
+# headline lattice: 634.8 MB for 3,290,503 active nodes), scaled to a launch by the active nodes
+TRAFFIC_PER_ACTIVE_NODE_CHEB32 = 634.8e6 / 3290503
 
 HEADLINE = "gyroid"
 HEADLINE_FORM = "fp32"  # the precision form of `value` and `e2e` (plain FP64 and the others reported beside it)
@@ -580,7 +580,7 @@ def main():
         "setup_s": setup_s,  # model creation (outside the timed solves): the setup path
         "e2e": {"value": e2e_value, "unit": "MDOF/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": TRAFFIC_BYTES_CHEB32, "kernel": "k_tile<float,TOP_CHEB> level 0 (FP32 Chebyshev step)", "ms": ms_cheb,
+                     "traffic": TRAFFIC_PER_ACTIVE_NODE_CHEB32 * act_nodes, "kernel": "k_tile<float,TOP_CHEB> level 0 (FP32 Chebyshev step)", "ms": ms_cheb,
                      "algorithmic_bytes": alg_bytes, "peak_kind": peak_kind, "fp64_apply_ms": ms_apply64},
         "l_bracket": lbr,
         "batched": batched,

@@ -22,6 +22,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
 #include <map>
 #include <memory>
@@ -620,12 +621,16 @@ __global__ void k_restrict(LevelView F, LevelView C, const VF* __restrict__ rf, 
 }
 
 // zf += P zc at free fine DOFs (trilinear: coarse i/2 and, when odd, (i+1)/2, weight 1/2 each);
-// VC / VF as in k_restrict, the iterate scales differing by the power of two sp: zf += sp P zc
+// VC / VF as in k_restrict, the iterate scales differing by the power of two sp: zf += sp P zc.
+// list: the fine level's active nodes (inactive ones are all held and never written), or null for
+// every node of the level.
 template <class VC = float, class VF = float>
-__global__ void k_prolong(LevelView F, int CPX, int CNY, const VC* __restrict__ zc, VF* __restrict__ zf, float sp, Ctl ctl) {
+__global__ void k_prolong(LevelView F, int CPX, int CNY, const int* __restrict__ list, long long count, const VC* __restrict__ zc,
+                          VF* __restrict__ zf, float sp, Ctl ctl) {
     if (skipped(ctl)) return;
     const long long CNX = CPX, CNXY = (long long)CPX * CNY;
-    for (long long fn = blockIdx.x * (long long)blockDim.x + threadIdx.x; fn < F.nNodes; fn += (long long)gridDim.x * blockDim.x) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count; t += (long long)gridDim.x * blockDim.x) {
+        const long long fn = list ? (long long)list[t] : t;
         const uint8_t mask = F.nmask[fn];
         if ((mask & 7) == 7) continue;
         int i, j, k;
@@ -1532,6 +1537,7 @@ struct SharedModel {
     bool halfOk = false;  // every level >= 1 fits FP16 with its scale
     double refineEta = 0.1;
     std::mutex listMu;
+    std::atomic<bool> actReady{false};  // act / nAct complete for every level
     cudaStream_t ms = nullptr;     // allocation / upload stream of the shared data
     cudaEvent_t readyEv = nullptr; // recorded when the uploads are done; contexts wait on it
 
@@ -1913,6 +1919,7 @@ void SharedModel::ensureActiveLists() {
             upload(btTiles, tl, bytes, ms);
         }
     }
+    actReady.store(true, std::memory_order_release);
     check(cudaEventRecord(readyEv, ms), "event");
 }
 
@@ -2011,6 +2018,10 @@ struct SolverImpl {
         check(cudaMemcpyAsync(host, staging, n * 8, cudaMemcpyDeviceToHost, stream), "download");
     }
     int vecGrid(int64_t n) const { return gridFor(n, dev::VEC_THREADS, smCount * 8); }
+    // level l's active-node list when the model has made them (the prolongation's work list)
+    // (only once this context's stream has waited for the lists' upload)
+    const int* fineList(int l) const { return listsWaited ? M->act[size_t(l)].as<int>() : nullptr; }
+    bool listsWaited = false;
     dev::SolveState* st() const { return state.as<dev::SolveState>(); }
     double* part() const { return partials.as<double>(); }
     unsigned* tick() const { return ticket.as<unsigned>(); }
@@ -2303,7 +2314,12 @@ float* SolverImpl::vcycle(int l, dev::Ctl ctl, bool own16, bool firstDone) {
     launch(dev::k_restrict<float, float>, gridFor(pn(l + 1), 256, smCount * 16), 256, 0, stream, D.view, C.view, b, Wc.r.as<float>(),
            fuse ? Wc.d.as<float>() : nullptr, fuse ? Wc.z.as<float>() : nullptr, c0c, 1.f, ctl);
     float* zc = vcycle(l + 1, ctl, own16, fuse);
-    launch(dev::k_prolong<float, float>, gridFor(pn(l), 256, smCount * 16), 256, 0, stream, D.view, C.view.PX, hc.NY, zc, a, 1.f, ctl);
+    {
+        const int* pl = fineList(l);
+        const int64_t pc = pl ? M->nAct[size_t(l)] : pn(l);
+        launch(dev::k_prolong<float, float>, gridFor(pc, 256, smCount * 16), 256, 0, stream, D.view, C.view.PX, hc.NY, pl, (long long)pc, zc, a,
+               1.f, ctl);
+    }
     op32<dev::OP_CHEB>(l, a, b, 0.f, D.cf0, ctl, own16);  // post-smoothing: d = c0 D^-1 (r - K a); b = a + d
     std::swap(a, b);
     for (size_t k = 0; k < D.chebC1.size(); k++) {
@@ -2362,7 +2378,12 @@ float* SolverImpl::vcycleHalf(dev::Ctl ctl, bool own16, bool firstDone) {
     launch(dev::k_restrict<float, __half>, gridFor(pn(1), 256, smCount * 16), 256, 0, stream, D.view, C.view, b, Wc.r.as<__half>(),
            fuse ? Wc.d.as<__half>() : nullptr, fuse ? Wc.z.as<__half>() : nullptr, c0c * dc, 0.125f, ctl);
     const __half* zc = vcycle16(1, ctl, own16, fuse);
-    launch(dev::k_prolong<__half, float>, gridFor(pn(0), 256, smCount * 16), 256, 0, stream, D.view, C.view.PX, hc.NY, zc, a, 8.f / dc, ctl);
+    {
+        const int* pl = fineList(0);
+        const int64_t pc = pl ? M->nAct[0] : pn(0);
+        launch(dev::k_prolong<__half, float>, gridFor(pc, 256, smCount * 16), 256, 0, stream, D.view, C.view.PX, hc.NY, pl, (long long)pc, zc, a,
+               8.f / dc, ctl);
+    }
     op32<dev::OP_CHEB>(0, a, b, 0.f, D.cf0, ctl, own16);
     std::swap(a, b);
     for (size_t k = 0; k < D.chebC1.size(); k++) {
@@ -2418,8 +2439,12 @@ __half* SolverImpl::vcycle16(int l, dev::Ctl ctl, bool own16, bool firstDone) {
     launch(dev::k_restrict<__half, __half>, gridFor(pn(l + 1), 256, smCount * 16), 256, 0, stream, D.view, C.view, b, Wc.r.as<__half>(),
            fuse ? Wc.d.as<__half>() : nullptr, fuse ? Wc.z.as<__half>() : nullptr, c0c * dc, 0.125f, ctl);
     const __half* zc = vcycle16(l + 1, ctl, own16, fuse);
-    launch(dev::k_prolong<__half, __half>, gridFor(pn(l), 256, smCount * 16), 256, 0, stream, D.view, C.view.PX, hc.NY, zc, a, 8.f * dl / dc,
-           ctl);
+    {
+        const int* pl = fineList(l);
+        const int64_t pc = pl ? M->nAct[size_t(l)] : pn(l);
+        launch(dev::k_prolong<__half, __half>, gridFor(pc, 256, smCount * 16), 256, 0, stream, D.view, C.view.PX, hc.NY, pl, (long long)pc, zc, a,
+               8.f * dl / dc, ctl);
+    }
     op16<dev::OP_CHEB>(l, a, b, 0.f, D.cf0, ctl, own16);
     std::swap(a, b);
     for (size_t k = 0; k < D.chebC1.size(); k++) {
@@ -2696,7 +2721,9 @@ void SolverImpl::startIterations() {
     pend.half = half;
     if (!exactOneLevel()) {
         M->ensureStencils(own16 || (mixed && M->mixedOwn16));
+        const bool ready = M->actReady.load(std::memory_order_acquire);
         check(cudaStreamWaitEvent(stream, M->readyEv, 0), "wait");
+        listsWaited = listsWaited || ready;
     }
     if (half) {
         M->ensureActiveLists();

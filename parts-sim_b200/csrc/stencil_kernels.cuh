@@ -7,8 +7,9 @@
 // node instead keeps its assembled row: the 27 3x3 blocks coupling it to its neighbours, summed once
 // at setup over the voxels the two nodes share. A pass then streams 243 coefficients per node
 // (coalesced: 16-byte chunks, chunk-major over the node list) and does 243 multiply-adds; the
-// gather of the 27 neighbours' values is unchanged. The sums run in another order than the per-voxel gather
-// (FP32 rounding differs; the stored blocks are the exact sums of the same FP32 matrices).
+// gather of the 27 neighbours' values is unchanged. The sums run in another order than the
+// per-voxel gather (FP32 rounding differs; the stored blocks are the exact sums of the same FP32
+// matrices).
 #pragma once
 
 #include "kernels.cuh"
