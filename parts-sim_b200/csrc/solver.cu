@@ -2019,6 +2019,8 @@ struct SolverImpl {
     }
     int vecGrid(int64_t n) const { return gridFor(n, dev::VEC_THREADS, smCount * 8); }
     // level l's active-node list when the model has made them (the prolongation's work list)
+    // the V-cycle being recorded reads the FP16 stencils (the FP32-Krylov forms)
+    bool stn16Pass = false;
     // (only once this context's stream has waited for the lists' upload)
     const int* fineList(int l) const { return listsWaited ? M->act[size_t(l)].as<int>() : nullptr; }
     bool listsWaited = false;
@@ -2178,17 +2180,21 @@ void SolverImpl::op32(int l, const float* xin, float* y, float c1, float c2, dev
     }
     const bool o16 = own16 && D.hasOwn, diff = o16 && M->ownDiff;
     constexpr int SM_ = MODE == dev::OP_CHEB ? dev::TOP_CHEB : (MODE == dev::OP_RESID ? dev::TOP_RESID : dev::TOP_APPLY);
-    // the assembled stencils of the listed nodes (FP16 in the reduced-precision forms)
+    // the assembled stencils of the listed nodes: FP16 in the FP32-Krylov forms, FP32 in the
+    // FP64-Krylov ones (PS_PREC_MIXED included: FP16 rounding of the assembled sums, the uniformly
+    // scaled voxels' exact FP32 part included, moved its iteration count on the ill-conditioned
+    // L-bracket at rel. res. 1e-11 from the reference's 3015 to 3501)
+    const bool s16 = o16 && stn16Pass;
     auto stencilPass = [&]() {
         const int g = gridFor(D.nStn, 256, smCount * 16);
-        if (o16)
+        if (s16)
             launch(dev::k_stn<SM_, __half, float>, g, 256, 0, stream, D.view, D.stnNodes, D.nStn, D.stn16.as<__half>(), D.stnScale, xin, y, rr, dd,
                    c1, c2, 1.f, 0, ctl);
         else
             launch(dev::k_stn<SM_, float, float>, g, 256, 0, stream, D.view, D.stnNodes, D.nStn, D.stn32.as<float>(), 1.f, xin, y, rr, dd, c1, c2,
                    1.f, 0, ctl);
     };
-    const bool stn = l > 0 && !diff && D.nStn > 0 && (o16 ? D.stn16.p != nullptr : D.stn32.p != nullptr);
+    const bool stn = l > 0 && !diff && D.nStn > 0 && (s16 ? D.stn16.p != nullptr : D.stn32.p != nullptr);
     if (stn && !D.useTiles) {
         stencilPass();
         return;
@@ -2719,8 +2725,9 @@ void SolverImpl::startIterations() {
     const bool own16 = o.precision == PS_PREC_MIXED && M->mixedOwn16;
     pend.mixed = mixed;
     pend.half = half;
+    stn16Pass = mixed;
     if (!exactOneLevel()) {
-        M->ensureStencils(own16 || (mixed && M->mixedOwn16));
+        M->ensureStencils(mixed && M->mixedOwn16);
         const bool ready = M->actReady.load(std::memory_order_acquire);
         check(cudaStreamWaitEvent(stream, M->readyEv, 0), "wait");
         listsWaited = listsWaited || ready;

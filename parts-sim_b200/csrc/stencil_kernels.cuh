@@ -94,8 +94,11 @@ __device__ __forceinline__ void ldChunk(const __half* p, float (&v)[8]) {
 // One FP32 pass (APPLY / CHEB / RESID, the epilogues of k_list) over the listed nodes of a level
 // with their assembled stencils: ST = float, or __half times the level's power-of-two scale ss.
 // V = __half: the FP16 coarse-level vectors (rho and c2 as in k_list). Nodes off the list are not
-// written.
-template <int MODE, class ST, class V = float>
+// written. A thread may carry NPT nodes (list entries g, g + T, ... for T threads in the grid)
+// through the same unrolled sweep so that their loads overlap; measured on the B200, two nodes a
+// thread (80-90 registers, half the resident warps) made the gyroid and SIMP solves 10-14 %
+// slower than one, which the passes use.
+template <int MODE, class ST, class V = float, int NPT = 1>
 __global__ void __launch_bounds__(256) k_stn(LevelView L, const int* __restrict__ list, int count, const ST* __restrict__ stn, float ss,
                                              const V* __restrict__ x, V* __restrict__ y, const V* __restrict__ r, V* __restrict__ d, float c1,
                                              float c2, float rho, int raw, Ctl ctl) {
@@ -103,49 +106,74 @@ __global__ void __launch_bounds__(256) k_stn(LevelView L, const int* __restrict_
     constexpr bool H = !std::is_same<V, float>::value;
     constexpr int CW = std::is_same<ST, float>::value ? 4 : 8;
     const long long NX = L.PX, NXY = (long long)L.PX * L.NY;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count; t += (long long)gridDim.x * blockDim.x) {
-        const long long n = list[t];
-        const uint8_t mask = __ldg(L.nmask + n);
-        int i, j, k;
-        nodeCoords(L, n, i, j, k);
-        float a[3] = {0.f, 0.f, 0.f};
-        float cf[CW];
+    const long long T = (long long)gridDim.x * blockDim.x;
+    for (long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; t0 < count; t0 += NPT * T) {
+        long long n[NPT], t[NPT];
+        bool live[NPT];
+        int ii[NPT], jj[NPT], kk[NPT];
+        uint8_t mask[NPT];
+#pragma unroll
+        for (int u = 0; u < NPT; u++) {
+            t[u] = t0 + u * T;
+            live[u] = t[u] < count;
+            if (!live[u]) t[u] = t0;  // a repeat of the first node, computed and not stored
+            n[u] = list[t[u]];
+            mask[u] = __ldg(L.nmask + n[u]);
+            nodeCoords(L, n[u], ii[u], jj[u], kk[u]);
+        }
+        float a[NPT][3];
+        float cf[NPT][CW];
+#pragma unroll
+        for (int u = 0; u < NPT; u++) a[u][0] = a[u][1] = a[u][2] = 0.f;
         int have = -1;  // the chunk in cf (known at compile time once the loops are unrolled)
 #pragma unroll
         for (int m = 0; m < 27; m++) {
             const int ox = m % 3 - 1, oy = (m / 3) % 3 - 1, oz = m / 9 - 1;
-            // no voxel couples the node to a neighbour outside the grid: its values read as 0
-            const bool in = i + ox >= 0 && j + oy >= 0 && k + oz >= 0 && i + ox < L.NX && j + oy < L.NY && k + oz < L.NZ;
-            const V* xp = x + 3 * (n + ox + oy * NX + oz * NXY);
-            const float xm[3] = {in ? ldv<float>(xp) : 0.f, in ? ldv<float>(xp + 1) : 0.f, in ? ldv<float>(xp + 2) : 0.f};
+            float xm[NPT][3];
+#pragma unroll
+            for (int u = 0; u < NPT; u++) {
+                // no voxel couples the node to a neighbour outside the grid: its values read as 0
+                const bool in = ii[u] + ox >= 0 && jj[u] + oy >= 0 && kk[u] + oz >= 0 && ii[u] + ox < L.NX && jj[u] + oy < L.NY &&
+                                kk[u] + oz < L.NZ;
+                const V* xp = x + 3 * (n[u] + ox + oy * NX + oz * NXY);
+                xm[u][0] = in ? ldv<float>(xp) : 0.f;
+                xm[u][1] = in ? ldv<float>(xp + 1) : 0.f;
+                xm[u][2] = in ? ldv<float>(xp + 2) : 0.f;
+            }
 #pragma unroll
             for (int e = 0; e < 9; e++) {
                 const int c = 9 * m + e;
                 if (c / CW != have) {
                     have = c / CW;
-                    ldChunk(stn + ((long long)have * count + t) * CW, cf);
+#pragma unroll
+                    for (int u = 0; u < NPT; u++) ldChunk(stn + ((long long)have * count + t[u]) * CW, cf[u]);
                 }
-                a[e / 3] += cf[c % CW] * xm[e % 3];
+#pragma unroll
+                for (int u = 0; u < NPT; u++) a[u][e / 3] += cf[u][c % CW] * xm[u][e % 3];
             }
         }
         const float sc = (std::is_same<ST, float>::value ? 1.f : ss) * (H ? rho : 1.f);
-        const float acc[3] = {a[0] * sc, a[1] * sc, a[2] * sc};
 #pragma unroll
-        for (int q = 0; q < 3; q++) {
-            const long long id = 3 * n + q;
-            const bool fx = fixedDof(mask, q);
-            if (MODE == TOP_APPLY) {
-                stv(y + id, (!raw && fx) ? 0.f : acc[q]);
-            } else if (MODE == TOP_RESID) {
-                stv(y + id, fx ? 0.f : ldf(r + id) - acc[q]);
-            } else {
-                if (fx) {
-                    stv(d + id, 0.f);
-                    stv(y + id, 0.f);
+        for (int u = 0; u < NPT; u++) {
+            if (!live[u]) continue;
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                const float acc = a[u][q] * sc;
+                const long long id = 3 * n[u] + q;
+                const bool fx = fixedDof(mask[u], q);
+                if (MODE == TOP_APPLY) {
+                    stv(y + id, (!raw && fx) ? 0.f : acc);
+                } else if (MODE == TOP_RESID) {
+                    stv(y + id, fx ? 0.f : ldf(r + id) - acc);
                 } else {
-                    const float dn = c1 * ldf(d + id) + c2 * L.invD[id] * (ldf(r + id) - acc[q]);
-                    stv(d + id, dn);
-                    stv(y + id, ldf(x + id) + dn);
+                    if (fx) {
+                        stv(d + id, 0.f);
+                        stv(y + id, 0.f);
+                    } else {
+                        const float dn = c1 * ldf(d + id) + c2 * L.invD[id] * (ldf(r + id) - acc);
+                        stv(d + id, dn);
+                        stv(y + id, ldf(x + id) + dn);
+                    }
                 }
             }
         }
