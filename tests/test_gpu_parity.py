@@ -246,6 +246,38 @@ def test_split_boundary_nodes_in_the_smoother(monkeypatch, precision):
     assert rel(rb.u, ra.u) < 1e-5
 
 
+@pytest.mark.parametrize("model,precision", [("gyroid", "fp64"), ("gyroid", "fp32"), ("simp", "fp64"), ("simp", "fp32"),
+                                             ("lbracket", "mixed")])
+def test_assembled_stencils_on_every_galerkin_level(monkeypatch, model, precision):
+    """The assembled stencils of the Galerkin levels (FP32 in the FP64-Krylov forms, FP16 in the
+    FP32-Krylov ones), forced onto every level >= 1 whatever its size and on both the untiled levels
+    (every active node) and a split tiled level (its boundary nodes), against the per-voxel gather
+    (PSFEA_STENCIL_LEVELS=0): the same solution to the solve tolerance, iteration counts within 15 %,
+    and a true FP64 residual by the oracle's operator."""
+    m = {"gyroid": lambda: W.gyroid(64, 64, 32), "simp": lambda: W.simp(32, 16, 16, nrhs=1),
+         "lbracket": lambda: W.l_bracket(128, 64, 64, holes=16, seed=3)}[model]()
+    f = m.f if m.f.ndim == 1 else m.f[0]
+    monkeypatch.setenv("PSFEA_TILE_MIN_NODES", "20000")  # level 1 of the L-bracket tiled (and split)
+    monkeypatch.setenv("PSFEA_STENCIL_LEVELS", "0")
+    A = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    monkeypatch.setenv("PSFEA_STENCIL_LEVELS", "-1")
+    monkeypatch.setenv("PSFEA_STENCIL_MIN_NODES", "1")
+    B = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    ra = A.solve(f, tol=1e-8, max_iter=3000, precision=precision)
+    rb = B.solve(f, tol=1e-8, max_iter=3000, precision=precision)
+    assert ra.converged and rb.converged, (ra.iterations, rb.iterations)
+    assert abs(ra.iterations - rb.iterations) <= max(2, 0.15 * ra.iterations), (ra.iterations, rb.iterations)
+    P = oracle.OracleModel("port", m.dims, m.density, m.nu, m.bc, m.coarsest_max_dof)
+    fixed = P.fixed(0).astype(bool)
+    res = f - P.apply(rb.u)
+    res[fixed] = 0
+    assert np.linalg.norm(res) / np.linalg.norm(np.where(fixed, 0, f)) <= 1e-7
+    assert rel(rb.u, ra.u) < 1e-5
+    # the stencils are made once per model and form: a second solve repeats the first bitwise
+    rc = B.solve(f, tol=1e-8, max_iter=3000, precision=precision)
+    assert rc.iterations == rb.iterations and np.array_equal(rc.u, rb.u)
+
+
 def test_solve_into_a_pinned_caller_buffer():
     """solve(out=...) writes u into the caller's array (here pinned host memory) and returns it:
     bitwise the same as a solve into a new array; a buffer of the wrong type is refused."""
