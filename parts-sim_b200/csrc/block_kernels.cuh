@@ -226,46 +226,97 @@ __device__ __forceinline__ void applyNbr(const LevelView& L, const Coefs<T>& C, 
 //   BOP_DOT    y = K x (held 0) and each right-hand side's CG step alpha = rz / (x . y); x . y <= 0
 //              ends that right-hand side as a breakdown (voxel_fea.cpp:902-905)
 // The product is the single-vector one (applyAt, voxel_fea.cpp:422-486) with the block's stride.
-template <class T, int MODE, bool OWN16, int RB>
+// The block path's assembled stencils are node-major: node t's 243 coefficients (c = 9 m + 3 p + q,
+// m the neighbour (ox + 1) + 3 (oy + 1) + 9 (oz + 1)) contiguous at t * STN_ROW, padded to 244 so
+// that a row is a whole number of 16-byte pieces. A warp copies its nodes' rows into shared memory
+// with 16-byte loads (512 contiguous bytes per instruction) and every lane of a node then reads them
+// as broadcasts: 243 multiply-adds per node and right-hand side against up to 576 for the
+// per-voxel gather, the coefficients read from HBM once per node for the whole block.
+constexpr int STN_ROW = 244;
+template <class T>
+__host__ __device__ constexpr size_t stnBlockSmem(int npw) { return size_t(BLOCK_THREADS / 32) * npw * STN_ROW * sizeof(T); }
+
+template <class T, int S>
+__device__ __forceinline__ void stnBlock(const LevelView& L, const T* __restrict__ row, const T* __restrict__ x, long long n, int i, int j,
+                                         int k, T acc[3]) {
+    const long long NX = L.PX, NXY = (long long)L.PX * L.NY;
+    T a0 = T(0), a1 = T(0), a2 = T(0);
+#pragma unroll
+    for (int m = 0; m < 27; m++) {
+        const int ox = m % 3 - 1, oy = (m / 3) % 3 - 1, oz = m / 9 - 1;
+        const bool in = i + ox >= 0 && j + oy >= 0 && k + oz >= 0 && i + ox < L.NX && j + oy < L.NY && k + oz < L.NZ;
+        const T* xp = x + 3 * S * (n + ox + oy * NX + oz * NXY);
+        const T x0 = in ? __ldg(xp) : T(0), x1 = in ? __ldg(xp + S) : T(0), x2 = in ? __ldg(xp + 2 * S) : T(0);
+        const T* b = row + 9 * m;
+        a0 += b[0] * x0 + b[1] * x1 + b[2] * x2;
+        a1 += b[3] * x0 + b[4] * x1 + b[5] * x2;
+        a2 += b[6] * x0 + b[7] * x1 + b[8] * x2;
+    }
+    acc[0] = a0;
+    acc[1] = a1;
+    acc[2] = a2;
+}
+
+// STN: the product from the level's assembled stencils (stn, over act) instead of the gather.
+template <class T, int MODE, bool OWN16, int RB, bool STN = false>
 __global__ void __launch_bounds__(BLOCK_THREADS, 2) kb_op(LevelView L, Coefs<T> C, const int* __restrict__ act, int nAct,
-                                                       const T* __restrict__ x, T* __restrict__ y, const float* __restrict__ r,
-                                                       float* __restrict__ d, float c1, float c2, int raw, BlockState* bs, double* partials,
-                                                       unsigned* ticket, Ctl ctl) {
+                                                       const T* __restrict__ stn, const T* __restrict__ x, T* __restrict__ y,
+                                                       const float* __restrict__ r, float* __restrict__ d, float c1, float c2, int raw,
+                                                       BlockState* bs, double* partials, unsigned* ticket, Ctl ctl) {
     if (skipped(ctl)) return;
     constexpr int NPW = 32 / RB;
     const int lane = threadIdx.x & 31, q = lane % RB, sub = lane / RB;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    extern __shared__ __align__(16) unsigned char kbRaw[];
+    T* rows = reinterpret_cast<T*>(kbRaw) + (threadIdx.x >> 5) * NPW * STN_ROW;  // this warp's NPW stencil rows
     double dot[1] = {0.0};
-    for (long long t = warp * NPW + sub; t < nAct; t += nw * NPW) {
-        const long long n = act[t];
-        const uint8_t mask = __ldg(L.nmask + n);
-        int i, j, k;
-        nodeCoords(L, n, i, j, k);
-        T acc[3];
-        applyNbr<T, OWN16, RB>(L, C, x + q, i, j, k, n, mask, acc);
+    // warp-uniform sweep (the stencil rows are shared within the warp); lanes past the list idle
+    for (long long tb = warp * NPW; tb < nAct; tb += nw * NPW) {
+        const long long t = tb + sub;
+        if constexpr (STN) {
+            constexpr int VP = 16 / int(sizeof(T)), PIECES = STN_ROW / VP;  // 16-byte pieces of a row
+            for (int e = lane; e < NPW * PIECES; e += 32) {
+                const int u = e / PIECES, g = e - u * PIECES;
+                if (tb + u < nAct) {
+                    const uint4 v = __ldcs(reinterpret_cast<const uint4*>(stn + (tb + u) * STN_ROW) + g);
+                    reinterpret_cast<uint4*>(rows + u * STN_ROW)[g] = v;
+                }
+            }
+            __syncwarp();
+        }
+        if (t < nAct) {
+            const long long n = act[t];
+            const uint8_t mask = __ldg(L.nmask + n);
+            int i, j, k;
+            nodeCoords(L, n, i, j, k);
+            T acc[3];
+            if constexpr (STN) stnBlock<T, RB>(L, rows + sub * STN_ROW, x + q, n, i, j, k, acc);
+            else applyNbr<T, OWN16, RB>(L, C, x + q, i, j, k, n, mask, acc);
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const long long id = (3 * n + c) * RB + q;
-            const bool fx = fixedDof(mask, c);
-            if constexpr (MODE == BOP_APPLY) {
-                y[id] = (!raw && fx) ? T(0) : acc[c];
-            } else if constexpr (MODE == BOP_DOT) {
-                const T yv = fx ? T(0) : acc[c];
-                y[id] = yv;
-                dot[0] += double(x[id]) * double(yv);
-            } else if constexpr (MODE == BOP_RESID) {
-                y[id] = fx ? T(0) : T(r[id]) - acc[c];
-            } else {
-                if (fx) {
-                    d[id] = 0.f;
-                    y[id] = T(0);
+            for (int c = 0; c < 3; c++) {
+                const long long id = (3 * n + c) * RB + q;
+                const bool fx = fixedDof(mask, c);
+                if constexpr (MODE == BOP_APPLY) {
+                    y[id] = (!raw && fx) ? T(0) : acc[c];
+                } else if constexpr (MODE == BOP_DOT) {
+                    const T yv = fx ? T(0) : acc[c];
+                    y[id] = yv;
+                    dot[0] += double(x[id]) * double(yv);
+                } else if constexpr (MODE == BOP_RESID) {
+                    y[id] = fx ? T(0) : T(r[id]) - acc[c];
                 } else {
-                    const float dn = c1 * d[id] + c2 * __ldg(L.invD + 3 * n + c) * (r[id] - float(acc[c]));
-                    d[id] = dn;
-                    y[id] = x[id] + T(dn);
+                    if (fx) {
+                        d[id] = 0.f;
+                        y[id] = T(0);
+                    } else {
+                        const float dn = c1 * d[id] + c2 * __ldg(L.invD + 3 * n + c) * (r[id] - float(acc[c]));
+                        d[id] = dn;
+                        y[id] = x[id] + T(dn);
+                    }
                 }
             }
         }
+        if constexpr (STN) __syncwarp();  // the rows are refilled next
     }
     if constexpr (MODE == BOP_DOT) {
         double tot[1];

@@ -212,6 +212,40 @@ __device__ __forceinline__ void stv(__half* p, float v) { *p = __float2half_rn(v
 __device__ __forceinline__ float ldf(const float* p) { return *p; }
 __device__ __forceinline__ float ldf(const __half* p) { return __half2float(*p); }
 
+// Layout: coefficient c = 9 m + 3 p + q (m the neighbour (ox + 1) + 3 (oy + 1) + 9 (oz + 1), p the
+// row and q the column component) of listed node t sits in chunk c / CW of CW consecutive values
+// (16 bytes: CW = 4 floats or 8 halves), chunks stored chunk-major over the nodes, so that a warp
+// reads one chunk of 32 consecutive nodes as 512 contiguous bytes. The tail of the last chunk is 0.
+template <int CW>
+__host__ __device__ constexpr int stnChunks() { return (243 + CW - 1) / CW; }
+template <int CW>
+__host__ __device__ __forceinline__ long long stnAt(int c, long long t, long long count) { return ((c / CW) * count + t) * CW + c % CW; }
+
+// one 16-byte chunk of coefficients as floats
+__device__ __forceinline__ void ldChunk(const float* p, float (&v)[4]) {
+    const float4 u = __ldcs(reinterpret_cast<const float4*>(p));
+    v[0] = u.x;
+    v[1] = u.y;
+    v[2] = u.z;
+    v[3] = u.w;
+}
+__device__ __forceinline__ void ldChunk(const __half* p, float (&v)[8]) {
+    const uint4 u = __ldcs(reinterpret_cast<const uint4*>(p));
+    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[e]));
+        v[2 * e] = f.x;
+        v[2 * e + 1] = f.y;
+    }
+}
+
+__device__ __forceinline__ void ldChunk(const double* p, double (&v)[2]) {
+    const double2 u = __ldcs(reinterpret_cast<const double2*>(p));
+    v[0] = u.x;
+    v[1] = u.y;
+}
+
 __device__ __forceinline__ void nodeCoords(const LevelView& L, long long n, int& i, int& j, int& k) {
     if (n <= 0xffffffffLL) {  // two 32-bit divisions: a 64-bit one is a long software sequence
         const unsigned u = unsigned(n), px = unsigned(L.PX), ny = unsigned(L.NY);

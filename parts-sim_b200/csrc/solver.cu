@@ -1543,6 +1543,7 @@ struct SharedModel {
 
     ~SharedModel() {
         for (auto& a : act) a.release();
+        for (auto& b : bstn32) b.release();
         btTiles.release();
         for (auto& D : L) D.release();
         cDof.release();
@@ -1572,6 +1573,11 @@ struct SharedModel {
     // the assembled stencils of the levels in stencilLevels (FP16 copies too when half); the
     // callers' streams wait on readyEv
     void ensureStencils(bool half);
+    // the block path's stencils: FP32 over the active nodes of every level below the finest
+    // (PSFEA_BLOCK_STENCIL=0: none, the per-voxel gather)
+    void ensureBlockStencils();
+    std::vector<DevMem> bstn32;
+    bool blockStencils = true;
     int64_t stencilLevels = ~int64_t(1);  // PSFEA_STENCIL_LEVELS: bit l = level l (never level 0)
     int64_t stencilMinNodes = 65536;      // PSFEA_STENCIL_MIN_NODES: smaller node lists keep the gather
     bool foldBranch = true;               // PSFEA_FOLD_BRANCH: the FP32-Krylov fold as a conditional graph branch
@@ -1597,6 +1603,7 @@ void SharedModel::adopt(Hierarchy&& h) {
     if (const char* e = std::getenv("PSFEA_STENCIL_LEVELS")) stencilLevels = std::atoll(e) & ~int64_t(1);
     if (const char* e = std::getenv("PSFEA_STENCIL_MIN_NODES")) stencilMinNodes = std::atoll(e);
     if (const char* e = std::getenv("PSFEA_FOLD_BRANCH")) foldBranch = std::atoi(e) != 0;
+    if (const char* e = std::getenv("PSFEA_BLOCK_STENCIL")) blockStencils = std::atoi(e) != 0;
     if (const char* e = std::getenv("PSFEA_EBE_SPLIT")) ebeSplit = std::atoi(e) == 1 ? 1 : 3;
     check(cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking), "stream");
     check(cudaEventCreateWithFlags(&readyEv, cudaEventDisableTiming), "event");
@@ -1851,7 +1858,7 @@ void SharedModel::ensureStencils(bool half) {
         const int grid = gridFor(int64_t(cnt) * 27, 256, smCount * 32);
         if (!half && !D.stn32.p) {
             D.stn32.alloc(size_t(cnt) * dev::stnChunks<4>() * 4 * sizeof(float), bytes, ms);
-            dev::k_stn_build<float><<<grid, 256, 0, ms>>>(D.view, D.c32, D.stnNodes, cnt, D.stn32.as<float>(), 1.f);
+            dev::k_stn_build<float, float><<<grid, 256, 0, ms>>>(D.view, D.c32, D.stnNodes, cnt, D.stn32.as<float>(), 1.f);
             check(cudaGetLastError(), "stencil build");
             built = true;
         }
@@ -1871,12 +1878,35 @@ void SharedModel::ensureStencils(bool half) {
             const double bound = 8.0 * std::max(emax, smax * kb) + dmax;
             D.stnScale = bound > 0 ? float(std::exp2(std::ceil(std::log2(bound / 16384.0)))) : 1.f;
             D.stn16.alloc(size_t(cnt) * dev::stnChunks<8>() * 8 * sizeof(__half), bytes, ms);
-            dev::k_stn_build<__half><<<grid, 256, 0, ms>>>(D.view, D.c32, D.stnNodes, cnt, D.stn16.as<__half>(), 1.f / D.stnScale);
+            dev::k_stn_build<__half, float><<<grid, 256, 0, ms>>>(D.view, D.c32, D.stnNodes, cnt, D.stn16.as<__half>(), 1.f / D.stnScale);
             check(cudaGetLastError(), "stencil build");
             built = true;
         }
     }
     if (built) check(cudaEventRecord(readyEv, ms), "event");
+}
+
+void SharedModel::ensureBlockStencils() {
+    if (!blockStencils) return;
+    std::lock_guard<std::mutex> g(listMu);
+    if (!bstn32.empty()) return;
+    bstn32.resize(L.size());
+    for (size_t l = 0; l < L.size(); l++) {
+        DevLevel& D = L[l];
+        const int cnt = nAct[l];
+        if (!cnt) continue;
+        const int grid = gridFor(int64_t(cnt) * 27, 256, smCount * 32);
+        if (l > 0) {
+            // (the finest level keeps the gather, in FP32 and in FP64: its uniform element matrix is
+            // a kernel operand, and its constant-operand multiply-adds issue as fast as the
+            // stencil's shared-memory loads and multiply-adds together; measured on the SIMP block
+            // solve, stencils there were 20 % slower in FP32 and no faster in FP64)
+            bstn32[l].alloc(size_t(cnt) * dev::STN_ROW * sizeof(float), bytes, ms);
+            dev::k_stn_build<float, float, true><<<grid, 256, 0, ms>>>(D.view, D.c32, act[l].as<int>(), cnt, bstn32[l].as<float>(), 1.f);
+            check(cudaGetLastError(), "block stencil build");
+        }
+    }
+    check(cudaEventRecord(readyEv, ms), "event");
 }
 
 void SharedModel::ensureActiveLists() {
@@ -2949,6 +2979,16 @@ struct BlockImpl final : BlockBase {
 
     BlockImpl(std::shared_ptr<SharedModel> model) : M(std::move(model)), H(M->H), L(M->L), smCount(M->smCount) {
         M->ensureActiveLists();
+        M->ensureBlockStencils();
+        static std::once_flag attrOnce;
+        std::call_once(attrOnce, [] {
+            // the stencil rows a CTA's warps stage (31 KB for an 8-wide block)
+            auto set = [](auto kernel, size_t b) {
+                check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b)), "attr");
+            };
+            set(dev::kb_op<float, dev::BOP_CHEB, false, RB, true>, dev::stnBlockSmem<float>(32 / RB));
+            set(dev::kb_op<float, dev::BOP_RESID, false, RB, true>, dev::stnBlockSmem<float>(32 / RB));
+        });
         check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
         check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
         check(cudaMallocHost(&hostState, sizeof(dev::BlockState)), "cudaMallocHost");
@@ -3026,12 +3066,18 @@ struct BlockImpl final : BlockBase {
             if constexpr (sizeof(T) == 8) return D.c64;
             else return D.c32;
         }();
-        if (own16 && D.hasOwn)
-            launch(dev::kb_op<T, MODE, true, RB>, laneGrid(l), dev::BLOCK_THREADS, 0, D.view, C, act(l), nAct(l), xin, y, rr, dd, c1, c2,
-                   raw ? 1 : 0, bs(), part(), tick(), ctl);
+        // the assembled stencils of the Galerkin levels
+        const T* stn = nullptr;
+        if constexpr (sizeof(T) == 4) stn = (M->bstn32.empty() || l == 0) ? nullptr : M->bstn32[size_t(l)].template as<float>();
+        if (stn)
+            launch(dev::kb_op<T, MODE, false, RB, true>, laneGrid(l), dev::BLOCK_THREADS, dev::stnBlockSmem<T>(32 / RB), D.view, C, act(l), nAct(l),
+                   stn, xin, y, rr, dd, c1, c2, raw ? 1 : 0, bs(), part(), tick(), ctl);
+        else if (own16 && D.hasOwn)
+            launch(dev::kb_op<T, MODE, true, RB>, laneGrid(l), dev::BLOCK_THREADS, 0, D.view, C, act(l), nAct(l), static_cast<const T*>(nullptr),
+                   xin, y, rr, dd, c1, c2, raw ? 1 : 0, bs(), part(), tick(), ctl);
         else
-            launch(dev::kb_op<T, MODE, false, RB>, laneGrid(l), dev::BLOCK_THREADS, 0, D.view, C, act(l), nAct(l), xin, y, rr, dd, c1, c2,
-                   raw ? 1 : 0, bs(), part(), tick(), ctl);
+            launch(dev::kb_op<T, MODE, false, RB>, laneGrid(l), dev::BLOCK_THREADS, 0, D.view, C, act(l), nAct(l), static_cast<const T*>(nullptr),
+                   xin, y, rr, dd, c1, c2, raw ? 1 : 0, bs(), part(), tick(), ctl);
     }
 
     void coarse(const float* rin, float* zout, dev::Ctl ctl) {

@@ -19,24 +19,18 @@
 namespace psfea {
 namespace dev {
 
-// Layout: coefficient c = 9 m + 3 p + q (m the neighbour (ox + 1) + 3 (oy + 1) + 9 (oz + 1), p the
-// row and q the column component) of listed node t sits in chunk c / CW of CW consecutive values
-// (16 bytes: CW = 4 floats or 8 halves), chunks stored chunk-major over the nodes, so that a warp
-// reads one chunk of 32 consecutive nodes as 512 contiguous bytes. The tail of the last chunk is 0.
-template <int CW>
-__host__ __device__ constexpr int stnChunks() { return (243 + CW - 1) / CW; }
-template <int CW>
-__host__ __device__ __forceinline__ long long stnAt(int c, long long t, long long count) { return ((c / CW) * count + t) * CW + c % CW; }
-
 __device__ __forceinline__ void stStn(float* p, float v, float) { *p = v; }
+__device__ __forceinline__ void stStn(double* p, double v, float) { *p = v; }
 __device__ __forceinline__ void stStn(__half* p, float v, float inv) { *p = __float2half_rn(v * inv); }
 
 // one thread per (listed node, neighbour o): block (n, n + o), rows of n's corner and columns of the
 // neighbour's corner in each voxel holding both (s Kb for a uniformly scaled voxel, its own matrix
-// otherwise); the diagonal shift joins the centre block. FP32 sums, stored as floats (4-value
-// chunks) or as halves times inv (8-value chunks).
-template <class ST>
-__global__ void k_stn_build(LevelView L, Coefs<float> C, const int* __restrict__ list, int count, ST* __restrict__ stn, float inv) {
+// otherwise); the diagonal shift joins the centre block. Sums in CT (FP32, or FP64 for the block
+// path's FP64 product), stored as floats (4-value chunks), doubles (2-value chunks) or halves
+// times inv (8-value chunks).
+// NODE_MAJOR: the block path's layout instead (row t at t * STN_ROW, block_kernels.cuh).
+template <class ST, class CT = float, bool NODE_MAJOR = false>
+__global__ void k_stn_build(LevelView L, Coefs<CT> C, const int* __restrict__ list, int count, ST* __restrict__ stn, float inv) {
     constexpr int CW = 16 / int(sizeof(ST));
     const long long total = (long long)count * 27;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
@@ -45,7 +39,7 @@ __global__ void k_stn_build(LevelView L, Coefs<float> C, const int* __restrict__
         int i, j, k;
         nodeCoords(L, n, i, j, k);
         const int ox = m % 3 - 1, oy = (m / 3) % 3 - 1, oz = m / 9 - 1;
-        float blk[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        CT blk[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int v = 0; v < 8; v++) {
             const int di = v & 1, dj = (v >> 1) & 1, dk = v >> 2;
             // the voxel at offset (di - 1, dj - 1, dk - 1) holds the neighbour when o - d + 1 is 0 or 1 per axis
@@ -57,37 +51,19 @@ __global__ void k_stn_build(LevelView L, Coefs<float> C, const int* __restrict__
             if (!w) continue;
             const int a = cornerOf(1 - di, 1 - dj, 1 - dk), b = cornerOf(bx, by, bz);
             if (!(w & OWN_BIT)) {
-                const float s = __uint_as_float(w);
+                const CT s = CT(__uint_as_float(w));
                 for (int p = 0; p < 3; p++)
                     for (int q = 0; q < 3; q++) blk[3 * p + q] += s * C.Kb[(3 * a + p) * 24 + 3 * b + q];
             } else {
                 const float* M = L.own + (long long)(w & ~OWN_BIT) * 576;
                 for (int p = 0; p < 3; p++)
-                    for (int q = 0; q < 3; q++) blk[3 * p + q] += M[(3 * a + p) * 24 + 3 * b + q];
+                    for (int q = 0; q < 3; q++) blk[3 * p + q] += CT(M[(3 * a + p) * 24 + 3 * b + q]);
             }
         }
         if (m == 13 && L.dadd32)
-            for (int p = 0; p < 3; p++) blk[4 * p] += L.dadd32[3 * n + p];
-        for (int c = 0; c < 9; c++) stStn(stn + stnAt<CW>(9 * m + c, t, count), blk[c], inv);
-    }
-}
-
-// one 16-byte chunk of coefficients as floats
-__device__ __forceinline__ void ldChunk(const float* p, float (&v)[4]) {
-    const float4 u = __ldcs(reinterpret_cast<const float4*>(p));
-    v[0] = u.x;
-    v[1] = u.y;
-    v[2] = u.z;
-    v[3] = u.w;
-}
-__device__ __forceinline__ void ldChunk(const __half* p, float (&v)[8]) {
-    const uint4 u = __ldcs(reinterpret_cast<const uint4*>(p));
-    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[e]));
-        v[2 * e] = f.x;
-        v[2 * e + 1] = f.y;
+            for (int p = 0; p < 3; p++) blk[4 * p] += sizeof(CT) == 8 ? CT(L.dadd[3 * n + p]) : CT(L.dadd32[3 * n + p]);
+        for (int c = 0; c < 9; c++)
+            stStn(stn + (NODE_MAJOR ? (long long)t * STN_ROW + 9 * m + c : stnAt<CW>(9 * m + c, t, count)), blk[c], inv);
     }
 }
 
