@@ -226,35 +226,55 @@ __device__ __forceinline__ void applyNbr(const LevelView& L, const Coefs<T>& C, 
 //   BOP_DOT    y = K x (held 0) and each right-hand side's CG step alpha = rz / (x . y); x . y <= 0
 //              ends that right-hand side as a breakdown (voxel_fea.cpp:902-905)
 // The product is the single-vector one (applyAt, voxel_fea.cpp:422-486) with the block's stride.
-// The block path's assembled stencils are node-major: node t's 243 coefficients (c = 9 m + 3 p + q,
-// m the neighbour (ox + 1) + 3 (oy + 1) + 9 (oz + 1)) contiguous at t * STN_ROW, padded to 244 so
-// that a row is a whole number of 16-byte pieces. A warp copies its nodes' rows into shared memory
-// with 16-byte loads (512 contiguous bytes per instruction) and every lane of a node then reads them
-// as broadcasts: 243 multiply-adds per node and right-hand side against up to 576 for the
-// per-voxel gather, the coefficients read from HBM once per node for the whole block.
-constexpr int STN_ROW = 244;
+// The block path's assembled stencils are node-major: node t's row at t * STN_ROW holds its 27 3x3
+// blocks with the neighbours taken in pairs (m, m + 1) = (2 P, 2 P + 1), P = 0..13 (m = (ox + 1) +
+// 3 (oy + 1) + 9 (oz + 1); the 28th slot is 0): entry (p, q) of the pair's two blocks side by side
+// at 18 P + 2 (3 p + q) + (m & 1). A warp copies its nodes' rows into shared memory with 16-byte
+// loads (512 contiguous bytes per instruction) and every lane of a node reads them as broadcasts;
+// one paired FMA then advances both neighbours of a pair: 126 paired FMAs per node and right-hand
+// side where the per-voxel gather takes 288 (576 multiply-adds), the coefficients read from HBM
+// once per node for the whole block.
+constexpr int STN_ROW = 252;
+__host__ __device__ constexpr int stnPairAt(int m, int p, int q) { return 18 * (m >> 1) + 2 * (3 * p + q) + (m & 1); }
 template <class T>
 __host__ __device__ constexpr size_t stnBlockSmem(int npw) { return size_t(BLOCK_THREADS / 32) * npw * STN_ROW * sizeof(T); }
 
 template <class T, int S>
 __device__ __forceinline__ void stnBlock(const LevelView& L, const T* __restrict__ row, const T* __restrict__ x, long long n, int i, int j,
                                          int k, T acc[3]) {
+    static_assert(sizeof(T) == 4, "the paired layout is FP32");
     const long long NX = L.PX, NXY = (long long)L.PX * L.NY;
-    T a0 = T(0), a1 = T(0), a2 = T(0);
-#pragma unroll
-    for (int m = 0; m < 27; m++) {
+    auto xOf = [&](int m, float (&v)[3]) {
         const int ox = m % 3 - 1, oy = (m / 3) % 3 - 1, oz = m / 9 - 1;
-        const bool in = i + ox >= 0 && j + oy >= 0 && k + oz >= 0 && i + ox < L.NX && j + oy < L.NY && k + oz < L.NZ;
+        const bool in = m < 27 && i + ox >= 0 && j + oy >= 0 && k + oz >= 0 && i + ox < L.NX && j + oy < L.NY && k + oz < L.NZ;
         const T* xp = x + 3 * S * (n + ox + oy * NX + oz * NXY);
-        const T x0 = in ? __ldg(xp) : T(0), x1 = in ? __ldg(xp + S) : T(0), x2 = in ? __ldg(xp + 2 * S) : T(0);
-        const T* b = row + 9 * m;
-        a0 += b[0] * x0 + b[1] * x1 + b[2] * x2;
-        a1 += b[3] * x0 + b[4] * x1 + b[5] * x2;
-        a2 += b[6] * x0 + b[7] * x1 + b[8] * x2;
+        v[0] = in ? __ldg(xp) : 0.f;
+        v[1] = in ? __ldg(xp + S) : 0.f;
+        v[2] = in ? __ldg(xp + 2 * S) : 0.f;
+    };
+    const float4* R = reinterpret_cast<const float4*>(row);
+    float2 a2[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    float4 cf = make_float4(0.f, 0.f, 0.f, 0.f);
+    int have = -1;
+#pragma unroll
+    for (int P = 0; P < 14; P++) {
+        float u[3], w[3];
+        xOf(2 * P, u);
+        xOf(2 * P + 1, w);
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+            const int f = 18 * P + 2 * e;  // the pair's entry (p, q) = (e / 3, e % 3): floats f, f + 1
+            if (f / 4 != have) {
+                have = f / 4;
+                cf = R[have];
+            }
+            const float2 b = (f % 4 == 0) ? make_float2(cf.x, cf.y) : make_float2(cf.z, cf.w);
+            a2[e / 3] = __ffma2_rn(b, make_float2(u[e % 3], w[e % 3]), a2[e / 3]);
+        }
     }
-    acc[0] = a0;
-    acc[1] = a1;
-    acc[2] = a2;
+    acc[0] = a2[0].x + a2[0].y;
+    acc[1] = a2[1].x + a2[1].y;
+    acc[2] = a2[2].x + a2[2].y;
 }
 
 // STN: the product from the level's assembled stencils (stn, over act) instead of the gather.

@@ -1578,6 +1578,10 @@ struct SharedModel {
     void ensureBlockStencils();
     std::vector<DevMem> bstn32;
     bool blockStencils = true;
+    // PSFEA_BLOCK_STENCIL0=1: stencils on the finest level too. Off: its uniform element matrix is a
+    // kernel operand, and measured on the SIMP block solve its stencils were 16-20 % slower (paired
+    // or not) than the constant-operand gather
+    bool blockStencil0 = false;
     int64_t stencilLevels = ~int64_t(1);  // PSFEA_STENCIL_LEVELS: bit l = level l (never level 0)
     int64_t stencilMinNodes = 65536;      // PSFEA_STENCIL_MIN_NODES: smaller node lists keep the gather
     bool foldBranch = true;               // PSFEA_FOLD_BRANCH: the FP32-Krylov fold as a conditional graph branch
@@ -1604,6 +1608,7 @@ void SharedModel::adopt(Hierarchy&& h) {
     if (const char* e = std::getenv("PSFEA_STENCIL_MIN_NODES")) stencilMinNodes = std::atoll(e);
     if (const char* e = std::getenv("PSFEA_FOLD_BRANCH")) foldBranch = std::atoi(e) != 0;
     if (const char* e = std::getenv("PSFEA_BLOCK_STENCIL")) blockStencils = std::atoi(e) != 0;
+    if (const char* e = std::getenv("PSFEA_BLOCK_STENCIL0")) blockStencil0 = std::atoi(e) != 0;
     if (const char* e = std::getenv("PSFEA_EBE_SPLIT")) ebeSplit = std::atoi(e) == 1 ? 1 : 3;
     check(cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking), "stream");
     check(cudaEventCreateWithFlags(&readyEv, cudaEventDisableTiming), "event");
@@ -1896,11 +1901,7 @@ void SharedModel::ensureBlockStencils() {
         const int cnt = nAct[l];
         if (!cnt) continue;
         const int grid = gridFor(int64_t(cnt) * 27, 256, smCount * 32);
-        if (l > 0) {
-            // (the finest level keeps the gather, in FP32 and in FP64: its uniform element matrix is
-            // a kernel operand, and its constant-operand multiply-adds issue as fast as the
-            // stencil's shared-memory loads and multiply-adds together; measured on the SIMP block
-            // solve, stencils there were 20 % slower in FP32 and no faster in FP64)
+        if (l > 0 || blockStencil0) {
             bstn32[l].alloc(size_t(cnt) * dev::STN_ROW * sizeof(float), bytes, ms);
             dev::k_stn_build<float, float, true><<<grid, 256, 0, ms>>>(D.view, D.c32, act[l].as<int>(), cnt, bstn32[l].as<float>(), 1.f);
             check(cudaGetLastError(), "block stencil build");
@@ -3067,12 +3068,15 @@ struct BlockImpl final : BlockBase {
             else return D.c32;
         }();
         // the assembled stencils of the Galerkin levels
-        const T* stn = nullptr;
-        if constexpr (sizeof(T) == 4) stn = (M->bstn32.empty() || l == 0) ? nullptr : M->bstn32[size_t(l)].template as<float>();
-        if (stn)
-            launch(dev::kb_op<T, MODE, false, RB, true>, laneGrid(l), dev::BLOCK_THREADS, dev::stnBlockSmem<T>(32 / RB), D.view, C, act(l), nAct(l),
-                   stn, xin, y, rr, dd, c1, c2, raw ? 1 : 0, bs(), part(), tick(), ctl);
-        else if (own16 && D.hasOwn)
+        if constexpr (sizeof(T) == 4) {
+            const float* stn = M->bstn32.empty() ? nullptr : M->bstn32[size_t(l)].template as<float>();
+            if (stn) {
+                launch(dev::kb_op<float, MODE, false, RB, true>, laneGrid(l), dev::BLOCK_THREADS, dev::stnBlockSmem<float>(32 / RB), D.view, C,
+                       act(l), nAct(l), stn, xin, y, rr, dd, c1, c2, raw ? 1 : 0, bs(), part(), tick(), ctl);
+                return;
+            }
+        }
+        if (own16 && D.hasOwn)
             launch(dev::kb_op<T, MODE, true, RB>, laneGrid(l), dev::BLOCK_THREADS, 0, D.view, C, act(l), nAct(l), static_cast<const T*>(nullptr),
                    xin, y, rr, dd, c1, c2, raw ? 1 : 0, bs(), part(), tick(), ctl);
         else

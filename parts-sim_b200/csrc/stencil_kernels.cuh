@@ -28,7 +28,7 @@ __device__ __forceinline__ void stStn(__half* p, float v, float inv) { *p = __fl
 // otherwise); the diagonal shift joins the centre block. Sums in CT (FP32, or FP64 for the block
 // path's FP64 product), stored as floats (4-value chunks), doubles (2-value chunks) or halves
 // times inv (8-value chunks).
-// NODE_MAJOR: the block path's layout instead (row t at t * STN_ROW, block_kernels.cuh).
+// NODE_MAJOR: the block path's paired layout instead (row t at t * STN_ROW, block_kernels.cuh).
 template <class ST, class CT = float, bool NODE_MAJOR = false>
 __global__ void k_stn_build(LevelView L, Coefs<CT> C, const int* __restrict__ list, int count, ST* __restrict__ stn, float inv) {
     constexpr int CW = 16 / int(sizeof(ST));
@@ -63,7 +63,7 @@ __global__ void k_stn_build(LevelView L, Coefs<CT> C, const int* __restrict__ li
         if (m == 13 && L.dadd32)
             for (int p = 0; p < 3; p++) blk[4 * p] += sizeof(CT) == 8 ? CT(L.dadd[3 * n + p]) : CT(L.dadd32[3 * n + p]);
         for (int c = 0; c < 9; c++)
-            stStn(stn + (NODE_MAJOR ? (long long)t * STN_ROW + 9 * m + c : stnAt<CW>(9 * m + c, t, count)), blk[c], inv);
+            stStn(stn + (NODE_MAJOR ? (long long)t * STN_ROW + stnPairAt(m, c / 3, c % 3) : stnAt<CW>(9 * m + c, t, count)), blk[c], inv);
     }
 }
 
