@@ -414,10 +414,19 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == 8 ? PSFEA_TILE_CTAS
     }
     if (tileHasR(MODE)) ok = ok && mbarWait(bar + 1, TILE_WAIT_POLLS);
     if (ok) {
-        // epilogue of the column's nodes except the boundary ones
+        // epilogue of the column's nodes except the boundary ones. An inactive node (all its DOFs
+        // held; r, d and x are 0 there) gives y = 0: with r staged in place of the output
+        // (smoother, residual) its slots already hold that, a separate output tile gets zeros
 #pragma unroll
         for (int z = 0; z < TZ; z++) {
             if ((bmask >> z) & 1u) continue;
+            if (!(mk[z] & NM_ACTIVE)) {
+                if (!tileHasR(MODE)) {  // a separate output tile: its slots are zeros
+                    T* yn = ys + (z * TY + cy) * TROW + 3 * cx;
+                    yn[0] = yn[1] = yn[2] = T(0);
+                }
+                continue;
+            }
             T kx[3] = {T(0), T(0), T(0)};
             if (mk[z] & NM_UNIFORM) {
                 const T s = T(__uint_as_float(vs[vOff(cx, cy, z)]));
