@@ -226,6 +226,13 @@ void ps_fea_destroy(ps_fea_t* h);
 typedef struct ps_hierarchy ps_hierarchy_t;
 ps_status ps_hierarchy_create(const int32_t dims[3], const float* density, double nu, const uint8_t* bc,
                               int64_t coarsest_max_dof, const double* diag_add, ps_hierarchy_t** out);
+/* The same hierarchy with the Galerkin coarse matrices (voxel_fea.cpp:268-386, the coarsen step of
+ * the VoxelFEA constructor) computed on the current CUDA device wherever a level's classes of
+ * equal child patterns number at least PSFEA_DEVICE_GALERKIN_MIN (default 4096: graded grids),
+ * bitwise equal to the host build; ps_fea_create builds this way when PSFEA_DEVICE_GALERKIN=1.
+ * The result holds no device memory. PS_ENODEV without a device. */
+ps_status ps_hierarchy_create_dev(const int32_t dims[3], const float* density, double nu, const uint8_t* bc,
+                                  int64_t coarsest_max_dof, const double* diag_add, ps_hierarchy_t** out);
 int32_t ps_hierarchy_num_levels(const ps_hierarchy_t* h);
 ps_status ps_hierarchy_level_info(const ps_hierarchy_t* h, int32_t level, int64_t info[9]);
 ps_status ps_hierarchy_level_fixed(const ps_hierarchy_t* h, int32_t level, uint8_t* out);

@@ -443,6 +443,24 @@ ps_status ps_hierarchy_create(const int32_t dims[3], const float* density, doubl
     });
 }
 
+ps_status ps_hierarchy_create_dev(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsest_max_dof,
+                                  const double* diag_add, ps_hierarchy_t** out) {
+    return guarded([&] {
+        if (!out || !dims) return fail(PS_EINVAL, "The structural grid must have three positive dimensions.");
+        *out = nullptr;
+        auto engine = psfea::makeDeviceGalerkin();
+        auto* h = new ps_hierarchy;
+        try {
+            h->H = psfea::buildHierarchy(dims, density, nu, bc, coarsest_max_dof, diag_add, engine.get());
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+        return PS_OK;
+    });
+}
+
 int32_t ps_hierarchy_num_levels(const ps_hierarchy_t* h) { return h ? int32_t(h->H.levels.size()) : 0; }
 
 ps_status ps_hierarchy_level_info(const ps_hierarchy_t* h, int32_t level, int64_t info[9]) {

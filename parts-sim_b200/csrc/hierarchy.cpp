@@ -12,7 +12,8 @@
 //   stop when free DOFs <= coarsestMaxDof, 12 levels, or 1x1x1 .... :174-180
 //   coarsest dense matrix, Cholesky with tiny pivots replaced by
 //   the largest diagonal, none when m == 0 or m > 3000 ........... :612-661
-// Everything runs over all host cores; the result does not depend on the thread count.
+// Everything runs over all host cores; the result does not depend on the thread count. An optional
+// engine (galerkin.cu) forms the own matrices of graded levels on the device, bitwise the same.
 #include "hierarchy.hpp"
 
 #include <cmath>
@@ -179,7 +180,7 @@ void galerkinAdd(double* out, const double* K, int c, double s) {
         }
 }
 
-HostLevel coarsen(const HostLevel& F) {
+HostLevel coarsen(const HostLevel& F, GalerkinEngine* engine) {
     HostLevel C = makeGrid((F.nx + 1) >> 1, (F.ny + 1) >> 1, (F.nz + 1) >> 1);
     double M[8][576];
     double Kc[576] = {};
@@ -295,13 +296,18 @@ HostLevel coarsen(const HostLevel& F) {
             }
         }
     }
-    parallelFor(int64_t(rep.size()), [&](int64_t c0, int64_t c1) {
-        std::vector<double> out(576), Kf(576);
-        for (int64_t c = c0; c < c1; c++) {
-            const int64_t o = rep[size_t(c)];
-            computeOwn(ownVox[size_t(o)], out.data(), Kf.data(), C.own.data() + o * 576);
-        }
-    }, 256);
+    if (engine && nOwn > 0 && int64_t(rep.size()) >= engine->minClasses()) {
+        // every own matrix (class members included: they come out bitwise equal to their class's)
+        engine->computeOwn(F, C, ownVox, M, C.own.data());
+    } else {
+        parallelFor(int64_t(rep.size()), [&](int64_t c0, int64_t c1) {
+            std::vector<double> out(576), Kf(576);
+            for (int64_t c = c0; c < c1; c++) {
+                const int64_t o = rep[size_t(c)];
+                computeOwn(ownVox[size_t(o)], out.data(), Kf.data(), C.own.data() + o * 576);
+            }
+        }, 256);
+    }
     parallelFor(nOwn, [&](int64_t o0, int64_t o1) {
         for (int64_t o = o0; o < o1; o++) {
             const int64_t r = rep[size_t(C.ownClass[size_t(o)])];
@@ -471,7 +477,7 @@ void chebyshevCoefficients(double lmax, double& first, double& c1, double& c2) {
 }
 
 Hierarchy buildHierarchy(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsestMaxDof,
-                         const double* diagAdd) {
+                         const double* diagAdd, GalerkinEngine* engine) {
     if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1) throw Error(PS_EINVAL, "The structural grid must have three positive dimensions.");
     if (int64_t(dims[0] + 1) * (dims[1] + 1) * (dims[2] + 1) >= (int64_t(1) << 31))
         throw Error(PS_EINVAL, "The structural grid has more than 2^31 nodes.");
@@ -502,7 +508,7 @@ Hierarchy buildHierarchy(const int32_t dims[3], const float* density, double nu,
         const HostLevel& L = H.levels.back();
         if (L.freeDof <= coarsestMaxDof || H.levels.size() >= 12) break;
         if (L.nx <= 1 && L.ny <= 1 && L.nz <= 1) break;
-        HostLevel C = coarsen(L);
+        HostLevel C = coarsen(L, engine);
         H.levels.push_back(std::move(C));
     }
     buildCoarsest(H);

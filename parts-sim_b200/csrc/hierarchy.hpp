@@ -75,9 +75,27 @@ struct Hierarchy {
     bool hasFactor() const { return !coarseInv.empty(); }
 };
 
-// Validates the inputs (Error(PS_EINVAL) with the reference's messages) and builds everything.
+// Computes the own Galerkin matrices of a coarse level somewhere other than the host loop (the
+// device engine of galerkin.cu): every own matrix o of C (coarse voxel ownVox[o]) as the host loop
+// computes it, bitwise (the same FP64 products and sums in the same order, rounded once to 32 bits).
+// M: the 8 child products P_c^T F.Kb P_c. coarsen() hands a level over when its classes of equal
+// child patterns number at least minClasses() (graded grids: every matrix distinct); lattices with
+// a few hundred classes stay on the host.
+struct GalerkinEngine {
+    virtual ~GalerkinEngine() = default;
+    virtual int64_t minClasses() const = 0;
+    virtual void computeOwn(const HostLevel& F, const HostLevel& C, const std::vector<int64_t>& ownVox, const double (*M)[576],
+                            float* out) = 0;
+};
+
+// the device engine on the current CUDA device (galerkin.cu), taking levels of at least
+// minClasses classes (PSFEA_DEVICE_GALERKIN_MIN overrides); throws Error(PS_ENODEV / PS_ECUDA)
+std::unique_ptr<GalerkinEngine> makeDeviceGalerkin(int64_t minClasses = 4096);
+
+// Validates the inputs (Error(PS_EINVAL) with the reference's messages) and builds everything;
+// with an engine, the own matrices of graded coarse levels come from it.
 Hierarchy buildHierarchy(const int32_t dims[3], const float* density, double nu, const uint8_t* bc, int64_t coarsestMaxDof,
-                         const double* diagAdd);
+                         const double* diagAdd, GalerkinEngine* engine = nullptr);
 
 // tridiagonal (a, b) largest eigenvalue by Sturm-count bisection (voxel_fea.cpp:506-530)
 double tridiagonalMax(const std::vector<double>& a, const std::vector<double>& b);

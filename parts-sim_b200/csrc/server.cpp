@@ -20,6 +20,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -102,6 +103,23 @@ void fail(ps_server* S, Request* R, ps_status st, const std::string& msg) {
 
 void builderLoop(ps_server* S) {
     cudaSetDevice(S->device);
+    // PSFEA_SERVER_GALERKIN=1: each build thread forms the Galerkin coarse matrices of its requests
+    // on the device (bitwise the host's) for levels of at least PSFEA_SERVER_GALERKIN_MIN (64)
+    // classes of child patterns. Off by default: on the 512-request stream it made builds slower
+    // (p50 3.9 -> 6.4 s) and the stream 21.3 -> 18.7 MDOF/s; the solves, not the builds, hold the
+    // requests back, and the products' round trips share the device with them.
+    std::unique_ptr<GalerkinEngine> engine;
+    {
+        const char* e = std::getenv("PSFEA_SERVER_GALERKIN");
+        const char* m = std::getenv("PSFEA_SERVER_GALERKIN_MIN");
+        if (e && std::atoi(e) != 0) {
+            try {
+                engine = makeDeviceGalerkin(m ? std::atoll(m) : 64);
+            } catch (const Error&) {
+                engine.reset();  // no device for the engine: the requests' builds stay on the host
+            }
+        }
+    }
     for (;;) {
         Request* R = nullptr;
         {
@@ -114,7 +132,8 @@ void builderLoop(ps_server* S) {
         ps_status st = PS_OK;
         std::string err;
         try {
-            auto h = std::make_unique<Hierarchy>(buildHierarchy(R->dims, R->density.data(), R->nu, R->bc.data(), R->coarsest, nullptr));
+            auto h = std::make_unique<Hierarchy>(buildHierarchy(R->dims, R->density.data(), R->nu, R->bc.data(), R->coarsest, nullptr,
+                                                                engine.get()));
             R->need = estimateDeviceBytes(*h);
             R->hier = std::move(h);
             R->density.clear();

@@ -136,6 +136,7 @@ _prune_dev = _sig("ps_prune_floating_dev", C.c_int, _I32P, C.c_void_p, C.c_void_
 _last_error = _sig("ps_last_error", C.c_char_p)
 _opts_default = _sig("ps_solve_opts_default", None, C.POINTER(SolveOpts))
 _h_create = _sig("ps_hierarchy_create", C.c_int, _I32P, _F32P, C.c_double, _U8P, C.c_int64, C.c_void_p, C.POINTER(C.c_void_p))
+_h_create_dev = _sig("ps_hierarchy_create_dev", C.c_int, _I32P, _F32P, C.c_double, _U8P, C.c_int64, C.c_void_p, C.POINTER(C.c_void_p))
 _h_nlev = _sig("ps_hierarchy_num_levels", C.c_int32, _P)
 _h_info = _sig("ps_hierarchy_level_info", C.c_int, _P, C.c_int32, _I64P)
 _h_fixed = _sig("ps_hierarchy_level_fixed", C.c_int, _P, C.c_int32, _U8P)
@@ -147,7 +148,7 @@ _h_destroy = _sig("ps_hierarchy_destroy", None, _P)
 EXPORTS = ("ps_solve_opts_default", "ps_fea_create", "ps_fea_solve", "ps_fea_solve_dev", "ps_fea_solve_batch", "ps_fea_precondition",
            "ps_fea_apply", "ps_fea_stresses", "ps_fea_reactions", "ps_fea_ndof", "ps_fea_num_levels", "ps_fea_level_info",
            "ps_fea_level_fixed", "ps_fea_level_lmax", "ps_fea_device_bytes", "ps_fea_destroy", "ps_element_matrix",
-           "ps_prune_floating", "ps_last_error", "ps_hierarchy_create", "ps_hierarchy_num_levels", "ps_hierarchy_level_info",
+           "ps_prune_floating", "ps_last_error", "ps_hierarchy_create", "ps_hierarchy_create_dev", "ps_hierarchy_num_levels", "ps_hierarchy_level_info",
            "ps_hierarchy_level_fixed", "ps_hierarchy_level_own", "ps_hierarchy_level_kb", "ps_hierarchy_destroy",
            "ps_fea_set_stream", "ps_fea_time_kernel", "ps_fea_kernel_launches", "ps_fea_apply_dot_noalloc", "ps_fea_precondition_block",
            "ps_topology_opts_default", "ps_topology_run", "ps_break_test", "ps_fea_autotune", "ps_fea_create_tuned",
@@ -440,9 +441,11 @@ class VoxelFEA:
 
 
 class Hierarchy:
-    """The host-side multigrid hierarchy alone (no GPU needed), for inspection and tests."""
+    """The host-side multigrid hierarchy alone, for inspection and tests. device=False: built on the
+    host threads (no GPU needed); device=True: the Galerkin coarse matrices of graded levels are
+    computed on the current CUDA device (the build ``VoxelFEA`` handles use), bitwise the same."""
 
-    def __init__(self, dims, density, nu, bc, coarsest_max_dof=1100, diag_add=None):
+    def __init__(self, dims, density, nu, bc, coarsest_max_dof=1100, diag_add=None, device=False):
         dims = np.ascontiguousarray(dims, np.int32)
         density = np.ascontiguousarray(density, np.float32).ravel()
         bc = np.ascontiguousarray(bc, np.uint8).ravel()
@@ -451,7 +454,7 @@ class Hierarchy:
             raise ValueError("Structural grid, density and fixture sizes do not match.")
         self._diag = None if diag_add is None else np.ascontiguousarray(diag_add, np.float64).ravel()
         h = C.c_void_p()
-        st = _h_create(dims, density, float(nu), bc, int(coarsest_max_dof), _ptr(self._diag), C.byref(h))
+        st = (_h_create_dev if device else _h_create)(dims, density, float(nu), bc, int(coarsest_max_dof), _ptr(self._diag), C.byref(h))
         if st != PS_OK:
             _raise(st)
         self.h = h
