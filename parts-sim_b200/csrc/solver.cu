@@ -1382,12 +1382,19 @@ struct DevMem {
 
 // a level's per-node (comps 1) or per-DOF (comps 3) host array in the pitched device layout,
 // padding entries `fill`
-template <class T, class A>
-std::vector<T> pitched(const std::vector<T, A>& v, int comps, const HostLevel& h, int PX, T fill) {
-    std::vector<T> o(size_t(PX) * h.NY * h.NZ * comps, fill);
+// (rows copied over the host threads, converted to T on the way, padding written per row)
+template <class T, class S, class A>
+std::vector<T, UninitAlloc<T>> pitched(const std::vector<S, A>& v, int comps, const HostLevel& h, int PX, T fill) {
+    std::vector<T, UninitAlloc<T>> o(size_t(PX) * h.NY * h.NZ * comps);
     const size_t rowIn = size_t(h.NX) * comps, rowOut = size_t(PX) * comps;
-    for (int64_t row = 0; row < int64_t(h.NY) * h.NZ; row++)
-        std::copy(v.begin() + row * rowIn, v.begin() + (row + 1) * rowIn, o.begin() + row * rowOut);
+    parallelFor(int64_t(h.NY) * h.NZ, [&](int64_t r0, int64_t r1) {
+        for (int64_t row = r0; row < r1; row++) {
+            T* out = o.data() + row * rowOut;
+            const S* in = v.data() + row * rowIn;
+            for (size_t q = 0; q < rowIn; q++) out[q] = T(in[q]);
+            for (size_t q = rowIn; q < rowOut; q++) out[q] = fill;
+        }
+    }, 1024);
     return o;
 }
 std::vector<uint32_t> pitchedWords(const HostLevel& h, int px) {
@@ -1751,10 +1758,20 @@ void SharedModel::uploadLevel(int l) {
     if (D.hasOwn) {
         upload(D.own, own, bytes, ms);
         // halves with a power-of-two level scale keeping the largest entry near 2^14
+        // (the largest entry by chunks over the host threads: the max does not depend on the split)
+        const int64_t nEnt = int64_t(own.size()), chunk = int64_t(1) << 20;
+        std::vector<double> cmax(size_t((nEnt + chunk - 1) / chunk), 0.0);
+        parallelFor(int64_t(cmax.size()), [&](int64_t c0, int64_t c1) {
+            for (int64_t c = c0; c < c1; c++) {
+                float m = 0.f;
+                for (int64_t i = c * chunk, e = std::min(nEnt, (c + 1) * chunk); i < e; i++) m = std::max(m, std::fabs(own[size_t(i)]));
+                cmax[size_t(c)] = double(m);
+            }
+        }, 1);
         double kmax = 0;
-        for (float v : own) kmax = std::max(kmax, double(std::fabs(v)));
+        for (double v : cmax) kmax = std::max(kmax, v);
         const float hs = kmax > 0 ? float(std::exp2(std::ceil(std::log2(kmax / 16384.0)))) : 1.f;
-        std::vector<__half> h16(own.size());
+        std::vector<__half, UninitAlloc<__half>> h16(own.size());  // every entry written below
         const float inv = 1.f / hs;
         parallelFor(int64_t(own.size()), [&](int64_t lo, int64_t hi) {
             for (int64_t i = lo; i < hi; i++) h16[size_t(i)] = __float2half_rn(own[size_t(i)] * inv);
@@ -1762,12 +1779,10 @@ void SharedModel::uploadLevel(int l) {
         upload(D.own16, h16, bytes, ms);
         D.view.hs = hs;
     }
-    std::vector<float> invD(h.invDiag.begin(), h.invDiag.end());
-    upload(D.invD, pitched<float>(invD, 3, h, PX, 0.f), bytes, ms);
+    upload(D.invD, pitched<float>(h.invDiag, 3, h, PX, 0.f), bytes, ms);
     if (!h.diagAdd.empty()) {
         upload(D.dadd, pitched<double>(h.diagAdd, 3, h, PX, 0.0), bytes, ms);
-        std::vector<float> d32(h.diagAdd.begin(), h.diagAdd.end());
-        upload(D.dadd32, pitched<float>(d32, 3, h, PX, 0.f), bytes, ms);
+        upload(D.dadd32, pitched<float>(h.diagAdd, 3, h, PX, 0.f), bytes, ms);
     }
     if (l == 0) upload(D.bc, pitched<uint8_t>(h.bc, 3, h, PX, uint8_t(0)), bytes, ms);
     {
