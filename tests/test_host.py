@@ -139,6 +139,17 @@ def test_no_device_is_reported_not_faked(have_gpu):
         psfea.VoxelFEA((4, 1, 1), np.ones(4, np.float32), 0.3, np.zeros(3 * 5 * 2 * 2, np.uint8))
 
 
+def test_device_hierarchy_build_needs_a_device(have_gpu):
+    """The device Galerkin build reports the missing device; the host build of the same model works."""
+    if have_gpu:
+        pytest.skip("a GPU is present")
+    dims, dens, bc = (4, 2, 2), np.ones(16, np.float32), np.zeros(3 * 5 * 3 * 3, np.uint8)
+    bc[:3 * 5 * 3] = 1
+    with pytest.raises(psfea.SolverError, match="ENODEV"):
+        psfea.Hierarchy(dims, dens, 0.3, bc, device=True)
+    assert psfea.Hierarchy(dims, dens, 0.3, bc).n_levels >= 1
+
+
 def test_server_needs_a_device(have_gpu):
     if have_gpu:
         pytest.skip("a GPU is present")
