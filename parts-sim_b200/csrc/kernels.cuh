@@ -414,7 +414,7 @@ template <int MODE> __host__ __device__ constexpr unsigned tileStage1Bytes() {
     return unsigned((tileHasR(MODE) ? tileBytesT<float>() : 0) + (tileHasD(MODE) ? 2 * tileBytesT<float>() : 0));
 }
 
-// ---- TMA and shared-memory barrier primitives (PTX, sm_90 and later; no cluster multicast)
+// ---- TMA and shared-memory barrier primitives (PTX, sm_90 and later; every copy lands in the issuing CTA's own shared memory)
 __device__ __forceinline__ unsigned smemAddr(const void* p) { return unsigned(__cvta_generic_to_shared(p)); }
 __device__ __forceinline__ void mbarInit(uint64_t* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smemAddr(bar)), "r"(count) : "memory");
