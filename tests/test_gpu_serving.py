@@ -5,6 +5,7 @@ is honoured."""
 import numpy as np
 import pytest
 
+import oracle
 import psfea
 import voxel_models as W
 
@@ -52,3 +53,33 @@ def test_bad_request_fails_alone():
     srv.close()
     assert rb["status"] == psfea.PS_EINVAL
     assert rg["converged"]
+
+
+def test_served_stream_requests_match_the_reference_solver():
+    """Requests drawn like the serving stream's (boxes with spherical voids, the three materials,
+    one face held, a traction on the opposite one; 24-56 voxels per axis here), served with the
+    bench's mixed form and with the drop-in, against the reference's own VoxelFEA::solve (compiled
+    from its sources) on the same arrays: the level-0 fixed mask bit-exact, the displacements
+    within 1e-6 relative L2 with both solvers driven to rel. res. 1e-10, the FP64-Krylov iteration
+    counts within 15 % of the reference's."""
+    models = [W.box_with_voids(W.Rng(5 * 1000003 + q), lo=24, hi=56) for q in range(4)]
+    out = {}
+    for precision in ("mixed", "fp64"):
+        srv = psfea.Server(max_active=4, build_threads=2)
+        ids = [srv.submit(m.dims, m.density, m.nu, m.bc, m.f, tol=1e-10, max_iter=5000, precision=precision, coarsest_max_dof=300)
+               for m in models]
+        out[precision] = [srv.wait(i) for i in ids]
+        srv.close()
+    for q, m in enumerate(models):
+        ref = oracle.OracleModel("reference", m.dims, m.density, m.nu, m.bc, 300)
+        u_ref, it_ref, res_ref, conv_ref = ref.solve(m.f, 1e-10, 5000)
+        S = psfea.VoxelFEA(m.dims, m.density, m.nu, m.bc, 300)
+        np.testing.assert_array_equal(S.fixed(0), ref.fixed(0))
+        S.close()
+        for precision in ("mixed", "fp64"):
+            r = out[precision][q]
+            assert r["status"] == psfea.PS_OK and r["converged"], (q, precision, r["status"])
+            err = float(np.linalg.norm(r["u"] - u_ref) / np.linalg.norm(u_ref))
+            assert err <= 1e-6, (q, m.dims, precision, err, r["iterations"], it_ref, res_ref, conv_ref)
+            assert abs(r["iterations"] - it_ref) <= 0.15 * it_ref + 1, (q, precision, r["iterations"], it_ref)
+        ref.close()
