@@ -980,14 +980,24 @@ __global__ void k_mx_fold2(long long nNodes, const uint8_t* __restrict__ nmask, 
 }
 
 // rzNew = r32.z32, zq = z32.q32 (FP64 sums); beta as in the FP64 form
-__global__ void k_mx_dots(long long nDof, const float* __restrict__ r, const float* __restrict__ z, const float* __restrict__ q,
-                          SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
+// r.z and z.q over the free DOFs (node by node: the held DOFs, every DOF of an inactive node
+// included, add nothing and are not read)
+__global__ void k_mx_dots(long long nNodes, const uint8_t* __restrict__ nmask, const float* __restrict__ r, const float* __restrict__ z,
+                          const float* __restrict__ q, SolveState* st, double* partials, unsigned* ticket, Ctl ctl) {
     if (skipped(ctl)) return;
     const bool first = st->first;
     double v[2] = {0, 0};
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x) {
-        v[0] += double(r[i]) * z[i];
-        if (!first) v[1] += double(z[i]) * q[i];
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+        if ((mask & 7) == 7) continue;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            if (fixedDof(mask, c)) continue;
+            const long long i = 3 * n + c;
+            const float zi = z[i];
+            v[0] += double(r[i]) * zi;
+            if (!first) v[1] += double(zi) * q[i];
+        }
     }
     double tot[2];
     if (gridReduce<2>(v, 0u, partials, ticket, tot) && threadIdx.x == 0) {
@@ -1012,12 +1022,26 @@ __global__ void k_mx_rescale(long long nDof, float* __restrict__ r32, const floa
     }
 }
 
-__global__ void k_mx_p(long long nDof, const float* __restrict__ z, float* __restrict__ p, const SolveState* st, Ctl ctl) {
+// p = z + beta p at the free DOFs; the first direction of a solve also writes 0 at every held DOF,
+// which then stays 0 (the later steps skip held DOFs and inactive nodes)
+__global__ void k_mx_p(long long nNodes, const uint8_t* __restrict__ nmask, const float* __restrict__ z, float* __restrict__ p,
+                       const SolveState* st, Ctl ctl) {
     if (skipped(ctl)) return;
     const float beta = float(st->beta);
     const bool first = st->first;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nDof; i += (long long)gridDim.x * blockDim.x)
-        p[i] = first ? z[i] : z[i] + beta * p[i];
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nNodes; n += (long long)gridDim.x * blockDim.x) {
+        const uint8_t mask = nmask[n];
+        if (!first && (mask & 7) == 7) continue;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const long long i = 3 * n + c;
+            if (fixedDof(mask, c)) {
+                if (first) p[i] = 0.f;
+                continue;
+            }
+            p[i] = first ? z[i] : z[i] + beta * p[i];
+        }
+    }
 }
 
 // ---------------------------------------------------------------- misc
@@ -2712,9 +2736,9 @@ void SolverImpl::recordMixedIteration(dev::Ctl ctl, bool refine, bool half) {
                    dev::Ctl{ctl.skipIf, &st()->restart});
         foldKernels = 0;
         float* z32 = vcycleFor(half, ctl, M->mixedOwn16, true);
-        launch(dev::k_mx_dots, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), W0.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(),
-               ctl);
-        launch(dev::k_mx_p, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), z32, p32.as<float>(), st(), ctl);
+        launch(dev::k_mx_dots, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, W0.r.as<float>(), z32, q32.as<float>(), st(),
+               part(), tick(), ctl);
+        launch(dev::k_mx_p, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, z32, p32.as<float>(), st(), ctl);
         return;
     }
     const cudaGraphNode_t* deps = nullptr;
@@ -2747,8 +2771,9 @@ void SolverImpl::recordMixedIteration(dev::Ctl ctl, bool refine, bool half) {
     check(cudaStreamEndCapture(stream, &body), "capture the fold");
     stream = mainStream;
     float* z32 = vcycleFor(half, ctl, M->mixedOwn16, true);  // the first smoothing step came with the update or the fold
-    launch(dev::k_mx_dots, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), W0.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
-    launch(dev::k_mx_p, vecGrid(pd(0)), dev::VEC_THREADS, 0, stream, pd(0), z32, p32.as<float>(), st(), ctl);
+    launch(dev::k_mx_dots, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, W0.r.as<float>(), z32, q32.as<float>(), st(), part(),
+           tick(), ctl);
+    launch(dev::k_mx_p, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, z32, p32.as<float>(), st(), ctl);
 }
 
 void SolverImpl::startSolve(const double* fDev, const double* x0Dev, const ps_solve_opts& o, double* uDev, double* uHost) {
@@ -2829,8 +2854,9 @@ void SolverImpl::startIterations() {
         launch(dev::k_vc_load, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, r.as<double>(), W0.r.as<float>(),
                D.invD.as<float>(), W0.d.as<float>(), W0.z.as<float>(), D.cf0, st(), ctl);
         float* z32 = vcycleFor(half, ctl, M->mixedOwn16, true);
-        launch(dev::k_mx_dots, vecGrid(n), dev::VEC_THREADS, 0, stream, n, W0.r.as<float>(), z32, q32.as<float>(), st(), part(), tick(), ctl);
-        launch(dev::k_mx_p, vecGrid(n), dev::VEC_THREADS, 0, stream, n, z32, p32.as<float>(), st(), ctl);
+        launch(dev::k_mx_dots, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, W0.r.as<float>(), z32, q32.as<float>(), st(),
+               part(), tick(), ctl);
+        launch(dev::k_mx_p, vecGrid(pn(0)), dev::VEC_THREADS, 0, stream, pn(0), D.view.nmask, z32, p32.as<float>(), st(), ctl);
     } else {
         float* z32 = nullptr;
         if (exactOneLevel()) {
